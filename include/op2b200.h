@@ -1,0 +1,192 @@
+/*
+ * op2b200.h -- C-ABI of the B200 (sm_100a) PyOP2 backend library.
+ *
+ * Every entry point takes plain pointers, sizes and opaque uint64_t handles
+ * (device pointers, streams, modules, plans, sparsities).  No torch or Python
+ * types cross this boundary, so the library can be bound from ctypes (the
+ * Python backend does this), cffi, or any FFI.
+ *
+ * All functions return OP2B_OK (0) on success or one of the OP2B_ERR_* codes;
+ * op2b_last_error() returns the message of the last failure on the calling
+ * thread.  Nothing in the library calls abort() or exit().
+ *
+ * Citations name the reference (gbts/PyOP2) interface each entry point
+ * replaces, as path:line within that project.
+ */
+#ifndef OP2B200_H
+#define OP2B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OP2B_OK            0
+#define OP2B_ERR_CUDA      1   /* a CUDA runtime call failed              */
+#define OP2B_ERR_NVRTC     2   /* JIT compilation of a par_loop stub      */
+#define OP2B_ERR_ARG       3   /* invalid argument (size, handle, index)  */
+#define OP2B_ERR_NOMEM     4   /* device or host allocation failed        */
+#define OP2B_ERR_STATE     5   /* library not initialised / already shut  */
+#define OP2B_ERR_MAP       6   /* a Map value lies outside its target Set */
+
+/* ------------------------------------------------------------------------
+ * Context.  Replaces cuda._setup (pyop2/cuda.py:824-847), which created one
+ * PyCUDA context and stream and read WARP_SIZE / MAX_SHARED_MEMORY_PER_BLOCK,
+ * and op2.exit (pyop2/op2.py:84-90).
+ * ---------------------------------------------------------------------- */
+int op2b_init(int device);
+int op2b_shutdown(void);
+int op2b_version(void);
+int op2b_last_error(char *buf, size_t len);
+/* sm_count, max opt-in dynamic shared memory per block, compute capability,
+ * global memory bytes, L2 bytes. */
+int op2b_device_info(int32_t *sm_count, int32_t *smem_optin, int32_t *cc_major,
+                     int32_t *cc_minor, uint64_t *total_mem, uint64_t *l2_bytes);
+
+/* ------------------------------------------------------------------------
+ * Device memory and transfers.  Replaces the PyCUDA gpuarray allocations and
+ * set()/get() used by DeviceDataMixin._allocate_device/_to_device/_from_device
+ * (pyop2/cuda.py:133-153) and Map._to_device (pyop2/cuda.py:375-388).
+ * Allocation is stream-ordered (no device-wide synchronisation on free).
+ * ---------------------------------------------------------------------- */
+int op2b_malloc(uint64_t *dptr, uint64_t bytes);
+int op2b_free(uint64_t dptr);
+int op2b_host_alloc(uint64_t *hptr, uint64_t bytes);   /* pinned host memory */
+int op2b_host_free(uint64_t hptr);
+int op2b_memcpy_h2d(uint64_t dst, const void *src, uint64_t bytes, uint64_t stream);
+int op2b_memcpy_d2h(void *dst, uint64_t src, uint64_t bytes, uint64_t stream);
+int op2b_memcpy_d2d(uint64_t dst, uint64_t src, uint64_t bytes, uint64_t stream);
+int op2b_memset(uint64_t dst, int value, uint64_t bytes, uint64_t stream);
+/* AoS <-> SoA reorder on the device, [n][dim] <-> [dim][n] with elements of
+ * elem_bytes (1,2,4,8).  Replaces DeviceDataMixin._maybe_to_soa/_maybe_to_aos
+ * (pyop2/device.py:153-174), which transposed on the host. */
+int op2b_transpose(uint64_t dst, uint64_t src, int64_t n, int32_t dim,
+                   int32_t elem_bytes, int32_t to_soa, uint64_t stream);
+/* Check that every value of a Map lies in [0, to_size); returns OP2B_ERR_MAP
+ * with the first offending position otherwise.  The reference trusted Map
+ * values (pyop2/base.py:1040-1048); out-of-range values would make a device
+ * kernel read outside a Dat. */
+int op2b_map_validate(uint64_t map, int64_t n_values, int32_t to_size,
+                      int64_t *bad_index, uint64_t stream);
+
+/* ------------------------------------------------------------------------
+ * Streams, events, CUDA graphs.  The reference used a single stream and
+ * synchronised after every par_loop (pyop2/cuda.py:656-658).  stream == 0
+ * names the library's own default op2 stream.
+ * ---------------------------------------------------------------------- */
+int op2b_default_stream(uint64_t *stream);
+int op2b_stream_create(uint64_t *stream);
+int op2b_stream_destroy(uint64_t stream);
+int op2b_stream_sync(uint64_t stream);
+int op2b_device_sync(void);
+int op2b_event_create(uint64_t *event);
+int op2b_event_destroy(uint64_t event);
+int op2b_event_record(uint64_t event, uint64_t stream);
+int op2b_event_sync(uint64_t event);
+int op2b_event_elapsed_ms(uint64_t start, uint64_t stop, float *ms);
+int op2b_stream_wait_event(uint64_t stream, uint64_t event);
+int op2b_graph_begin(uint64_t stream);
+int op2b_graph_end(uint64_t stream, uint64_t *graph_exec);
+int op2b_graph_launch(uint64_t graph_exec, uint64_t stream);
+int op2b_graph_destroy(uint64_t graph_exec);
+
+/* ------------------------------------------------------------------------
+ * JIT modules.  Replaces cuda.JITModule.compile (pyop2/cuda.py:610-651):
+ * PyCUDA SourceModule + Const upload.  The source is compiled by NVRTC for
+ * sm_100a straight to a cubin, which the caller may cache and reload.
+ * ---------------------------------------------------------------------- */
+int op2b_nvrtc_compile(const char *src, const char *name, const char *const *opts,
+                       int32_t nopts, void **cubin, uint64_t *cubin_bytes,
+                       char *log, uint64_t log_len);
+int op2b_cubin_free(void *cubin);
+int op2b_module_load(const void *cubin, uint64_t *module);
+int op2b_module_unload(uint64_t module);
+int op2b_module_function(uint64_t module, const char *name, uint64_t *fn);
+/* Device address and size of a __constant__ / __device__ symbol of a module
+ * (Const._to_device, pyop2/cuda.py:314-320). */
+int op2b_module_global(uint64_t module, const char *name, uint64_t *dptr, uint64_t *bytes);
+int op2b_function_set_smem(uint64_t fn, int32_t bytes);
+/* Launch fn with ONE by-value parameter: the packed struct params[0..nbytes).
+ * The generated stubs all take a single struct argument. */
+int op2b_launch(uint64_t fn, uint32_t grid, uint32_t block, uint32_t smem,
+                uint64_t stream, const void *params, uint64_t nbytes);
+/* Colour-by-colour launch of an indirect stub: for colour c the int32 pair at
+ * params+col_field_offset is set to (first block of c, blocks in c) and the
+ * stub is launched on grid = blocks in c.  Replaces the per-colour host loop
+ * with a stream synchronise before each launch (pyop2/cuda.py:757-800). */
+int op2b_launch_colored(uint64_t fn, int32_t ncolors, const int32_t *ncolblk,
+                        uint32_t block, uint32_t smem, uint64_t stream,
+                        void *params, uint64_t nbytes, uint64_t col_field_offset);
+
+/* ------------------------------------------------------------------------
+ * Plan: partitioning, staging maps and conflict colouring, built on the GPU.
+ * Replaces plan.pyx Plan.__cinit__ (pyop2/plan.pyx:93-376) and the cached
+ * _GenericPlan (pyop2/device.py:257-322).
+ *
+ * Staging pairs (one per unique indirect (Dat, Map)): stage_map[s] device map
+ * [set_size][stage_arity[s]], stage_nidx[s] indices taken from
+ * stage_idx[stage_idx_off[s] ...], stage_bytes[s] = itemsize*cdim of the Dat.
+ * Race groups (one per Dat written with INC, or Mat row set when matrix
+ * colouring is on): race_nent[g] (map, idx) entries taken from the flat
+ * race_map/race_arity/race_idx arrays, target Set size race_size[g].
+ * flags: bit0 staging, bit1 thread colouring.
+ * ---------------------------------------------------------------------- */
+#define OP2B_PLAN_STAGING         1
+#define OP2B_PLAN_THREAD_COLORING 2
+
+int op2b_plan_build(int32_t set_size, int32_t part_size,
+                    int32_t nstage, const uint64_t *stage_map, const int32_t *stage_arity,
+                    const int32_t *stage_nidx, const int32_t *stage_idx_off,
+                    const int32_t *stage_idx, const int32_t *stage_bytes,
+                    int32_t nrace, const int32_t *race_nent, const int32_t *race_size,
+                    const uint64_t *race_map, const int32_t *race_arity,
+                    const int32_t *race_idx, int32_t flags, uint64_t stream,
+                    uint64_t *plan);
+/* Scalars: nblocks, ncolors, nshared (max staged bytes per block, 16-byte
+ * aligned per pair), ninds (unique staging pairs), max_nthrcol,
+ * total staged ind_map length, loc_map rows. */
+int op2b_plan_info(uint64_t plan, int32_t *nblocks, int32_t *ncolors, int32_t *nshared,
+                   int32_t *ninds, int32_t *max_nthrcol, int64_t *ind_map_len,
+                   int32_t *loc_rows);
+/* Device arrays of the plan, in the reference layout (plan.pyx:140-212,
+ * 274-376):  0 nelems, 1 offset, 2 ind_map, 3 loc_map (int16), 4 ind_sizes,
+ * 5 ind_offs, 6 nindirect, 7 thrcol, 8 nthrcol, 9 blkmap, 10 ncolblk, and
+ * 11 blkcol (colour of every block). */
+int op2b_plan_array(uint64_t plan, int32_t which, uint64_t *dptr, int64_t *count);
+/* Host copy of ncolblk (ncolors entries), used to launch colour by colour. */
+int op2b_plan_ncolblk_host(uint64_t plan, int32_t *out, int32_t n);
+int op2b_plan_free(uint64_t plan);
+
+/* ------------------------------------------------------------------------
+ * Sparsity: CSR pattern built on the GPU.  Replaces core.build_sparsity
+ * (pyop2/op_lib_core.pyx:544-596) and build_sparsity_pattern_seq
+ * (pyop2/sparsity_utils.cxx:5-51): rows = rmult*rmap+r, cols = cmult*cmap+c,
+ * union over all map pairs, colidx sorted within each row.
+ * iterset_size[m] is the element count of pair m (its row map's from-set).
+ * ---------------------------------------------------------------------- */
+int op2b_sparsity_build(int32_t rmult, int32_t cmult, int32_t nrows, int32_t ncols,
+                        int32_t nmaps, const uint64_t *rmaps, const int32_t *rarity,
+                        const uint64_t *cmaps, const int32_t *carity,
+                        const int32_t *iterset_size, uint64_t stream, uint64_t *sparsity);
+/* lsize = nrows*rmult rows; nz = number of stored entries. */
+int op2b_sparsity_info(uint64_t sparsity, int32_t *lsize, int64_t *nz);
+/* Device arrays: rowptr (lsize+1 int32), colidx (nz int32), nnz (lsize int32). */
+int op2b_sparsity_arrays(uint64_t sparsity, uint64_t *rowptr, uint64_t *colidx,
+                         uint64_t *nnz);
+int op2b_sparsity_free(uint64_t sparsity);
+
+/* ------------------------------------------------------------------------
+ * Mat operations on the device CSR values (dtype 4 = float32, 8 = float64).
+ * Replaces cuda.Mat.zero_rows / zero (pyop2/cuda.py:289-301) and PETSc
+ * MatZeroRowsLocal (pyop2/petsc_base.py:131-135).
+ * ---------------------------------------------------------------------- */
+int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx,
+                       const int32_t *rows, int32_t nrows_zero, double diag,
+                       int32_t elem_bytes, uint64_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OP2B200_H */

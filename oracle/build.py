@@ -1,0 +1,57 @@
+"""Build the oracle's native parts.  TEST INFRASTRUCTURE ONLY.
+
+* ``oracle/_build/liboracle.so`` from ``oracle/csrc/oracle_core.c`` (gcc).
+* ``oracle/_ref/libref_sparsity.so``: the reference's own
+  ``pyop2/sparsity_utils.cxx`` compiled unmodified with g++ against the shim
+  header ``oracle/ref_shim/op_lib_core.h``, when the reference sources are
+  present (``OP2B_REFERENCE`` or /root/reference).  The reference's build
+  system is not used: its other native parts need OP2-Common and PETSc, which
+  are not available, so only this one translation unit is compiled.
+"""
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_OUT = os.path.join(HERE, "_ref")
+REFERENCE = os.environ.get("OP2B_REFERENCE", "/root/reference")
+
+
+def _stale(target, deps):
+    return not os.path.exists(target) or any(os.path.getmtime(d) > os.path.getmtime(target)
+                                             for d in deps)
+
+
+def build_oracle(force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    src = os.path.join(HERE, "csrc", "oracle_core.c")
+    out = os.path.join(BUILD, "liboracle.so")
+    if force or _stale(out, [src]):
+        subprocess.check_call(["gcc", "-O2", "-std=gnu99", "-shared", "-fPIC", src, "-o", out])
+    return out
+
+
+def build_ref(force=False):
+    """Compile the reference's sparsity_utils.cxx; None if it is absent."""
+    src = os.path.join(REFERENCE, "pyop2", "sparsity_utils.cxx")
+    if not os.path.exists(src):
+        return None
+    os.makedirs(REF_OUT, exist_ok=True)
+    out = os.path.join(REF_OUT, "libref_sparsity.so")
+    if force or _stale(out, [src]):
+        subprocess.check_call(["g++", "-O2", "-shared", "-fPIC",
+                               "-I" + os.path.join(HERE, "ref_shim"),
+                               "-I" + os.path.join(REFERENCE, "pyop2"), src, "-o", out])
+    return out
+
+
+def ref_lib_path():
+    p = os.path.join(REF_OUT, "libref_sparsity.so")
+    return p if os.path.exists(p) else None
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_ref(force="--force" in sys.argv))

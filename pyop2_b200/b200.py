@@ -1,0 +1,1041 @@
+"""The B200 (sm_100a) CUDA backend of the OP2 API.
+
+Replaces pyop2/cuda.py.  Objects keep their data resident in device memory
+owned by libop2b200.so and move it lazily, following the reference's
+DeviceDataMixin state machine (pyop2/device.py:103-183): DEVICE_UNALLOCATED,
+HOST (host copy newer), DEVICE (device copy newer), BOTH.
+
+* ``Sparsity`` is built on the GPU (op2b_sparsity_build); host copies of
+  rowptr/colidx/nnz are kept for the API (pyop2/base.py:1268-1312).
+* ``Mat`` values are a device CSR array assembled in place by the par_loop
+  stub; ``values``/``array``/``zero``/``zero_rows`` as pyop2/cuda.py:272-301.
+* ``Global`` reductions are finalised on the device; the host copy is fetched
+  when ``data`` is read.
+* ``par_loop`` JIT-compiles one stub per loop signature (NVRTC, cached in
+  memory and on disk), builds the plan on the GPU for indirect loops (cached
+  per iteration set, partition size, Maps and indices, like
+  pyop2/device.py:257-303) and launches colour by colour.
+"""
+
+import ctypes as C
+import hashlib
+import os
+import weakref
+
+import numpy as np
+
+from . import base, codegen
+from . import configuration as cfg
+from . import _lib
+from ._lib import call
+from .base import (INC, MAX, MIN, READ, RW, WRITE, IdentityMap, IterationIndex,  # noqa: F401
+                   i)
+from .exceptions import DeviceError, MapValueError
+from .logger import debug
+from .utils import as_tuple, maybe_setflags, verify_reshape
+
+DEVICE_UNALLOCATED = 'DEVICE_UNALLOCATED'
+HOST = 'HOST'
+DEVICE = 'DEVICE'
+BOTH = 'BOTH'
+
+_state = {'init': False, 'sm_count': 148, 'smem_optin': 232448, 'stream': 0, 'err': None,
+          'l2_bytes': 0}
+
+
+def _setup():
+    """Load the library and initialise the device (pyop2/cuda.py:824-847)."""
+    if _state['init']:
+        return
+    _lib.load()
+    call("op2b_init", int(cfg.cfg['device']))
+    sm, smem, ma, mi = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+    tot, l2 = C.c_uint64(), C.c_uint64()
+    call("op2b_device_info", C.byref(sm), C.byref(smem), C.byref(ma), C.byref(mi), C.byref(tot),
+         C.byref(l2))
+    s = C.c_uint64()
+    call("op2b_default_stream", C.byref(s))
+    _state.update(init=True, sm_count=sm.value, smem_optin=smem.value, stream=s.value,
+                  cc=(ma.value, mi.value), total_mem=tot.value, l2_bytes=l2.value)
+    _state['err'] = DeviceBuffer(16)
+    _state['err'].memset(0)
+
+
+def _teardown():
+    if not _state['init']:
+        return
+    try:
+        call("op2b_stream_sync", 0)
+    except DeviceError:
+        pass
+    ParLoop._bound_cache.clear()
+    _PLAN_CACHE.clear()
+    _state['init'] = False
+
+
+def device_info():
+    return dict(_state)
+
+
+def synchronize():
+    call("op2b_stream_sync", 0)
+
+
+def check_errors():
+    """Raise if a stub recorded a Mat insertion outside its Sparsity (PETSc's
+    NEW_NONZERO_ALLOCATION_ERR, pyop2/petsc_base.py:113-115)."""
+    err = _state['err']
+    if err is None:
+        return
+    h = np.zeros(4, dtype=np.int32)
+    err.to_host(h)
+    if h[0]:
+        err.memset(0)
+        raise MapValueError("Mat entry (%d, %d) is not in the Sparsity pattern" % (h[1], h[2]))
+
+
+# ----------------------------------------------------------- device memory
+class DeviceBuffer(object):
+    """A block of device memory, freed (stream-ordered) with the object."""
+
+    __slots__ = ("ptr", "nbytes", "__weakref__")
+
+    def __init__(self, nbytes):
+        self.nbytes = int(nbytes)
+        p = C.c_uint64()
+        call("op2b_malloc", C.byref(p), max(self.nbytes, 16))
+        self.ptr = p.value
+
+    def __del__(self):
+        if getattr(self, "ptr", 0) and _state['init'] and _lib._lib is not None:
+            _lib._lib.op2b_free(self.ptr)
+            self.ptr = 0
+
+    def from_host(self, arr):
+        arr = np.ascontiguousarray(arr)
+        assert arr.nbytes <= self.nbytes
+        call("op2b_memcpy_h2d", self.ptr, arr.ctypes.data, arr.nbytes, 0)
+
+    def to_host(self, arr):
+        assert arr.flags['C_CONTIGUOUS'] and arr.nbytes <= self.nbytes
+        call("op2b_memcpy_d2h", arr.ctypes.data, self.ptr, arr.nbytes, 0)
+
+    def memset(self, value=0, nbytes=None):
+        call("op2b_memset", self.ptr, value, self.nbytes if nbytes is None else nbytes, 0)
+
+
+def _upload(arr):
+    arr = np.ascontiguousarray(arr)
+    buf = DeviceBuffer(arr.nbytes)
+    buf.from_host(arr)
+    return buf
+
+
+def pinned_empty(shape, dtype):
+    """A numpy array in pinned host memory (fast, asynchronous copies)."""
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape)) * dtype.itemsize
+    p = C.c_uint64()
+    call("op2b_host_alloc", C.byref(p), max(n, 16))
+    raw = (C.c_char * max(n, 16)).from_address(p.value)
+    arr = np.frombuffer(raw, dtype=np.uint8, count=n).view(dtype).reshape(shape)
+    weakref.finalize(raw, _lib._lib.op2b_host_free, p.value)
+    arr_holder = _PinnedHolder(arr, raw)
+    return arr_holder.array
+
+
+class _PinnedHolder(object):
+    def __init__(self, array, raw):
+        self.array = array
+        self.raw = raw
+        array_base = array
+        while array_base.base is not None and isinstance(array_base.base, np.ndarray):
+            array_base = array_base.base
+
+
+# ------------------------------------------------------------------ classes
+Arg = base.Arg
+Set = base.Set
+Halo = base.Halo
+IterationSpace = base.IterationSpace
+
+
+class Kernel(base.Kernel):
+    """User kernel; the code is compiled for the device inside the stub."""
+
+
+class DeviceDataMixin(object):
+    """Host/device coherence (pyop2/device.py:103-183)."""
+
+    DEVICE_UNALLOCATED = DEVICE_UNALLOCATED
+    HOST = HOST
+    DEVICE = DEVICE
+    BOTH = BOTH
+
+    @property
+    def state(self):
+        return self._state
+
+    @state.setter
+    def state(self, value):
+        self._state = value
+
+    @property
+    def _bytes_per_elem(self):
+        return self.dtype.itemsize * self.cdim
+
+    @property
+    def _is_scalar(self):
+        return self.cdim == 1
+
+
+class Dat(DeviceDataMixin, base.Dat):
+
+    def __init__(self, dataset, data=None, dtype=None, name=None, soa=None, uid=None):
+        base.Dat.__init__(self, dataset, data, dtype, name, soa, uid)
+        self._state = DEVICE_UNALLOCATED
+        self._device = None
+
+    # host views ---------------------------------------------------------
+    @property
+    def data(self):
+        if self.dataset.total_size > 0 and self._data.size == 0:
+            raise RuntimeError("Illegal access: no data associated with this Dat!")
+        maybe_setflags(self._data, write=True)
+        self._from_device()
+        if self._state is not DEVICE_UNALLOCATED:
+            self._state = HOST
+        self.needs_halo_update = True
+        return self._data
+
+    @data.setter
+    def data(self, value):
+        maybe_setflags(self._data, write=True)
+        self._data = verify_reshape(value, self.dtype, self._data.shape)
+        if self._state is not DEVICE_UNALLOCATED:
+            self._state = HOST
+
+    @property
+    def data_ro(self):
+        if self.dataset.total_size > 0 and self._data.size == 0:
+            raise RuntimeError("Illegal access: no data associated with this Dat!")
+        maybe_setflags(self._data, write=True)
+        self._from_device()
+        if self._state is not DEVICE_UNALLOCATED:
+            self._state = BOTH
+        maybe_setflags(self._data, write=False)
+        return self._data
+
+    # device side --------------------------------------------------------
+    def _allocate_device(self):
+        if self._state is DEVICE_UNALLOCATED:
+            self._device = DeviceBuffer(max(self._data.nbytes, 16))
+            self._state = HOST
+
+    def _to_device(self):
+        self._allocate_device()
+        if self._state is HOST:
+            if self.soa and self.cdim > 1:
+                staging = _upload(self._data)
+                call("op2b_transpose", self._device.ptr, staging.ptr, self.dataset.total_size,
+                     self.cdim, self.dtype.itemsize, 1, 0)
+                del staging
+            else:
+                self._device.from_host(self._data)
+            self._state = BOTH
+
+    def _from_device(self):
+        if self._state is DEVICE:
+            maybe_setflags(self._data, write=True)
+            if self.soa and self.cdim > 1:
+                staging = DeviceBuffer(self._data.nbytes)
+                call("op2b_transpose", staging.ptr, self._device.ptr, self.dataset.total_size,
+                     self.cdim, self.dtype.itemsize, 0, 0)
+                staging.to_host(self._data)
+            else:
+                self._device.to_host(self._data)
+            self._state = BOTH
+
+    @property
+    def array(self):
+        """Device buffer of the values (uploaded if needed)."""
+        self._to_device()
+        return self._device
+
+    def zero(self):
+        """Zero the Dat on the device."""
+        self._allocate_device()
+        self._device.memset(0)
+        self._state = DEVICE
+
+    @property
+    def norm(self):
+        return np.linalg.norm(self.data_ro)
+
+
+class Const(DeviceDataMixin, base.Const):
+    """Global constant: a __constant__ symbol of each stub that names it,
+    uploaded when its value changed (pyop2/cuda.py:303-323)."""
+
+    def __init__(self, dim, data=None, name=None, dtype=None):
+        base.Const.__init__(self, dim, data, name, dtype)
+        self._version = 0
+        self._state = HOST
+
+    @property
+    def data(self):
+        self._version += 1
+        return self._data
+
+    @data.setter
+    def data(self, value):
+        self._data = verify_reshape(value, self.dtype, self.dim)
+        self._version += 1
+
+    def _from_device(self):
+        raise RuntimeError("Copying Const %s from device not allowed" % self)
+
+
+class Global(DeviceDataMixin, base.Global):
+
+    def __init__(self, dim, data=None, dtype=None, name=None):
+        base.Global.__init__(self, dim, data, dtype, name)
+        self._state = DEVICE_UNALLOCATED
+        self._device = None
+        self._partials = None
+        self._counter = None
+
+    @property
+    def data(self):
+        if len(self._data) == 0:
+            raise RuntimeError("Illegal access: No data associated with this Global!")
+        self._from_device()
+        if self._state is not DEVICE_UNALLOCATED:
+            self._state = HOST
+        return self._data
+
+    @data.setter
+    def data(self, value):
+        self._data = verify_reshape(value, self.dtype, self.dim)
+        if self._state is not DEVICE_UNALLOCATED:
+            self._state = HOST
+
+    @property
+    def data_ro(self):
+        self._from_device()
+        if self._state is not DEVICE_UNALLOCATED:
+            self._state = BOTH
+        return self._data
+
+    def _to_device(self):
+        if self._state is DEVICE_UNALLOCATED:
+            self._device = DeviceBuffer(max(self._data.nbytes, 16))
+            self._state = HOST
+        if self._state is HOST:
+            self._device.from_host(self._data)
+            self._state = BOTH
+
+    def _from_device(self):
+        if self._state is DEVICE:
+            self._device.to_host(self._data)
+            self._state = BOTH
+
+    def _reduction_buffers(self, nblocks):
+        """Per-CTA partials and the arrival counter of op2b_reduce (scratch)."""
+        need = max(1, nblocks) * self.cdim * self.dtype.itemsize
+        if self._partials is None or self._partials.nbytes < need:
+            self._partials = DeviceBuffer(need)
+        if self._counter is None:
+            self._counter = DeviceBuffer(16)
+            self._counter.memset(0)
+        return self._partials.ptr, self._counter.ptr
+
+
+_MAP_DEVICE = weakref.WeakValueDictionary()
+
+
+class Map(base.Map):
+    """Map with device values.  Maps whose values are the same host buffer
+    share one device copy (e.g. pecell / pevcell of the airfoil demo)."""
+
+    def __init__(self, iterset, dataset, dim, values=None, name=None):
+        if values is None:
+            raise MapValueError("Map values must be populated.")
+        base.Map.__init__(self, iterset, dataset, dim, values, name)
+        self._device = None
+
+    def _to_device(self):
+        if self._device is None:
+            v = self._values
+            key = (v.__array_interface__['data'][0], v.nbytes)
+            buf = _MAP_DEVICE.get(key)
+            if buf is None or buf.nbytes != v.nbytes:
+                buf = _upload(v)
+                if v.nbytes:
+                    _MAP_DEVICE[key] = buf
+                    self._keep_values = v
+            if cfg.cfg['validate_maps'] and v.size:
+                bad = C.c_int64(-1)
+                rc = _lib._lib.op2b_map_validate(buf.ptr, v.size, self._dataset.total_size,
+                                                 C.byref(bad), 0)
+                if rc != 0:
+                    raise MapValueError("Map %s: value at position %d lies outside its target "
+                                        "Set of size %d" % (self._name, bad.value,
+                                                            self._dataset.total_size))
+            self._device = buf
+        return self._device
+
+
+class Sparsity(base.Sparsity):
+    """CSR pattern built on the device (op2b_sparsity_build)."""
+
+    _cache = {}
+
+    def _build(self):
+        # built on the device at first use (_ensure), not at construction
+        self._handle = 0
+        self._host_arrays = None
+
+    def _ensure(self):
+        if self._handle:
+            return
+        nmaps = len(self._rmaps)
+        rptr = (C.c_uint64 * nmaps)(*[m._to_device().ptr for m in self._rmaps])
+        cptr = (C.c_uint64 * nmaps)(*[m._to_device().ptr for m in self._cmaps])
+        rar = (C.c_int32 * nmaps)(*[m.dim for m in self._rmaps])
+        car = (C.c_int32 * nmaps)(*[m.dim for m in self._cmaps])
+        its = (C.c_int32 * nmaps)(*[m.iterset.size for m in self._rmaps])
+        h = C.c_uint64()
+        rmult, cmult = self._dims
+        call("op2b_sparsity_build", rmult, cmult, self._nrows, self._ncols, nmaps, rptr, rar, cptr,
+             car, its, 0, C.byref(h))
+        lsize, nz = C.c_int32(), C.c_int64()
+        call("op2b_sparsity_info", h.value, C.byref(lsize), C.byref(nz))
+        rp, ci, nn = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        call("op2b_sparsity_arrays", h.value, C.byref(rp), C.byref(ci), C.byref(nn))
+        self._d_rowptr_, self._d_colidx_, self._d_nnzp = rp.value, ci.value, nn.value
+        self._lsize = lsize.value
+        self._d_nz_ = int(nz.value)
+        self._handle = h.value
+
+    @property
+    def _d_rowptr(self):
+        self._ensure()
+        return self._d_rowptr_
+
+    @property
+    def _d_colidx(self):
+        self._ensure()
+        return self._d_colidx_
+
+    @property
+    def _d_nz(self):
+        self._ensure()
+        return self._d_nz_
+
+    @property
+    def _o_nz(self):
+        return 0
+
+    @property
+    def _o_nnz(self):
+        return np.zeros(0, dtype=np.int32)
+
+    def _host(self):
+        self._ensure()
+        if self._host_arrays is None:
+            rowptr = np.empty(self._lsize + 1, dtype=np.int32)
+            colidx = np.empty(max(self._d_nz, 0), dtype=np.int32)
+            nnz = np.empty(self._lsize, dtype=np.int32)
+            call("op2b_memcpy_d2h", rowptr.ctypes.data, self._d_rowptr, rowptr.nbytes, 0)
+            call("op2b_memcpy_d2h", colidx.ctypes.data, self._d_colidx, colidx.nbytes, 0)
+            call("op2b_memcpy_d2h", nnz.ctypes.data, self._d_nnzp, nnz.nbytes, 0)
+            self._host_arrays = (rowptr, colidx, nnz)
+        return self._host_arrays
+
+    @property
+    def _rowptr(self):
+        return self._host()[0]
+
+    @property
+    def _colidx(self):
+        return self._host()[1]
+
+    @property
+    def _d_nnz(self):
+        return self._host()[2]
+
+    @property
+    def rowptr(self):
+        return self._rowptr
+
+    @property
+    def colidx(self):
+        return self._colidx
+
+    def __del__(self):
+        h = getattr(self, "_handle", 0)
+        if h and _state['init'] and _lib._lib is not None:
+            _lib._lib.op2b_sparsity_free(h)
+
+
+class Mat(DeviceDataMixin, base.Mat):
+    """Device CSR values on a Sparsity."""
+
+    def __init__(self, sparsity, dtype=None, name=None):
+        base.Mat.__init__(self, sparsity, dtype, name)
+        self._state = DEVICE_UNALLOCATED
+        self._vals = None
+
+    def _device_values(self):
+        if self._vals is None:
+            self._vals = DeviceBuffer(max(self._sparsity.nz, 1) * self.dtype.itemsize)
+            self._vals.memset(0)
+            self._state = DEVICE
+        return self._vals
+
+    @property
+    def array(self):
+        """CSR values (host copy)."""
+        check_errors()
+        out = np.zeros(self._sparsity.nz, dtype=self.dtype)
+        if self._vals is not None:
+            self._vals.to_host(out)
+        return out
+
+    @property
+    def values(self):
+        """Dense matrix (only sensible for small matrices)."""
+        rows = self._sparsity.nrows * self.dims[0]
+        cols = self._sparsity.ncols * self.dims[1]
+        ret = np.zeros((rows, cols), dtype=self.dtype)
+        vals = self.array
+        rowptr, colidx = self._sparsity._rowptr, self._sparsity._colidx
+        for r in range(rows):
+            ret[r, colidx[rowptr[r]:rowptr[r + 1]]] = vals[rowptr[r]:rowptr[r + 1]]
+        return ret
+
+    def zero(self):
+        self._device_values().memset(0)
+
+    def zero_rows(self, rows, diag_val):
+        """Zero the given rows except the diagonal, set to diag_val."""
+        rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).ravel())
+        vals = self._device_values()
+        call("op2b_mat_zero_rows", vals.ptr, self._sparsity._d_rowptr, self._sparsity._d_colidx,
+             rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, float(diag_val),
+             self.dtype.itemsize, 0)
+
+    def _assemble(self):
+        pass
+
+
+class Solver(base.Solver):
+    def solve(self, A, x, b):
+        raise NotImplementedError("The linear solve is not part of the B200 backend's hot path")
+
+
+# ------------------------------------------------------------------- plans
+_PLAN_CACHE = {}
+
+_PLAN_ARRAYS = ("nelems", "offset", "ind_map", "loc_map", "ind_sizes", "ind_offs", "nindirect",
+                "thrcol", "nthrcol", "blkmap", "ncolblk", "blkcol")
+
+
+class DevicePlan(object):
+    """A plan built on the GPU (op2b_plan_build), in plan.pyx's layout."""
+
+    def __init__(self, set_size, part_size, stages, races, staging=True, thread_coloring=True):
+        """stages: [(map, [idx...], bytes_per_elem)]; races: [([(map, idx)...], target_size)]."""
+        ns = len(stages)
+        smap = (C.c_uint64 * max(ns, 1))(*[m._to_device().ptr for m, _, _ in stages])
+        sar = (C.c_int32 * max(ns, 1))(*[m.dim for m, _, _ in stages])
+        snidx = (C.c_int32 * max(ns, 1))(*[len(ix) for _, ix, _ in stages])
+        offs, flat = [], []
+        for _, ix, _ in stages:
+            offs.append(len(flat))
+            flat += list(ix)
+        soff = (C.c_int32 * max(ns, 1))(*offs)
+        sidx = (C.c_int32 * max(len(flat), 1))(*flat)
+        sbytes = (C.c_int32 * max(ns, 1))(*[b for _, _, b in stages])
+        nr = len(races)
+        rnent = (C.c_int32 * max(nr, 1))(*[len(e) for e, _ in races])
+        rsize = (C.c_int32 * max(nr, 1))(*[s for _, s in races])
+        ents = [x for e, _ in races for x in e]
+        rmap = (C.c_uint64 * max(len(ents), 1))(*[m._to_device().ptr for m, _ in ents])
+        rar = (C.c_int32 * max(len(ents), 1))(*[m.dim for m, _ in ents])
+        ridx = (C.c_int32 * max(len(ents), 1))(*[ix for _, ix in ents])
+        flags = (1 if staging else 0) | (2 if thread_coloring else 0)
+        h = C.c_uint64()
+        call("op2b_plan_build", set_size, part_size, ns, smap, sar, snidx, soff, sidx, sbytes, nr,
+             rnent, rsize, rmap, rar, ridx, flags, 0, C.byref(h))
+        self._handle = h.value
+        nb, nc, nsh, ni, mx, ml, lr = (C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(),
+                                       C.c_int32(), C.c_int64(), C.c_int32())
+        call("op2b_plan_info", self._handle, C.byref(nb), C.byref(nc), C.byref(nsh), C.byref(ni),
+             C.byref(mx), C.byref(ml), C.byref(lr))
+        self.nblocks, self.ncolors, self.nshared, self.ninds = nb.value, nc.value, nsh.value, ni.value
+        self.max_nthrcol = mx.value
+        self.part_size = part_size
+        self.set_size = set_size
+        ncb = (C.c_int32 * max(self.ncolors, 1))()
+        call("op2b_plan_ncolblk_host", self._handle, ncb, self.ncolors)
+        self.ncolblk_host = ncb
+        self.max_blocks_per_color = max(list(ncb)[:self.ncolors] or [0])
+        self.dptr = {}
+        self.counts = {}
+        for k, name in enumerate(_PLAN_ARRAYS):
+            p, n = C.c_uint64(), C.c_int64()
+            call("op2b_plan_array", self._handle, k, C.byref(p), C.byref(n))
+            self.dptr[name] = p.value
+            self.counts[name] = n.value
+
+    def host_array(self, name):
+        dtype = np.int16 if name == "loc_map" else np.int32
+        out = np.zeros(self.counts[name], dtype=dtype)
+        if out.size:
+            call("op2b_memcpy_d2h", out.ctypes.data, self.dptr[name], out.nbytes, 0)
+        return out
+
+    def __getattr__(self, name):
+        if name in _PLAN_ARRAYS:
+            return self.host_array(name)
+        raise AttributeError(name)
+
+    def __del__(self):
+        h = getattr(self, "_handle", 0)
+        if h and _state['init'] and _lib._lib is not None:
+            _lib._lib.op2b_plan_free(h)
+
+
+def Plan(kernel, iset, *args, **kwargs):
+    """Reference-compatible plan constructor (pyop2/device.py:305-322,
+    plan.pyx:93-105): ``args`` are unwound Args, ``partition_size``,
+    ``matrix_coloring``, ``staging`` and ``thread_coloring`` as in the
+    reference.  Staging pairs follow the first appearance of each indirect
+    (Dat, Map); race groups are the INC Dats and, with matrix colouring, the
+    Mats' row Maps."""
+    ps = kwargs.get('partition_size', 1)
+    mc = kwargs.get('matrix_coloring', False)
+    st = kwargs.get('staging', True)
+    tc = kwargs.get('thread_coloring', True)
+    iset = iset._iterset if isinstance(iset, base.IterationSpace) else iset
+    stages, order = [], {}
+    for a in args:
+        if a._is_mat or not a._is_indirect:
+            continue
+        k = (id(a.data), id(a.map))
+        if k not in order:
+            order[k] = len(stages)
+            stages.append([a.map, [], a.data.dtype.itemsize * a.data.cdim])
+        stages[order[k]][1].append(a.idx)
+    races, rorder = [], {}
+    for a in args:
+        if a._is_indirect_reduction:
+            k = id(a.data)
+            if k not in rorder:
+                rorder[k] = len(races)
+                races.append([[], a.data.dataset.size])
+            races[rorder[k]][0].append((a.map, a.idx))
+        elif mc and a._is_mat:
+            k = id(a.data)
+            rmap = a.map[0]
+            if k not in rorder:
+                rorder[k] = len(races)
+                races.append([[], rmap.dataset.size])
+            races[rorder[k]][0] += [(rmap, r) for r in range(rmap.dim)]
+    return DevicePlan(iset.size, ps, [tuple(s) for s in stages], [tuple(r) for r in races],
+                      staging=st, thread_coloring=tc)
+
+
+# --------------------------------------------------------------- JIT cache
+_MODULES = {}
+
+
+class _Module(object):
+    def __init__(self, source, fmad, name):
+        opts = codegen.nvrtc_options(fmad=fmad)
+        digest = hashlib.sha256((source + "\0" + " ".join(opts)).encode()).hexdigest()
+        cubin = _disk_cache_get(digest)
+        if cubin is None:
+            arr = (C.c_char_p * len(opts))(*[o.encode() for o in opts])
+            out = C.c_void_p()
+            n = C.c_uint64()
+            log = C.create_string_buffer(1 << 16)
+            rc = _lib._lib.op2b_nvrtc_compile(source.encode(), (name + ".cu").encode(), arr,
+                                              len(opts), C.byref(out), C.byref(n), log, len(log))
+            if rc != 0:
+                raise DeviceError("NVRTC compilation of the %s stub failed:\n%s\n--- source ---\n%s"
+                                  % (name, _lib.last_error(), source[-6000:]))
+            cubin = C.string_at(out.value, n.value)
+            _lib._lib.op2b_cubin_free(out)
+            _disk_cache_put(digest, cubin)
+        self._cubin = cubin
+        h = C.c_uint64()
+        call("op2b_module_load", cubin, C.byref(h))
+        self.handle = h.value
+        fn = C.c_uint64()
+        call("op2b_module_function", self.handle, b"op2b_stub", C.byref(fn))
+        self.fn = fn.value
+        self.smem_set = 48 * 1024
+        self.const_versions = {}
+
+    def const_ptr(self, name):
+        p, n = C.c_uint64(), C.c_uint64()
+        call("op2b_module_global", self.handle, name.encode(), C.byref(p), C.byref(n))
+        return p.value, n.value
+
+    def ensure_smem(self, nbytes):
+        if nbytes > self.smem_set:
+            call("op2b_function_set_smem", self.fn, int(nbytes))
+            self.smem_set = nbytes
+
+
+def _disk_cache_get(digest):
+    path = os.path.join(cfg.cfg['cache_dir'], digest + ".cubin")
+    try:
+        with open(path, "rb") as f:
+            return f.read()
+    except OSError:
+        return None
+
+
+def _disk_cache_put(digest, cubin):
+    d = cfg.cfg['cache_dir']
+    try:
+        os.makedirs(d, exist_ok=True)
+        tmp = os.path.join(d, "%s.%d.tmp" % (digest, os.getpid()))
+        with open(tmp, "wb") as f:
+            f.write(cubin)
+        os.replace(tmp, os.path.join(d, digest + ".cubin"))
+    except OSError:
+        pass
+
+
+def _get_module(spec):
+    key = spec.key()
+    mod = _MODULES.get(key)
+    if mod is None:
+        src, layout, _ = codegen.generate(spec)
+        mod = _Module(src, spec.fmad, spec.kernel_name)
+        mod.layout = layout
+        mod.source = src
+        _MODULES[key] = mod
+    return mod
+
+
+# ------------------------------------------------------------------ par_loop
+def _acc_name(acc):
+    return acc._mode
+
+
+def loop_spec(loop, block_size=None, fmad=None):
+    """Static description of a par_loop: the LoopSpec of its stub plus the
+    unique Dats/Maps/Mats/Globals, the INC staging pairs and the plan race
+    groups.  Touches no device memory (used to generate and test stubs)."""
+    it = loop.it_space
+    iterset = it.iterset
+    extents = it.extents
+    args = loop.args
+    dats, dat_slot = [], {}
+    maps, map_slot = [], {}
+    mats, mat_slot = [], {}
+    gbls = []
+    specs = []
+    # access summary per Dat: read-only if every use is READ
+    dat_modes = {}
+    for a in args:
+        if a._is_dat:
+            dat_modes.setdefault(id(a.data), set()).add(a.access._mode)
+
+    def dslot(d):
+        k = id(d)
+        if k not in dat_slot:
+            dat_slot[k] = len(dats)
+            dats.append(d)
+        return dat_slot[k]
+
+    def mslot(m):
+        k = id(m)
+        if k not in map_slot:
+            map_slot[k] = len(maps)
+            maps.append(m)
+        return map_slot[k]
+
+    indirect = False
+    for a in args:
+        acc = a.access._mode
+        if a._is_global:
+            gbls.append(a.data)
+            specs.append(codegen.ArgSpec(kind="gbl", access=acc, ctype=a.data.ctype,
+                                         cdim=a.data.cdim, slot=len(gbls) - 1))
+        elif a._is_mat:
+            indirect = True
+            m = a.data
+            if id(m) not in mat_slot:
+                mat_slot[id(m)] = len(mats)
+                mats.append(m)
+            rm, cm = m.dims
+            if len(extents) != 2:
+                raise MapValueError("A Mat argument needs a 2-d iteration space")
+            specs.append(codegen.ArgSpec(
+                kind="mat", access=acc, ctype=m.ctype, cdim=1, slot=mat_slot[id(m)],
+                mslot=mslot(a.map[0]), cmslot=mslot(a.map[1]), idx=a.idx[0].index,
+                cidx=a.idx[1].index, arity=a.map[0].dim, carity=a.map[1].dim,
+                ext=extents[0], cext=extents[1], rm=rm, cm=cm))
+        elif a._is_direct:
+            d = a.data
+            specs.append(codegen.ArgSpec(kind="direct", access=acc, ctype=d.ctype, cdim=d.cdim,
+                                         slot=dslot(d), soa=bool(d.soa),
+                                         ro=dat_modes[id(d)] == {"READ"}))
+        else:
+            indirect = True
+            d = a.data
+            if d.soa:
+                raise NotImplementedError("SoA Dats are supported in direct loops only")
+            if a.idx is None:
+                kind, ix, ext = "vec", None, None
+            elif isinstance(a.idx, IterationIndex):
+                kind, ix = "its", a.idx.index
+                if ix >= len(extents):
+                    raise MapValueError("Iteration index %d outside the iteration space" % ix)
+                ext = extents[ix]
+            else:
+                kind, ix, ext = "ind", int(a.idx), None
+            specs.append(codegen.ArgSpec(kind=kind, access=acc, ctype=d.ctype, cdim=d.cdim,
+                                         slot=dslot(d), mslot=mslot(a.map), idx=ix,
+                                         arity=a.map.dim, ext=ext,
+                                         ro=dat_modes[id(d)] == {"READ"}))
+    # INC staging pairs and plan race groups (unwound like device.py:390-419)
+    stages, stage_of = [], {}
+    races, race_of = [], {}
+    for n, (a, s) in enumerate(zip(args, specs)):
+        if s.kind in ("ind", "vec", "its") and s.access == "INC":
+            key = (s.slot, s.mslot)
+            if key not in stage_of:
+                stage_of[key] = len(stages)
+                stages.append([s.slot, s.mslot, s.ctype, s.cdim, []])
+            st = stages[stage_of[key]]
+            unwound = [s.idx] if s.kind == "ind" else list(range(s.arity if s.kind == "vec" else s.ext))
+            s.stage = stage_of[key]
+            s.loc_rows = []
+            for ix in unwound:
+                s.loc_rows.append(len(st[4]))
+                st[4].append(ix)
+            rk = ("dat", s.slot)
+            if rk not in race_of:
+                race_of[rk] = len(races)
+                races.append([[], a.data.dataset.size])
+            races[race_of[rk]][0] += [(a.map, ix) for ix in unwound]
+        elif s.kind == "mat":
+            rk = ("mat", s.slot)
+            rmap = a.map[0]
+            if rk not in race_of:
+                race_of[rk] = len(races)
+                races.append([[], rmap.dataset.size])
+            races[race_of[rk]][0] += [(rmap, r) for r in range(rmap.dim)]
+    # loc_map rows are numbered over all staged pairs in order
+    base_row = 0
+    row_base = []
+    for st in stages:
+        row_base.append(base_row)
+        base_row += len(st[4])
+    for s in specs:
+        if s.loc_rows is not None:
+            s.loc_rows = [row_base[s.stage] + r for r in s.loc_rows]
+    consts = [(c.name, c.ctype, c.cdim) for c in base.Const._definitions()]
+    bs = int(block_size or cfg.cfg['block_size'])
+    spec = codegen.LoopSpec(loop.kernel.name, loop.kernel.code, extents, specs,
+                            [(d.ctype, bool(d.soa)) for d in dats], [m.dim for m in maps],
+                            [m.ctype for m in mats],
+                            [(g.ctype, g.cdim, s.access) for g, s in
+                             zip(gbls, [s for s in specs if s.kind == "gbl"])],
+                            consts, indirect,
+                            [(st[0], st[1], st[2], st[3], tuple(st[4])) for st in stages],
+                            bs, bool(cfg.cfg['fmad'] if fmad is None else fmad))
+    gspecs = [s for s in specs if s.kind == "gbl"]
+    return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
+                gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
+                iterset=iterset, block_size=bs)
+
+
+class _BoundLoop(object):
+    """Everything about a par_loop that does not change between calls with
+    the same objects: generated stub, plan, parameter block."""
+
+    def __init__(self, loop):
+        info = loop_spec(loop)
+        spec = info['spec']
+        specs = info['specs']
+        dats, maps, mats, gbls = info['dats'], info['maps'], info['mats'], info['gbls']
+        stages, races, indirect = info['stages'], info['races'], info['indirect']
+        iterset = info['iterset']
+        args = loop.args
+        self.spec = spec
+        self.module = _get_module(spec)
+        self.layout = self.module.layout
+        self.indirect = indirect
+        self.iterset = iterset
+        self.dats, self.maps, self.mats = dats, maps, mats
+        self.gbl_specs = [s for s in specs if s.kind == "gbl"]
+        self.dat_access = {}
+        for a, s in zip(args, specs):
+            if a._is_dat:
+                self.dat_access.setdefault(id(a.data), []).append(s.access)
+        self.refs = [weakref.ref(o) for o in dats + maps + mats]
+        self.consts = base.Const._definitions()
+        self.block_size = info['block_size']
+        bs = self.block_size
+        # plan
+        self.plan = None
+        if indirect:
+            ps = int(cfg.cfg['partition_size']) or self._default_part_size(stages)
+            pkey = (iterset.size, ps,
+                    tuple((id(maps[st[1]]), tuple(st[4])) for st in stages),
+                    tuple((tuple((id(m), ix) for m, ix in ents), size) for ents, size in races))
+            plan = _PLAN_CACHE.get(pkey)
+            if plan is None:
+                plan = DevicePlan(iterset.size, ps,
+                                  [(maps[st[1]], st[4], np.dtype(dats[st[0]].dtype).itemsize * st[3])
+                                   for st in stages],
+                                  [(ents, size) for ents, size in races],
+                                  staging=True, thread_coloring=True)
+                plan._keep = [m for m in maps]
+                _PLAN_CACHE[pkey] = plan
+            self.plan = plan
+            self.smem = plan.nshared
+            if self.smem > _state['smem_optin']:
+                raise DeviceError("par_loop %s needs %d bytes of shared memory per block; "
+                                  "lower partition_size" % (loop.kernel.name, self.smem))
+            self.module.ensure_smem(self.smem)
+        # static parameter values
+        vals = {}
+        if indirect:
+            p = self.plan.dptr
+            vals.update(blkmap=p["blkmap"], offset=p["offset"], nelems=p["nelems"],
+                        nthrcol=p["nthrcol"], thrcol=p["thrcol"], ind_map=p["ind_map"],
+                        ind_sizes=p["ind_sizes"], ind_offs=p["ind_offs"], loc_map=p["loc_map"])
+        for k, m in enumerate(maps):
+            vals["m%d" % k] = m._to_device().ptr
+        for j, m in enumerate(mats):
+            vals["mv%d" % j] = m._device_values().ptr
+            vals["mr%d" % j] = m.sparsity._d_rowptr
+            vals["mc%d" % j] = m.sparsity._d_colidx
+        vals["err"] = _state['err'].ptr
+        self.vals = vals
+        n = iterset.size
+        if indirect:
+            self.grid = 0
+            self.max_grid = self.plan.max_blocks_per_color
+        else:
+            self.grid = max(1, min((n + bs - 1) // bs, _state['sm_count'] * 8)) if n else 0
+            self.max_grid = self.grid
+
+    @staticmethod
+    def _default_part_size(stages):
+        return 512
+
+    def matches(self, loop):
+        objs = []
+        for a in loop.args:
+            if a._is_dat:
+                objs.append(a.data)
+        return all(r() is not None for r in self.refs)
+
+    def run(self, loop):
+        vals = self.vals
+        for j, d in enumerate(self.dats):
+            modes = self.dat_access[id(d)]
+            d._allocate_device()
+            if d._state is HOST:
+                d._to_device()
+            vals["d%d" % j] = d._device.ptr
+            if d.soa:
+                vals["ds%d" % j] = d.dataset.total_size
+            maybe_setflags(d._data, write=False)
+        for j, s in enumerate(self.gbl_specs):
+            g = loop.args[[k for k, a in enumerate(loop.args) if a._is_global][j]].data
+            g._to_device()
+            vals["g%d" % j] = g._device.ptr
+            if s.access != "READ":
+                pp, cc = g._reduction_buffers(self.max_grid)
+                vals["gp%d" % j] = pp
+                vals["gc%d" % j] = cc
+        mod = self.module
+        for c in self.consts:
+            if mod.const_versions.get(c.name) != (id(c), c._version):
+                ptr, nbytes = mod.const_ptr(c.name)
+                arr = np.ascontiguousarray(c._data)
+                if arr.nbytes != nbytes:
+                    raise RuntimeError("Const %s needs %d bytes, but only space for %d" %
+                                       (c.name, arr.nbytes, nbytes))
+                call("op2b_memcpy_h2d", ptr, arr.ctypes.data, arr.nbytes, 0)
+                mod.const_versions[c.name] = (id(c), c._version)
+        n = self.iterset.size
+        if n == 0:
+            return
+        params = C.create_string_buffer(self.layout.pack(n, 0, n, vals), self.layout.nbytes)
+        if self.indirect:
+            plan = self.plan
+            call("op2b_launch_colored", mod.fn, plan.ncolors, plan.ncolblk_host, self.block_size,
+                 self.smem, 0, params, self.layout.nbytes, codegen.ParamLayout.COL_OFFSET)
+        else:
+            call("op2b_launch", mod.fn, self.grid, self.block_size, 0, 0, params, self.layout.nbytes)
+        for j, d in enumerate(self.dats):
+            if any(m != "READ" for m in self.dat_access[id(d)]):
+                d._state = DEVICE
+        for j, s in enumerate(self.gbl_specs):
+            if s.access != "READ":
+                g = loop.args[[k for k, a in enumerate(loop.args) if a._is_global][j]].data
+                g._state = DEVICE
+        for m in self.mats:
+            m._state = DEVICE
+
+
+class ParLoop(base.ParLoop):
+
+    _bound_cache = {}
+
+    def _bound_key(self):
+        k = [self.kernel.cache_key, id(self.it_space.iterset), self.it_space.extents]
+        for a in self.args:
+            if a._is_global:
+                k.append(("g", a.data.dtype.str, a.data.cdim, a.access._mode))
+            elif a._is_mat:
+                k.append(("m", id(a.data), id(a.map[0]), id(a.map[1]), a.idx[0].index,
+                          a.idx[1].index, a.access._mode))
+            else:
+                ix = a.idx.index if isinstance(a.idx, IterationIndex) else a.idx
+                k.append(("d", id(a.data), id(a.map), isinstance(a.idx, IterationIndex), ix,
+                          a.access._mode))
+        k.append(tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()))
+        k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad']))
+        return tuple(k)
+
+    def compute(self):
+        key = self._bound_key()
+        bl = ParLoop._bound_cache.get(key)
+        if bl is None or not bl.matches(self):
+            bl = _BoundLoop(self)
+            ParLoop._bound_cache[key] = bl
+        bl.run(self)
+        self.maybe_set_halo_update_needed()
+
+
+def par_loop(kernel, it_space, *args):
+    """Run a parallel loop on the device (asynchronous; results are fetched
+    when the host reads them)."""
+    ParLoop(kernel, it_space, *args).compute()
+
+
+class _SingleRank(object):
+    rank = 0
+    size = 1
+
+
+class _MPIConfig(object):
+    comm = _SingleRank()
+    parallel = False
+
+
+MPI = _MPIConfig()

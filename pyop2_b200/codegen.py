@@ -1,0 +1,485 @@
+"""CUDA source generation for par_loop stubs (compiled by NVRTC for sm_100a).
+
+One stub is generated per loop signature.  Its single parameter is a struct
+(``op2b_params``) of 8-byte fields, packed by the host (:class:`ParamLayout`).
+
+Direct loops (no Map, no Mat) run a grid-stride loop, one thread per element.
+Indirect loops run one CTA per plan block of the current block colour; the
+host launches the colours in order (pyop2/cuda.py:757-800 did the same with a
+synchronise per colour).  Per element the stub:
+
+* loads READ / RW / INC(direct) rows into registers with vector loads and
+  gathers READ rows through the Map (pyop2/host.py:91-134 gave the kernel
+  pointers into the global arrays; the kernel now sees register copies);
+* passes WRITE / RW indirect rows and direct WRITE rows as global pointers;
+* gives INC indirect args zeroed register rows, and after the kernel adds them
+  into shared memory at the plan's block-local slot (``loc_map``), one thread
+  colour at a time, then adds each shared row once into the Dat
+  (cuda_indirect_loop.jinja2:105-210 did this with a staged gather of every
+  indirect Dat);
+* for a Mat arg builds the local tensor the sequential wrapper builds
+  (pyop2/sequential.py:62-70, host.py:145-207) and adds it into the CSR values
+  at the positions found by binary search in the row, in the thread-colour
+  section (the plan colours the Mat's row Map), so no atomics are needed;
+* keeps Global reductions in registers and reduces them deterministically on
+  the device (op2b_device.cuh: op2b_reduce).
+"""
+
+import os
+import struct
+
+_DEVICE_HEADER = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "device",
+                              "op2b_device.cuh")
+
+_ACC_CODE = {"READ": 0, "WRITE": 1, "RW": 2, "INC": 3, "MIN": 4, "MAX": 5}
+_RED_OP = {"INC": 0, "MIN": 1, "MAX": 2}
+
+
+def device_header():
+    with open(_DEVICE_HEADER) as f:
+        return f.read()
+
+
+class ArgSpec(object):
+    """Static description of one actual par_loop argument.
+
+    kind: 'gbl' | 'direct' | 'ind' | 'vec' | 'its' | 'mat'
+    slot: unique Dat / Global / Mat slot;  mslot: unique Map slot (rmap for a Mat)
+    cmslot: column Map slot of a Mat;  idx: Map index ('ind') or iteration
+    space index ('its');  arity / carity: Map arities;  ext: extent of the
+    iteration index;  rm, cm: Mat block dims;  soa: SoA Dat;
+    loc_rows: plan loc_map rows of an INC arg (one per unwound Map index);
+    stage: plan staging pair of an INC arg."""
+
+    __slots__ = ("kind", "access", "ctype", "cdim", "slot", "mslot", "cmslot", "idx", "cidx",
+                 "arity", "carity", "ext", "cext", "rm", "cm", "soa", "loc_rows", "stage",
+                 "ro")
+
+    def __init__(self, **kw):
+        for k in self.__slots__:
+            setattr(self, k, kw.get(k))
+
+    def key(self):
+        return tuple(tuple(v) if isinstance(v, list) else v
+                     for v in (getattr(self, k) for k in self.__slots__))
+
+
+class LoopSpec(object):
+    """Everything the generator needs about one loop."""
+
+    def __init__(self, kernel_name, kernel_code, extents, args, dats, maps, mats, gbls,
+                 consts, indirect, stages, block_size, fmad):
+        self.kernel_name = kernel_name
+        self.kernel_code = kernel_code
+        self.extents = tuple(extents)
+        self.args = args              # [ArgSpec]
+        self.dats = dats              # [(ctype, soa)] per unique Dat slot
+        self.maps = maps              # [arity] per unique Map slot
+        self.mats = mats              # [ctype] per Mat slot
+        self.gbls = gbls              # [(ctype, cdim, access)] per Global slot
+        self.consts = consts          # [(name, ctype, cdim)]
+        self.indirect = indirect
+        self.stages = stages          # [(dat slot, map slot, ctype, cdim, [idx...])] INC pairs
+        self.block_size = block_size
+        self.fmad = fmad
+
+    def key(self):
+        return (self.kernel_name, self.kernel_code, self.extents,
+                tuple(a.key() for a in self.args), tuple(self.dats), tuple(self.maps),
+                tuple(self.mats), tuple(self.gbls), tuple(self.consts), self.indirect,
+                tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
+                self.block_size, self.fmad)
+
+    @property
+    def needs_coloring(self):
+        return any(a.kind == "mat" or (a.kind in ("ind", "vec", "its") and a.access == "INC")
+                   for a in self.args)
+
+
+class ParamLayout(object):
+    """Field order of op2b_params.  The header is (set_size i64, col_first i32,
+    col_n i32, start i64, end i64); every other field is 8 bytes."""
+
+    HEADER = "<qiiqq"
+    COL_OFFSET = 8
+
+    def __init__(self, spec):
+        f = []
+        if spec.indirect:
+            f += ["blkmap", "offset", "nelems", "nthrcol", "thrcol", "ind_map", "ind_sizes",
+                  "ind_offs", "loc_map"]
+        for j in range(len(spec.dats)):
+            f.append("d%d" % j)
+            if spec.dats[j][1]:
+                f.append("ds%d" % j)
+        for k in range(len(spec.maps)):
+            f.append("m%d" % k)
+        for j in range(len(spec.mats)):
+            f += ["mv%d" % j, "mr%d" % j, "mc%d" % j]
+        for j, g in enumerate(spec.gbls):
+            f.append("g%d" % j)
+            if g[2] != "READ":
+                f += ["gp%d" % j, "gc%d" % j]
+        f.append("err")
+        self.fields = f
+        self.index = {n: i for i, n in enumerate(f)}
+        self.fmt = self.HEADER + "Q" * len(f)
+        self.nbytes = struct.calcsize(self.fmt)
+
+    def pack(self, set_size, start, end, values):
+        return struct.pack(self.fmt, set_size, 0, 0, start, end,
+                           *[int(values.get(n, 0)) for n in self.fields])
+
+
+def _struct_decl(spec, layout):
+    lines = ["struct op2b_params {", "  op2b_i64 set_size;", "  int col_first, col_n;",
+             "  op2b_i64 start, end;"]
+    types = {"blkmap": "const int *", "offset": "const int *", "nelems": "const int *",
+             "nthrcol": "const int *", "thrcol": "const int *", "ind_map": "const int *",
+             "ind_sizes": "const int *", "ind_offs": "const int *", "loc_map": "const short *",
+             "err": "int *"}
+    for n in layout.fields:
+        if n in types:
+            t = types[n]
+        elif n.startswith("ds"):
+            t = "op2b_i64 "
+        elif n.startswith("d"):
+            t = "%s *" % spec.dats[int(n[1:])][0]
+        elif n.startswith("mv"):
+            t = "%s *" % spec.mats[int(n[2:])]
+        elif n.startswith("mr") or n.startswith("mc") or n.startswith("m"):
+            t = "const int *"
+        elif n.startswith("gp"):
+            t = "%s *" % spec.gbls[int(n[2:])][0]
+        elif n.startswith("gc"):
+            t = "unsigned *"
+        elif n.startswith("g"):
+            t = "%s *" % spec.gbls[int(n[1:])][0]
+        else:
+            raise AssertionError(n)
+        lines.append("  %s%s;" % (t, n))
+    lines.append("};")
+    return "\n".join(lines)
+
+
+def _kernel_source(spec):
+    """User kernel as a device function.  Every function of the user code is
+    compiled for the device (NVRTC -default-device) and the entry is forced
+    inline so its pointer arguments resolve to the stub's registers."""
+    code = spec.kernel_code
+    return ("#define OP2_STRIDE(a, idx) (a)[idx]\n"
+            "__forceinline__\n" + _mark_inline(code, spec.kernel_name) + "\n#undef OP2_STRIDE\n")
+
+
+def _mark_inline(code, name):
+    import re
+    pat = re.compile(r"(^|[;}\s])((?:static\s+|inline\s+)*void\s+%s\s*\()" % re.escape(name))
+    m = pat.search(code)
+    if not m:
+        return code
+    return code[:m.start(2)] + "__forceinline__ " + code[m.start(2):]
+
+
+def generate(spec):
+    """Return (source, ParamLayout, stub name) for a LoopSpec."""
+    layout = ParamLayout(spec)
+    out = []
+    w = out.append
+    w(device_header())
+    for name, ctype, cdim in spec.consts:
+        if cdim == 1:
+            w("__constant__ %s %s;" % (ctype, name))
+        else:
+            w("__constant__ %s %s[%d];" % (ctype, name, cdim))
+    w(_struct_decl(spec, layout))
+    w("#define OP2_STRIDE(a, idx) (a)[idx]")
+    w(_mark_inline(spec.kernel_code, spec.kernel_name))
+    w("#undef OP2_STRIDE")
+    body = _indirect_body(spec) if spec.indirect else _direct_body(spec)
+    w(body)
+    return "\n".join(out), layout, "op2b_stub"
+
+
+# ------------------------------------------------------------------ helpers
+def _ro(a):
+    return "true" if a.ro else "false"
+
+
+def _gbl_prologue(spec, lines):
+    for n, a in enumerate(spec.args):
+        if a.kind != "gbl":
+            continue
+        t, c = a.ctype, a.cdim
+        if a.access == "READ":
+            lines.append("  %s g%d_l[%d];" % (t, n, c))
+            lines.append("  for (int k = 0; k < %d; ++k) g%d_l[k] = p.g%d[k];" % (c, n, a.slot))
+        else:
+            lines.append("  %s r%d[%d];" % (t, n, c))
+            if a.access == "INC":
+                lines.append("  op2b_zero(r%d);" % n)
+            else:
+                lines.append("  for (int k = 0; k < %d; ++k) r%d[k] = p.g%d[k];" % (c, n, a.slot))
+
+
+def _gbl_epilogue(spec, lines):
+    for n, a in enumerate(spec.args):
+        if a.kind == "gbl" and a.access != "READ":
+            lines.append("  op2b_reduce<%d, %s, %d>(r%d, p.g%d, p.gp%d, p.gc%d);" %
+                         (_RED_OP[a.access], a.ctype, a.cdim, n, a.slot, a.slot, a.slot))
+
+
+def _direct_row(a, n, e, lines_pre, lines_post, indent):
+    """Code for a direct Dat arg of element e; returns the kernel argument."""
+    t, c, j = a.ctype, a.cdim, a.slot
+    if a.soa:
+        lines_pre.append("%s__align__(16) %s a%d[%d];" % (indent, t, n, c))
+        if a.access != "WRITE" or True:
+            lines_pre.append("%sop2b_load_soa(a%d, p.d%d, %s, p.ds%d);" % (indent, n, j, e, j))
+        if a.access != "READ":
+            lines_post.append("%sop2b_store_soa(p.d%d, %s, p.ds%d, a%d);" % (indent, j, e, j, n))
+        return "a%d" % n
+    if a.access == "WRITE":
+        return "p.d%d + (op2b_i64)(%s) * %d" % (j, e, c)
+    lines_pre.append("%s__align__(16) %s a%d[%d];" % (indent, t, n, c))
+    lines_pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + (op2b_i64)(%s) * %d);" %
+                     (indent, t, c, _ro(a), n, j, e, c))
+    if a.access != "READ":
+        lines_post.append("%sop2b_store(p.d%d + (op2b_i64)(%s) * %d, a%d);" % (indent, j, e, c, n))
+    return "a%d" % n
+
+
+def _kernel_call(spec, argexprs, indent):
+    itargs = ["i%d" % k for k in range(len(spec.extents))]
+    return "%s%s(%s);" % (indent, spec.kernel_name, ", ".join(argexprs + itargs))
+
+
+def _direct_body(spec):
+    bs = spec.block_size
+    L = ["extern \"C\" __global__ void __launch_bounds__(%d) op2b_stub(const op2b_params p) {" % bs]
+    _gbl_prologue(spec, L)
+    L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
+             " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
+    pre, post, exprs = [], [], []
+    for n, a in enumerate(spec.args):
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
+        else:
+            exprs.append(_direct_row(a, n, "e", pre, post, "    "))
+    L += pre
+    L += _itspace_open(spec, "    ")
+    L.append(_kernel_call(spec, exprs, "    " + "  " * len(spec.extents)))
+    L += _itspace_close(spec, "    ")
+    L += post
+    L.append("  }")
+    _gbl_epilogue(spec, L)
+    L.append("}")
+    return "\n".join(L)
+
+
+def _itspace_open(spec, indent):
+    out = []
+    for k, ext in enumerate(spec.extents):
+        out.append("%s#pragma unroll" % (indent + "  " * k))
+        out.append("%sfor (int i%d = 0; i%d < %d; ++i%d) {" % (indent + "  " * k, k, k, ext, k))
+    return out
+
+
+def _itspace_close(spec, indent):
+    return ["%s}" % (indent + "  " * k) for k in range(len(spec.extents) - 1, -1, -1)]
+
+
+def _indirect_body(spec):
+    bs = spec.block_size
+    ninds = len(spec.stages)
+    coloured = spec.needs_coloring
+    L = ["extern \"C\" __global__ void __launch_bounds__(%d) op2b_stub(const op2b_params p) {" % bs]
+    L.append("  if ((int)blockIdx.x >= p.col_n) return;")
+    L.append("  const int blk = p.blkmap[p.col_first + blockIdx.x];")
+    L.append("  const int start = p.offset[blk];")
+    L.append("  const int nelem = p.nelems[blk];")
+    L.append("  const op2b_i64 set_size = p.set_size;")
+    if ninds:
+        L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
+        L.append("  int smem_off = 0;")
+        nidx_prefix = 0
+        for s, (dslot, mslot, t, c, idxs) in enumerate(spec.stages):
+            L.append("  const int n_s%d = p.ind_sizes[blk * %d + %d];" % (s, ninds, s))
+            L.append("  %s *inc_s%d = (%s *)(op2b_smem + smem_off);" % (t, s, t))
+            L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (s, c, t))
+            L.append("  const int *ind_s%d = p.ind_map + (op2b_i64)%d * set_size + p.ind_offs[blk * %d + %d];"
+                     % (s, nidx_prefix, ninds, s))
+            L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) inc_s%d[t] = (%s)0;"
+                     % (s, c, bs, s, t))
+            nidx_prefix += len(idxs)
+        L.append("  __syncthreads();")
+    _gbl_prologue(spec, L)
+    if coloured:
+        L.append("  const int ncol = p.nthrcol[blk];")
+    L.append("  for (int base = 0; base < nelem; base += %d) {" % bs)
+    L.append("    const int idx = base + threadIdx.x;")
+    L.append("    const bool active = idx < nelem;")
+    L.append("    const int e = start + idx;")
+    ind = "    "
+    # map rows (needed by the kernel call and by the colour section)
+    used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
+                       {a.cmslot for a in spec.args if a.kind == "mat"})
+    for k in used_maps:
+        ar = spec.maps[k]
+        L.append("%s__align__(16) int mr%d[%d];" % (ind, k, ar))
+        L.append("%sif (active) op2b_load<int, %d, true>(mr%d, p.m%d + (op2b_i64)e * %d);"
+                 " else { for (int q = 0; q < %d; ++q) mr%d[q] = 0; }" % (ind, ar, k, k, ar, ar, k))
+    # INC locals and Mat local tensors live across the colour section
+    decl, pre, post, exprs = [], [], [], []
+    for n, a in enumerate(spec.args):
+        t, c = a.ctype, a.cdim
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
+        elif a.kind == "direct":
+            exprs.append(_direct_row(a, n, "e", pre, post, ind + "  "))
+        elif a.kind == "ind":
+            row = "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, a.idx, c)
+            if a.access == "INC":
+                decl.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind, t, n, c, n))
+                exprs.append("a%d" % n)
+            elif a.access == "READ":
+                pre.append("%s  __align__(16) %s a%d[%d];" % (ind, t, n, c))
+                pre.append("%s  op2b_load<%s, %d, %s>(a%d, %s);" % (ind, t, c, _ro(a), n, row))
+                exprs.append("a%d" % n)
+            else:
+                exprs.append(row)
+        elif a.kind in ("vec", "its"):
+            cnt = a.arity if a.kind == "vec" else a.ext
+            var = "i%d" % a.idx if a.kind == "its" else None
+            if a.access in ("READ", "INC"):
+                if a.access == "INC":
+                    decl.append("%s__align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
+                    decl.append("%sfor (int q = 0; q < %d; ++q) op2b_zero(a%d[q]);" % (ind, cnt, n))
+                else:
+                    pre.append("%s  __align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
+                    for r in range(cnt):
+                        pre.append("%s  op2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                                   % (ind, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
+                if a.kind == "vec":
+                    pre.append("%s  %s *a%d_v[%d] = {%s};" %
+                               (ind, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
+                    exprs.append("a%d_v" % n)
+                else:
+                    exprs.append("a%d[%s]" % (n, var))
+            else:
+                if a.kind == "vec":
+                    pre.append("%s  %s *a%d_v[%d] = {%s};" % (
+                        ind, t, n, cnt, ", ".join("p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, r, c)
+                                                   for r in range(cnt))))
+                    exprs.append("a%d_v" % n)
+                else:
+                    exprs.append("p.d%d + (op2b_i64)mr%d[%s] * %d" % (a.slot, a.mslot, var, c))
+        elif a.kind == "mat":
+            e0, e1 = spec.extents[0], spec.extents[1]
+            if a.rm * a.cm == 1:
+                decl.append("%s%s A%d[%d][%d];" % (ind, t, n, e0, e1))
+                exprs.append("(%s (*)[1])&A%d[i0][i1]" % (t, n))
+            else:
+                decl.append("%s%s A%d[%d][%d][%d][%d];" % (ind, t, n, e0, e1, a.rm, a.cm))
+                exprs.append("A%d[i0][i1]" % n)
+    L += decl
+    if coloured:
+        L.append("%sint col = -1;" % ind)
+    L.append("%sif (active) {" % ind)
+    L += pre
+    L += _itspace_open(spec, ind + "  ")
+    deep = ind + "  " + "  " * len(spec.extents)
+    for n, a in enumerate(spec.args):
+        if a.kind == "mat":
+            if a.rm * a.cm == 1:
+                L.append("%sA%d[i0][i1] = (%s)0;" % (deep, n, a.ctype))
+            else:
+                L.append("%sfor (int r = 0; r < %d; ++r) for (int c = 0; c < %d; ++c) A%d[i0][i1][r][c] = (%s)0;"
+                         % (deep, a.rm, a.cm, n, a.ctype))
+    L.append(_kernel_call(spec, exprs, deep))
+    L += _itspace_close(spec, ind + "  ")
+    L += post
+    if coloured:
+        L.append("%s  col = p.thrcol[e];" % ind)
+    L.append("%s}" % ind)
+    if coloured:
+        L.append("%sfor (int c = 0; c < ncol; ++c) {" % ind)
+        L.append("%s  if (col == c) {" % ind)
+        cs = ind + "    "
+        for n, a in enumerate(spec.args):
+            if a.kind in ("ind", "vec", "its") and a.access == "INC":
+                s = a.stage
+                c_ = a.cdim
+                if a.kind == "ind":
+                    rows = [("a%d" % n, a.loc_rows[0])]
+                else:
+                    cnt = a.arity if a.kind == "vec" else a.ext
+                    rows = [("a%d[%d]" % (n, r), a.loc_rows[r]) for r in range(cnt)]
+                for var, lr in rows:
+                    L.append("%s{ const int l = p.loc_map[(op2b_i64)%d * set_size + e];" % (cs, lr))
+                    L.append("%s  for (int k = 0; k < %d; ++k) inc_s%d[l * %d + k] += %s[k]; }"
+                             % (cs, c_, s, c_, var))
+            elif a.kind == "mat":
+                L += _mat_addto(spec, n, a, cs)
+        L.append("%s  }" % ind)
+        L.append("%s  __syncthreads();" % ind)
+        L.append("%s}" % ind)
+    L.append("  }")
+    # add the block's INC rows into the Dats; pairs of the same Dat in turn
+    if ninds:
+        L.append("  __syncthreads();")
+        seen_dats = set()
+        for s, (dslot, mslot, t, c, idxs) in enumerate(spec.stages):
+            if dslot in seen_dats:
+                L.append("  __syncthreads();")
+            seen_dats.add(dslot)
+            L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (s, c, bs))
+            L.append("    const int r = t / %d, k = t - r * %d;" % (c, c))
+            L.append("    p.d%d[(op2b_i64)ind_s%d[r] * %d + k] += inc_s%d[t];" % (dslot, s, c, s))
+            L.append("  }")
+    _gbl_epilogue(spec, L)
+    L.append("}")
+    return "\n".join(L)
+
+
+def _mat_addto(spec, n, a, ind):
+    """Add / insert the local tensor of Mat arg n into the CSR values
+    (pyop2/host.py:145-184: scalar fields add the whole block, vector fields
+    add entry by entry and skip zero values when adding)."""
+    e0, e1 = spec.extents[0], spec.extents[1]
+    j = a.slot
+    ins = a.access == "WRITE"
+    L = []
+    L.append("%sfor (int i0 = 0; i0 < %d; ++i0) for (int i1 = 0; i1 < %d; ++i1) {" % (ind, e0, e1))
+    ri = "i%d" % a.idx
+    ci = "i%d" % a.cidx
+    if a.rm * a.cm == 1:
+        L.append("%s  const int row = mr%d[%s], colj = mr%d[%s];" % (ind, a.mslot, ri, a.cmslot, ci))
+        L.append("%s  const int pos = op2b_csr_find(p.mr%d, p.mc%d, row, colj);" % (ind, j, j))
+        L.append("%s  if (pos < 0) op2b_flag_missing(p.err, row, colj);" % ind)
+        if ins:
+            L.append("%s  else p.mv%d[pos] = A%d[i0][i1];" % (ind, j, n))
+        else:
+            L.append("%s  else p.mv%d[pos] += A%d[i0][i1];" % (ind, j, n))
+    else:
+        L.append("%s  for (int r = 0; r < %d; ++r) for (int c = 0; c < %d; ++c) {" % (ind, a.rm, a.cm))
+        L.append("%s    const %s v = A%d[i0][i1][r][c];" % (ind, a.ctype, n))
+        if not ins:
+            L.append("%s    if (v == (%s)0) continue;" % (ind, a.ctype))
+        L.append("%s    const int row = %d * mr%d[%s] + r, colj = %d * mr%d[%s] + c;"
+                 % (ind, a.rm, a.mslot, ri, a.cm, a.cmslot, ci))
+        L.append("%s    const int pos = op2b_csr_find(p.mr%d, p.mc%d, row, colj);" % (ind, j, j))
+        L.append("%s    if (pos < 0) op2b_flag_missing(p.err, row, colj);" % ind)
+        if ins:
+            L.append("%s    else p.mv%d[pos] = v;" % (ind, j))
+        else:
+            L.append("%s    else p.mv%d[pos] += v;" % (ind, j))
+        L.append("%s  }" % ind)
+    L.append("%s}" % ind)
+    return L
+
+
+def nvrtc_options(fmad=False, extra=()):
+    opts = ["--gpu-architecture=sm_100a", "-default-device", "--std=c++17", "-lineinfo",
+            "--fmad=%s" % ("true" if fmad else "false"), "-DOP2B_NVRTC=1"]
+    opts += list(extra)
+    return opts

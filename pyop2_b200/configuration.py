@@ -1,0 +1,66 @@
+"""OP2 configuration: a dict of defaults updated by ``op2.init(**kwargs)``.
+
+Same keys as pyop2/assets/default.yaml (backend, debug, log_level) plus the
+keys of the B200 backend:
+
+* ``partition_size``: elements per plan block of indirect loops (default 0:
+  chosen per loop by the backend);
+* ``block_size``: threads per CTA of the generated stubs;
+* ``fmad``: allow fused multiply-add contraction in JIT-compiled kernels
+  (default False: every FP operation is rounded separately, like the host
+  compiler on x86-64, so direct loops reproduce host results bit for bit);
+* ``cache_dir``: directory of the on-disk cubin cache;
+* ``validate_maps``: check Map values against their target Set on upload.
+"""
+
+import os
+
+_defaults = {
+    'backend': 'b200',
+    'debug': 0,
+    'log_level': 'WARN',
+    'python_plan': True,
+    'partition_size': 0,
+    'block_size': 256,
+    'fmad': False,
+    'cache_dir': os.environ.get('OP2B_CACHE_DIR',
+                                os.path.join('/tmp', 'op2b200-cache-%d' % os.getuid())),
+    'validate_maps': True,
+    'device': 0,
+}
+
+_config = dict(_defaults)
+
+
+def configure(**kwargs):
+    for k, v in kwargs.items():
+        if k == 'log_level' and v is None:
+            continue
+        _config[k] = v
+
+
+def reset():
+    _config.clear()
+    _config.update(_defaults)
+
+
+def __getitem__(key):  # pragma: no cover - module-level item access shim
+    return _config[key]
+
+
+def get(key, default=None):
+    return _config.get(key, default)
+
+
+class _ConfigView(object):
+    def __getitem__(self, key):
+        return _config[key]
+
+    def __getattr__(self, key):
+        try:
+            return _config[key]
+        except KeyError:
+            raise AttributeError(key)
+
+
+cfg = _ConfigView()

@@ -1,0 +1,176 @@
+// Device helpers prepended to every JIT-compiled par_loop stub (NVRTC, sm_100a).
+//
+//  * op2b_load / op2b_store: move one Dat row of N elements of T between
+//    global memory and a register array with the widest aligned vector access
+//    (16-byte when the row size is a multiple of 16, then 8, then 4 bytes).
+//    The register arrays are declared __align__(16) by the generated stubs.
+//    Dat rows start at base + i * N * sizeof(T) with a 256-byte aligned base,
+//    so a row whose size is a multiple of 16 (8) bytes is 16 (8) byte aligned.
+//  * op2b_csr_find: position of (row, col) in a CSR pattern (binary search in
+//    the sorted colidx of the row), -1 if the pattern does not store it.
+//  * op2b_reduce: deterministic Global reduction (INC / MIN / MAX) of one
+//    register value per thread: warp shuffles, one partial per CTA, and the
+//    last CTA to finish folds the partials in CTA order into the Global.
+#pragma once
+
+typedef signed char op2b_i8;
+typedef unsigned char op2b_u8;
+typedef long long op2b_i64;
+typedef unsigned long long op2b_u64;
+
+#define OP2B_FULL_MASK 0xffffffffu
+
+template <typename T, int N, bool RO>
+__device__ __forceinline__ void op2b_load(T (&dst)[N], const T *__restrict__ src) {
+  constexpr int B = N * (int)sizeof(T);
+  if constexpr (B % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < B / 16; ++i) {
+      uint4 v = RO ? __ldg(reinterpret_cast<const uint4 *>(src) + i)
+                   : reinterpret_cast<const uint4 *>(src)[i];
+      reinterpret_cast<uint4 *>(dst)[i] = v;
+    }
+  } else if constexpr (B % 8 == 0) {
+#pragma unroll
+    for (int i = 0; i < B / 8; ++i) {
+      uint2 v = RO ? __ldg(reinterpret_cast<const uint2 *>(src) + i)
+                   : reinterpret_cast<const uint2 *>(src)[i];
+      reinterpret_cast<uint2 *>(dst)[i] = v;
+    }
+  } else if constexpr (B % 4 == 0 && sizeof(T) >= 4) {
+#pragma unroll
+    for (int i = 0; i < B / 4; ++i) {
+      unsigned v = RO ? __ldg(reinterpret_cast<const unsigned *>(src) + i)
+                      : reinterpret_cast<const unsigned *>(src)[i];
+      reinterpret_cast<unsigned *>(dst)[i] = v;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) dst[i] = src[i];
+  }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void op2b_store(T *__restrict__ dst, const T (&src)[N]) {
+  constexpr int B = N * (int)sizeof(T);
+  if constexpr (B % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < B / 16; ++i) {
+      reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+    }
+  } else if constexpr (B % 8 == 0) {
+#pragma unroll
+    for (int i = 0; i < B / 8; ++i) {
+      reinterpret_cast<uint2 *>(dst)[i] = reinterpret_cast<const uint2 *>(src)[i];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) dst[i] = src[i];
+  }
+}
+
+// SoA row: component k of element e lives at base[k * stride + e].
+template <typename T, int N>
+__device__ __forceinline__ void op2b_load_soa(T (&dst)[N], const T *__restrict__ base, op2b_i64 e,
+                                              op2b_i64 stride) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) dst[k] = base[k * stride + e];
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void op2b_store_soa(T *__restrict__ base, op2b_i64 e, op2b_i64 stride,
+                                               const T (&src)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) base[k * stride + e] = src[k];
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void op2b_zero(T (&a)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) a[k] = T(0);
+}
+
+__device__ __forceinline__ int op2b_csr_find(const int *__restrict__ rowptr,
+                                             const int *__restrict__ colidx, int row, int col) {
+  int lo = rowptr[row], hi = rowptr[row + 1];
+  const int end = hi;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (colidx[mid] < col)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < end && colidx[lo] == col) ? lo : -1;
+}
+
+// Record the first Mat insertion outside the Sparsity (PETSc raises
+// NEW_NONZERO_ALLOCATION_ERR there); err[1..2] = offending (row, col).
+__device__ __forceinline__ void op2b_flag_missing(int *err, int row, int col) {
+  if (atomicCAS(err, 0, 1) == 0) {
+    err[1] = row;
+    err[2] = col;
+  }
+}
+
+// ------------------------------------------------------------- reductions
+template <int OP, typename T>
+__device__ __forceinline__ T op2b_combine(T a, T b) {
+  if constexpr (OP == 0) return a + b;
+  else if constexpr (OP == 1) return b < a ? b : a;
+  else return b > a ? b : a;
+}
+
+template <int OP, typename T>
+__device__ __forceinline__ T op2b_warp_reduce(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = op2b_combine<OP>(v, __shfl_xor_sync(OP2B_FULL_MASK, v, o));
+  return v;
+}
+
+// Reduce v over the CTA; the result is valid in thread 0.  scratch holds 32 T.
+template <int OP, typename T>
+__device__ __forceinline__ T op2b_block_reduce(T v, T *scratch) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = op2b_warp_reduce<OP>(v);
+  __syncthreads();
+  if (lane == 0) scratch[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    // lanes past the last warp repeat warp 0's value: harmless for MIN/MAX,
+    // replaced by zero for sums.
+    T t = scratch[lane < nw ? lane : 0];
+    if (OP == 0 && lane >= nw) t = T(0);
+    v = op2b_warp_reduce<OP>(t);
+  }
+  return v;
+}
+
+// OP: 0 = INC (sum), 1 = MIN, 2 = MAX.  gbl: the Global's device value;
+// partials: >= gridDim.x * N values; counter: zero before the launch, reset to
+// zero by the last CTA.
+template <int OP, typename T, int N>
+__device__ __forceinline__ void op2b_reduce(const T (&v)[N], T *gbl, T *partials, unsigned *counter) {
+  __shared__ T red_scratch[32];
+  __shared__ bool red_last;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    T r = op2b_block_reduce<OP>(v[k], red_scratch);
+    if (threadIdx.x == 0) partials[blockIdx.x * N + k] = r;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) red_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!red_last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    T acc = OP == 0 ? T(0) : __ldcg(&partials[k]);
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+      acc = op2b_combine<OP>(acc, __ldcg(&partials[b * N + k]));
+    acc = op2b_block_reduce<OP>(acc, red_scratch);
+    if (threadIdx.x == 0) gbl[k] = op2b_combine<OP>(gbl[k], acc);
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}

@@ -1,0 +1,227 @@
+"""Airfoil-style finite-volume loop chain (the OP2 airfoil demo's loops).
+
+Kernels: the arithmetic of the OP2 airfoil demo (save_soln, adt_calc,
+res_calc, bres_calc, update; loop structure pyop2/demo/airfoil.py:86-131)
+written out for this package.  Constants: gamma 1.4, gamma-1 0.4, CFL 0.9,
+dissipation eps 0.05, free stream rho 1, u 0.5, v 0, p 1.
+
+:func:`build` declares the Sets/Maps/Dats/Consts through any module with the
+op2 API (the B200 backend's ``op2`` or the oracle), and :func:`iteration`
+runs one outer iteration: save_soln, then twice (adt_calc, res_calc,
+bres_calc, update with the rms reduction).
+"""
+
+import numpy as np
+
+from .meshes import airfoil_grid
+
+GAM = 1.4
+GM1 = 0.4
+CFL = 0.9
+EPS = 0.05
+RHO_INF, U_INF, V_INF, P_INF = 1.0, 0.5, 0.0, 1.0
+
+SAVE_SOLN = """
+void save_soln(double *q, double *qold) {
+  for (int k = 0; k < 4; k++) qold[k] = q[k];
+}
+"""
+
+# area / timestep of a cell from its four corners and state
+ADT_CALC = """
+void adt_calc(double *x1, double *x2, double *x3, double *x4, double *q, double *adt) {
+  double rinv = 1.0 / q[0];
+  double u = rinv * q[1];
+  double v = rinv * q[2];
+  double c = sqrt(gam * gm1 * (rinv * q[3] - 0.5 * (u * u + v * v)));
+  double ex, ey;
+  ex = x2[0] - x1[0]; ey = x2[1] - x1[1];
+  *adt = fabs(u * ey - v * ex) + c * sqrt(ex * ex + ey * ey);
+  ex = x3[0] - x2[0]; ey = x3[1] - x2[1];
+  *adt += fabs(u * ey - v * ex) + c * sqrt(ex * ex + ey * ey);
+  ex = x4[0] - x3[0]; ey = x4[1] - x3[1];
+  *adt += fabs(u * ey - v * ex) + c * sqrt(ex * ex + ey * ey);
+  ex = x1[0] - x4[0]; ey = x1[1] - x4[1];
+  *adt += fabs(u * ey - v * ex) + c * sqrt(ex * ex + ey * ey);
+  *adt = (*adt) / cfl;
+}
+"""
+
+# central flux plus scalar dissipation across an interior edge
+RES_CALC = """
+void res_calc(double *x1, double *x2, double *q1, double *q2,
+              double *adt1, double *adt2, double *res1, double *res2) {
+  double ex = x1[0] - x2[0];
+  double ey = x1[1] - x2[1];
+  double r1 = 1.0 / q1[0];
+  double pr1 = gm1 * (q1[3] - 0.5 * r1 * (q1[1] * q1[1] + q1[2] * q1[2]));
+  double vn1 = r1 * (q1[1] * ey - q1[2] * ex);
+  double r2 = 1.0 / q2[0];
+  double pr2 = gm1 * (q2[3] - 0.5 * r2 * (q2[1] * q2[1] + q2[2] * q2[2]));
+  double vn2 = r2 * (q2[1] * ey - q2[2] * ex);
+  double diss = 0.5 * ((*adt1) + (*adt2)) * eps;
+  double fl;
+  fl = 0.5 * (vn1 * q1[0] + vn2 * q2[0]) + diss * (q1[0] - q2[0]);
+  res1[0] += fl; res2[0] -= fl;
+  fl = 0.5 * (vn1 * q1[1] + pr1 * ey + vn2 * q2[1] + pr2 * ey) + diss * (q1[1] - q2[1]);
+  res1[1] += fl; res2[1] -= fl;
+  fl = 0.5 * (vn1 * q1[2] - pr1 * ex + vn2 * q2[2] - pr2 * ex) + diss * (q1[2] - q2[2]);
+  res1[2] += fl; res2[2] -= fl;
+  fl = 0.5 * (vn1 * (q1[3] + pr1) + vn2 * (q2[3] + pr2)) + diss * (q1[3] - q2[3]);
+  res1[3] += fl; res2[3] -= fl;
+}
+"""
+
+# wall (bound == 1: pressure only) or far-field boundary flux
+BRES_CALC = """
+void bres_calc(double *x1, double *x2, double *q1, double *adt1, double *res1, int *bound) {
+  double ex = x1[0] - x2[0];
+  double ey = x1[1] - x2[1];
+  double r1 = 1.0 / q1[0];
+  double pr1 = gm1 * (q1[3] - 0.5 * r1 * (q1[1] * q1[1] + q1[2] * q1[2]));
+  if (*bound == 1) {
+    res1[1] += pr1 * ey;
+    res1[2] += -pr1 * ex;
+  } else {
+    double vn1 = r1 * (q1[1] * ey - q1[2] * ex);
+    double r2 = 1.0 / qinf[0];
+    double pr2 = gm1 * (qinf[3] - 0.5 * r2 * (qinf[1] * qinf[1] + qinf[2] * qinf[2]));
+    double vn2 = r2 * (qinf[1] * ey - qinf[2] * ex);
+    double diss = (*adt1) * eps;
+    double fl;
+    fl = 0.5 * (vn1 * q1[0] + vn2 * qinf[0]) + diss * (q1[0] - qinf[0]);
+    res1[0] += fl;
+    fl = 0.5 * (vn1 * q1[1] + pr1 * ey + vn2 * qinf[1] + pr2 * ey) + diss * (q1[1] - qinf[1]);
+    res1[1] += fl;
+    fl = 0.5 * (vn1 * q1[2] - pr1 * ex + vn2 * qinf[2] - pr2 * ex) + diss * (q1[2] - qinf[2]);
+    res1[2] += fl;
+    fl = 0.5 * (vn1 * (q1[3] + pr1) + vn2 * (qinf[3] + pr2)) + diss * (q1[3] - qinf[3]);
+    res1[3] += fl;
+  }
+}
+"""
+
+# explicit update with the residual; accumulates the squared change
+UPDATE = """
+void update(double *qold, double *q, double *res, double *adt, double *rms) {
+  double ainv = 1.0 / (*adt);
+  for (int k = 0; k < 4; k++) {
+    double dq = ainv * res[k];
+    q[k] = qold[k] - dq;
+    res[k] = 0.0;
+    *rms += dq * dq;
+  }
+}
+"""
+
+
+def freestream():
+    e = P_INF / GM1 + 0.5 * RHO_INF * (U_INF ** 2 + V_INF ** 2)
+    return np.array([RHO_INF, RHO_INF * U_INF, RHO_INF * V_INF, e])
+
+
+def initial_q(ncells, seed=0, noise=0.01):
+    rng = np.random.default_rng(seed + 1)
+    return freestream()[None, :] * (1.0 + rng.uniform(-noise, noise, size=(ncells, 4)))
+
+
+class Airfoil(object):
+    """The op2 objects of one airfoil problem."""
+
+
+def build(op2, nx, ny, seed=0, grid=None, consts=True):
+    """Declare the airfoil problem through ``op2`` (B200 op2 or the oracle)."""
+    g = grid if grid is not None else airfoil_grid(nx, ny, seed)
+    A = Airfoil()
+    A.grid = g
+    A.nodes = op2.Set(g.nnodes, 2, "nodes")
+    A.edges = op2.Set(g.nedges, 1, "edges")
+    A.bedges = op2.Set(g.nbedges, 1, "bedges")
+    A.cells = op2.Set(g.ncells, 1, "cells")
+    A.vcells = op2.Set(g.ncells, 4, "vcells")
+    A.pedge = op2.Map(A.edges, A.nodes, 2, g.pedge, "pedge")
+    A.pecell = op2.Map(A.edges, A.cells, 2, g.pecell, "pecell")
+    A.pevcell = op2.Map(A.edges, A.vcells, 2, g.pecell, "pevcell")
+    A.pbedge = op2.Map(A.bedges, A.nodes, 2, g.pbedge, "pbedge")
+    A.pbecell = op2.Map(A.bedges, A.cells, 1, g.pbecell, "pbecell")
+    A.pbevcell = op2.Map(A.bedges, A.vcells, 1, g.pbecell, "pbevcell")
+    A.pcell = op2.Map(A.cells, A.nodes, 4, g.pcell, "pcell")
+    A.p_bound = op2.Dat(A.bedges, g.p_bound, np.int32, "p_bound")
+    A.p_x = op2.Dat(A.nodes, g.x, np.float64, "p_x")
+    q0 = initial_q(g.ncells, seed)
+    A.p_q = op2.Dat(A.vcells, q0, np.float64, "p_q")
+    A.p_qold = op2.Dat(A.vcells, q0.copy(), np.float64, "p_qold")
+    A.p_adt = op2.Dat(A.cells, np.zeros(g.ncells), np.float64, "p_adt")
+    A.p_res = op2.Dat(A.vcells, np.zeros((g.ncells, 4)), np.float64, "p_res")
+    if consts:
+        A.consts = [op2.Const(1, GAM, "gam", np.float64), op2.Const(1, GM1, "gm1", np.float64),
+                    op2.Const(1, CFL, "cfl", np.float64), op2.Const(1, EPS, "eps", np.float64),
+                    op2.Const(4, freestream(), "qinf", np.float64)]
+    A.k_save = op2.Kernel(SAVE_SOLN, "save_soln")
+    A.k_adt = op2.Kernel(ADT_CALC, "adt_calc")
+    A.k_res = op2.Kernel(RES_CALC, "res_calc")
+    A.k_bres = op2.Kernel(BRES_CALC, "bres_calc")
+    A.k_update = op2.Kernel(UPDATE, "update")
+    return A
+
+
+def save_soln(op2, A):
+    op2.par_loop(A.k_save, A.cells, A.p_q(op2.IdentityMap, op2.READ),
+                 A.p_qold(op2.IdentityMap, op2.WRITE))
+
+
+def adt_calc(op2, A):
+    op2.par_loop(A.k_adt, A.cells,
+                 A.p_x(A.pcell[0], op2.READ), A.p_x(A.pcell[1], op2.READ),
+                 A.p_x(A.pcell[2], op2.READ), A.p_x(A.pcell[3], op2.READ),
+                 A.p_q(op2.IdentityMap, op2.READ), A.p_adt(op2.IdentityMap, op2.WRITE))
+
+
+def res_calc(op2, A):
+    op2.par_loop(A.k_res, A.edges,
+                 A.p_x(A.pedge[0], op2.READ), A.p_x(A.pedge[1], op2.READ),
+                 A.p_q(A.pevcell[0], op2.READ), A.p_q(A.pevcell[1], op2.READ),
+                 A.p_adt(A.pecell[0], op2.READ), A.p_adt(A.pecell[1], op2.READ),
+                 A.p_res(A.pevcell[0], op2.INC), A.p_res(A.pevcell[1], op2.INC))
+
+
+def bres_calc(op2, A):
+    op2.par_loop(A.k_bres, A.bedges,
+                 A.p_x(A.pbedge[0], op2.READ), A.p_x(A.pbedge[1], op2.READ),
+                 A.p_q(A.pbevcell[0], op2.READ), A.p_adt(A.pbecell[0], op2.READ),
+                 A.p_res(A.pbevcell[0], op2.INC), A.p_bound(op2.IdentityMap, op2.READ))
+
+
+def update(op2, A, rms):
+    op2.par_loop(A.k_update, A.cells,
+                 A.p_qold(op2.IdentityMap, op2.READ), A.p_q(op2.IdentityMap, op2.WRITE),
+                 A.p_res(op2.IdentityMap, op2.RW), A.p_adt(op2.IdentityMap, op2.READ),
+                 rms(op2.INC))
+
+
+def iteration(op2, A, rms=None):
+    """One outer iteration (pyop2/demo/airfoil.py:88-131); returns the rms
+    Global of the second update."""
+    save_soln(op2, A)
+    for _ in range(2):
+        adt_calc(op2, A)
+        res_calc(op2, A)
+        bres_calc(op2, A)
+        g = rms if rms is not None else op2.Global(1, 0.0, np.float64, "rms")
+        update(op2, A, g)
+    return g
+
+
+def bytes_per_iteration(ncells, nnodes, nedges, nbedges):
+    """Algorithmic (compulsory) bytes of one outer iteration: every distinct
+    Map and Dat of a loop touched once (x2 for read-modify-write), maps with
+    identical values (pecell/pevcell, pbecell/pbevcell) counted once."""
+    f8 = 8
+    save = ncells * 4 * f8 * 2
+    adt = ncells * 4 * 4 + nnodes * 2 * f8 + ncells * 4 * f8 + ncells * f8
+    res = (nedges * 2 * 4 * 2 + nnodes * 2 * f8 + ncells * 4 * f8 + ncells * f8 +
+           2 * ncells * 4 * f8)
+    bres = nbedges * (2 * 4 + 4 + 2 * 2 * f8 + 4 * f8 + f8 + 2 * 4 * f8 + 4)
+    upd = ncells * 4 * f8 * 2 + 2 * ncells * 4 * f8 + ncells * f8
+    return {"save_soln": save, "adt_calc": adt, "res_calc": res, "bres_calc": bres,
+            "update": upd, "iteration": save + 2 * (adt + res + bres + upd)}

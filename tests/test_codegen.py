@@ -1,0 +1,136 @@
+"""Stub generation: every loop form of the reference's unit tests and of the
+workloads generates CUDA that NVRTC compiles for sm_100a.  NVRTC needs no GPU,
+so this runs on the CPU and catches generator errors before a GPU run."""
+
+import ctypes as C
+import re
+
+import numpy as np
+import pytest
+
+from pyop2_b200 import backends, codegen
+
+
+@pytest.fixture(scope="module")
+def host_op2():
+    """The op2 API with the B200 backend selected but no device initialised
+    (the data classes are host-only until a loop runs)."""
+    from pyop2_b200 import _lib, op2
+    if backends.get_backend() == "pyop2_b200.void":
+        backends.set_backend("b200")
+    _lib.load()
+    return op2
+
+
+def nvrtc_compile(spec):
+    from pyop2_b200 import _lib
+    src, layout, _ = codegen.generate(spec)
+    opts = codegen.nvrtc_options()
+    arr = (C.c_char_p * len(opts))(*[o.encode() for o in opts])
+    out, n = C.c_void_p(), C.c_uint64()
+    log = C.create_string_buffer(1 << 16)
+    rc = _lib._lib.op2b_nvrtc_compile(src.encode(), b"stub.cu", arr, len(opts), C.byref(out),
+                                      C.byref(n), log, len(log))
+    assert rc == 0, _lib.last_error() + "\n" + src
+    _lib._lib.op2b_cubin_free(out)
+    return src, layout, n.value
+
+
+def spec_of(op2, kernel, itspace, *args):
+    from pyop2_b200 import b200
+    return b200.loop_spec(b200.ParLoop(kernel, itspace, *args))["spec"]
+
+
+def test_direct_forms(host_op2):
+    op2 = host_op2
+    s1, s2 = op2.Set(10, 1), op2.Set(10, 2)
+    x = op2.Dat(s1, np.zeros(10, np.uint32), np.uint32)
+    y = op2.Dat(s2, np.zeros(20, np.uint32), np.uint32)
+    soa = op2.Dat(s2, np.zeros(20, np.uint32), np.uint32, soa=True)
+    g = op2.Global(1, 0, np.uint32)
+    g2 = op2.Global(2, (0, 0), np.float64)
+    for acc in (op2.READ, op2.WRITE, op2.RW, op2.INC):
+        nvrtc_compile(spec_of(op2, op2.Kernel("void k(unsigned int *a) { }", "k"), s1, x(op2.IdentityMap, acc)))
+    for acc in (op2.INC, op2.MIN, op2.MAX, op2.READ):
+        src, _, _ = nvrtc_compile(spec_of(op2, op2.Kernel("void k(unsigned int *a, unsigned int *g) { }", "k"),
+                                          s1, x(op2.IdentityMap, op2.READ), g(acc)))
+    nvrtc_compile(spec_of(op2, op2.Kernel("void k(unsigned int *a, double *g) { }", "k"), s2,
+                          y(op2.IdentityMap, op2.RW), g2(op2.INC)))
+    src, _, _ = nvrtc_compile(spec_of(op2, op2.Kernel(
+        "void k(unsigned int *a) { OP2_STRIDE(a, 0) = 1; OP2_STRIDE(a, 1) = 2; }", "k"), s2,
+        soa(op2.IdentityMap, op2.WRITE)))
+    assert "op2b_store_soa" in src
+
+
+def test_indirect_forms(host_op2, golden_matrices):
+    op2 = host_op2
+    el, nd, vnd = op2.Set(2), op2.Set(4), op2.Set(4, 2)
+    emap = np.asarray(golden_matrices["elem_node_map"], np.int32)
+    en = op2.Map(el, nd, 3, emap, "en")
+    evn = op2.Map(el, vnd, 3, emap, "evn")
+    coords = op2.Dat(vnd, np.zeros(8))
+    f = op2.Dat(nd, np.zeros(4))
+    b = op2.Dat(nd, np.zeros(4))
+    bv = op2.Dat(vnd, np.zeros(8))
+    mat = op2.Mat(op2.Sparsity((en, en)), np.float64)
+    vmat = op2.Mat(op2.Sparsity((evn, evn)), np.float64)
+    gl = op2.Global(1, 1.0, np.float64)
+    K = {k: op2.Kernel(v["code"], v["name"]) for k, v in golden_matrices["kernels"].items()}
+    srcs = []
+    srcs.append(nvrtc_compile(spec_of(op2, K["mass"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.INC),
+                                      coords(evn, op2.READ)))[0])
+    srcs.append(nvrtc_compile(spec_of(op2, K["mass_vector_ffc"], el(3, 3),
+                                      vmat((evn[op2.i[0]], evn[op2.i[1]]), op2.INC), coords(evn, op2.READ)))[0])
+    srcs.append(nvrtc_compile(spec_of(op2, K["kernel_set_vec"], el(3, 3),
+                                      vmat((evn[op2.i[0]], evn[op2.i[1]]), op2.WRITE), gl(op2.READ)))[0])
+    srcs.append(nvrtc_compile(spec_of(op2, K["rhs"], el, b(en, op2.INC), coords(evn, op2.READ),
+                                      f(en, op2.READ)))[0])
+    srcs.append(nvrtc_compile(spec_of(op2, K["rhs_ffc_itspace"], el(3), b(en[op2.i[0]], op2.INC),
+                                      coords(evn, op2.READ), f(en, op2.READ)))[0])
+    srcs.append(nvrtc_compile(spec_of(op2, K["rhs_ffc_vector_itspace"], el(3), bv(evn[op2.i[0]], op2.INC),
+                                      coords(evn, op2.READ), bv(evn, op2.READ)))[0])
+    for acc in (op2.WRITE, op2.RW, op2.READ):
+        srcs.append(nvrtc_compile(spec_of(op2, op2.Kernel("void k(double *a[1], double *g) { }", "k"), el,
+                                          b(en, acc), gl(op2.INC)))[0])
+    assert all("op2b_stub" in s for s in srcs)
+    assert "op2b_csr_find" in srcs[0]
+
+
+def test_airfoil_stubs(host_op2):
+    from pyop2_b200 import base
+    from pyop2_b200.workloads import airfoil
+    op2 = host_op2
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    A = airfoil.build(op2, 6, 3, 0)
+    from pyop2_b200 import b200
+    loops = [
+        (A.k_save, A.cells, [A.p_q(op2.IdentityMap, op2.READ), A.p_qold(op2.IdentityMap, op2.WRITE)]),
+        (A.k_adt, A.cells, [A.p_x(A.pcell[k], op2.READ) for k in range(4)] +
+         [A.p_q(op2.IdentityMap, op2.READ), A.p_adt(op2.IdentityMap, op2.WRITE)]),
+        (A.k_res, A.edges, [A.p_x(A.pedge[0], op2.READ), A.p_x(A.pedge[1], op2.READ),
+                            A.p_q(A.pevcell[0], op2.READ), A.p_q(A.pevcell[1], op2.READ),
+                            A.p_adt(A.pecell[0], op2.READ), A.p_adt(A.pecell[1], op2.READ),
+                            A.p_res(A.pevcell[0], op2.INC), A.p_res(A.pevcell[1], op2.INC)]),
+        (A.k_bres, A.bedges, [A.p_x(A.pbedge[0], op2.READ), A.p_x(A.pbedge[1], op2.READ),
+                              A.p_q(A.pbevcell[0], op2.READ), A.p_adt(A.pbecell[0], op2.READ),
+                              A.p_res(A.pbevcell[0], op2.INC), A.p_bound(op2.IdentityMap, op2.READ)]),
+        (A.k_update, A.cells, [A.p_qold(op2.IdentityMap, op2.READ), A.p_q(op2.IdentityMap, op2.WRITE),
+                               A.p_res(op2.IdentityMap, op2.RW), A.p_adt(op2.IdentityMap, op2.READ),
+                               op2.Global(1, 0.0, np.float64)(op2.INC)])]
+    for k, s, args in loops:
+        info = b200.loop_spec(b200.ParLoop(k, s, *args))
+        src, layout, n = nvrtc_compile(info["spec"])
+        assert n > 0
+    for c in A.consts:
+        c.remove_from_namespace()
+
+
+def test_param_layout_offsets():
+    spec = codegen.LoopSpec("k", "void k(double *a) {}", (), [], [("double", False)], [3], [], [], [],
+                            True, [], 256, False)
+    L = codegen.ParamLayout(spec)
+    assert L.COL_OFFSET == 8
+    assert L.nbytes == 32 + 8 * len(L.fields)
+    packed = L.pack(100, 0, 100, {"d0": 0x1000, "m0": 0x2000})
+    assert len(packed) == L.nbytes
