@@ -1,0 +1,430 @@
+"""Benchmark of the B200 PyOP2 backend on the airfoil loop chain.
+
+Workload: the airfoil finite-volume chain on a synthetic
+1200 x 600 quad mesh (720,000 cells, 1,438,200 interior edges, 3,600 boundary
+edges) with randomly permuted cell and node numbering, FP64.  One step = one
+outer iteration: save_soln, then twice (adt_calc, res_calc, bres_calc, update
+with the rms reduction) -- 9 par_loops, 565.6 MB of algorithmic traffic.
+
+Metric: par_loop achieved HBM GB/s = algorithmic bytes of the step / device
+time of the step.
+
+* ``value``: the step replayed as a CUDA graph recorded through the op2 API,
+  inputs resident in HBM, L2 flushed (256 MB write) before every step; each
+  step timed by its own pair of CUDA events on the op2 stream, summed.
+* ``e2e``: the same iterations run end to end through the public op2 API from
+  pinned host arrays: declaring the problem uploads maps and Dats (H2D inside
+  the timed region), every iteration issues its 9 par_loops from Python and
+  reads rms back (D2H), and the final solution is read back.
+* ``roofline``: res_calc, the largest loop, timed alone with CUDA events per
+  launch (all its colour launches) after an L2 flush.
+* ``cpu_baseline``: the oracle's restated OpenMP backend (pyop2/openmp.py) on
+  the host cores, a bounded sample of the same mesh.
+
+``--impl reference`` times the reference's CPU implementation of the path
+(the restated OpenMP backend; the Python 2 reference itself cannot run here)
+on the same workload and prints its line.
+
+Multi-GPU: replicas only (each rank runs its own mesh on its own GPU, no data
+exchange); torch.distributed supplies the barrier and the max over ranks.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+NX, NY = 1200, 600
+SEED = 0
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class _Dist(object):
+    """Barrier and max-over-ranks through torch.distributed (N > 1 only)."""
+
+    def __init__(self, ws, rank, local, backend):
+        self.ws, self.rank = ws, rank
+        self.pg = None
+        if ws > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+            self.dist, self.torch, self.backend = dist, torch, backend
+
+    def barrier(self):
+        if self.ws > 1:
+            self.dist.barrier()
+
+    def max(self, v):
+        if self.ws == 1:
+            return v
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler(object):
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _set_mesh(nx, ny):
+    global NX, NY
+    NX, NY = nx, ny
+
+
+def _bytes():
+    from pyop2_b200.workloads.meshes import airfoil_grid
+    from pyop2_b200.workloads import airfoil
+    g = airfoil_grid(NX, NY, SEED, permute=False)
+    return airfoil.bytes_per_iteration(g.ncells, g.nnodes, g.nedges, g.nbedges)
+
+
+def _traffic_from_profile():
+    """dram bytes (read+write) per res_calc launch from the committed ncu
+    summary, if one exists."""
+    p = os.path.join(HERE, "profiles", "ncu_metrics.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("res_calc_airfoil_1200x600", {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def _peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- CPU leg
+def cpu_airfoil(seconds=20.0, max_iters=50, threads=None):
+    """Restated OpenMP backend on the full mesh: iterations until ~seconds of
+    element-loop time; returns (GB/s, iterations, threads, loop seconds)."""
+    from oracle import seq
+    from pyop2_b200.workloads import airfoil
+    from pyop2_b200.workloads.meshes import airfoil_grid
+    nthreads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(nthreads)
+    seq._CONSTS.clear()
+    grid = airfoil_grid(NX, NY, SEED)
+    A = airfoil.build(seq, NX, NY, SEED, grid=grid)
+    loop_time = [0.0]
+    orig = seq.par_loop
+
+    def timed(*a, **k):
+        return orig(*a, openmp=True, part_size=1024, timer=lambda dt: loop_time.__setitem__(0, loop_time[0] + dt), **k)
+    seq.par_loop = timed
+    try:
+        airfoil.iteration(seq, A)  # compile + plan, not timed
+        loop_time[0] = 0.0
+        iters = 0
+        while iters < max_iters and (loop_time[0] < seconds or iters == 0):
+            airfoil.iteration(seq, A)
+            iters += 1
+    finally:
+        seq.par_loop = orig
+    bpi = _bytes()["iteration"]
+    return bpi * iters / loop_time[0] / 1e9, iters, nthreads, loop_time[0]
+
+
+def run_reference(args, ws, rank, local):
+    """--impl reference: the reference's CPU path (restated OpenMP backend)."""
+    if rank != 0:
+        return 0
+    t0 = time.time()
+    vals = []
+    steps = max(1, args.steps)
+    bpi = _bytes()["iteration"]
+    # bounded: about 60 s of element-loop work in total
+    gbs, iters, nthreads, secs = cpu_airfoil(seconds=min(60.0, 2.0 * steps), max_iters=steps)
+    line = {"metric": "par_loop achieved HBM GB/s (airfoil chain)", "value": round(gbs, 3),
+            "unit": "GB/s", "n_gpus": ws, "steps": iters, "warmup": 1,
+            "ms_per_step": round(1e3 * secs / iters, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "airfoil 1200x600, permuted numbering, FP64, one outer "
+                                   "iteration per step", "global_batch": 1, "seq_len": 0,
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads,
+                             "kind": "port",
+                             "sample": "%d airfoil iterations of the 1200x600 mesh, restated "
+                                       "OpenMP backend (oracle), element loops timed" % iters},
+            "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": round(time.time() - t0, 1)}
+    print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------- GPU leg
+def run_gpu(args, ws, rank, local):
+    from pyop2_b200 import op2, b200, base
+    from pyop2_b200.workloads import airfoil
+    from pyop2_b200.workloads.meshes import airfoil_grid
+    d = _Dist(ws, rank, local, "nccl" if ws > 1 else "gloo")
+    opts = {}
+    if args.part_size:
+        opts["partition_size"] = args.part_size
+    if args.block_size:
+        opts["block_size"] = args.block_size
+    op2.init(backend="b200", device=local, **opts)
+    bytes_ = _bytes()
+    bpi = bytes_["iteration"]
+    grid = airfoil_grid(NX, NY, SEED)
+
+    # ---------------- device-resident throughput (graph replay)
+    A = airfoil.build(op2, NX, NY, SEED, grid=grid)
+    rms = op2.Global(1, 0.0, np.float64, "rms")
+
+    def step():
+        rms.zero()
+        airfoil.iteration(op2, A, rms)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    b200.synchronize()
+    with b200.capture() as graph:
+        step()
+    for _ in range(args.warmup):
+        b200.l2_flush()
+        graph.launch()
+    b200.synchronize()
+    launches = sum(bl.plan.ncolors if bl.indirect else 1 for bl in _step_loops(A))
+    ev = [(b200.Event(), b200.Event()) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    # keep the GPU busy ~1 s so the 200 ms clock samples see it under load;
+    # the timed steps below follow without a pause
+    soak_end = time.time() + 1.0
+    while time.time() < soak_end:
+        for _ in range(20):
+            b200.l2_flush()
+            graph.launch()
+        b200.synchronize()
+    d.barrier()
+    b200.synchronize()
+    for k in range(args.steps):
+        b200.l2_flush()
+        ev[k][0].record()
+        graph.launch()
+        ev[k][1].record()
+    b200.synchronize()
+    d.barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_ms(b) for a, b in ev]
+    total_ms = d.max(sum(step_ms))
+    value = ws * bpi * args.steps / (total_ms * 1e-3) / 1e9
+    final_rms = float(np.sqrt(rms.data[0] / grid.ncells))
+
+    # ---------------- roofline: res_calc alone, per launch
+    res_ms = []
+    for _ in range(max(3, min(args.steps, 20))):
+        b200.l2_flush()
+        e0 = b200.Event().record()
+        airfoil.res_calc(op2, A)
+        e1 = b200.Event().record()
+        e1.synchronize()
+        res_ms.append(e0.elapsed_ms(e1))
+    res_avg = statistics.mean(res_ms)
+    res_bytes = bytes_["res_calc"]
+    peak, peak_kind = _peaks()
+    achieved = res_bytes / (res_avg * 1e-3) / 1e9
+    traffic = _traffic_from_profile()
+
+    e2e_val = e2e_ms = h2d = d2h = None
+    e2e_iters = args.steps
+    rms_hist = [0.0]
+    if not args.no_e2e:
+        # ---------------- end to end through the public API
+        for c in list(base.Const._defs):
+            c.remove_from_namespace()
+        del graph
+        e2e_iters = args.steps
+        def pin(src):
+            dst = b200.pinned_empty(src.shape, src.dtype)
+            dst[...] = src
+            return dst
+
+        class PinnedGrid(object):
+            pass
+        pg = PinnedGrid()
+        for k, v in vars(grid).items():
+            setattr(pg, k, pin(v) if isinstance(v, np.ndarray) else v)
+        q0 = airfoil.initial_q(grid.ncells, SEED)
+        host = {"q": pin(q0), "qold": pin(q0), "adt": pin(np.zeros(grid.ncells)),
+                "res": pin(np.zeros((grid.ncells, 4)))}
+        d.barrier()
+        b200.synchronize()
+        t0 = b200.Event().record()
+        E = airfoil.build(op2, NX, NY, SEED, grid=pg, q0=host["q"], qold0=host["qold"],
+                          zeros=(host["adt"], host["res"]))
+        rms_hist = []
+        for _ in range(e2e_iters):
+            r = airfoil.iteration(op2, E)
+            rms_hist.append(float(r.data[0]))
+        q_out = E.p_q.data_ro
+        t1 = b200.Event().record()
+        t1.synchronize()
+        e2e_ms = d.max(t0.elapsed_ms(t1))
+        e2e_val = ws * bpi * e2e_iters / (e2e_ms * 1e-3) / 1e9
+        h2d = (sum(getattr(pg, k).nbytes for k in ("pedge", "pecell", "pbedge", "pbecell", "pcell",
+                                                   "p_bound", "x")) +
+               sum(v.nbytes for v in host.values()) + e2e_iters * 2 * 8)
+        d2h = e2e_iters * 2 * 8 + q_out.nbytes
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        gbs, iters, nthreads, secs = cpu_airfoil(seconds=args.cpu_seconds, max_iters=50)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": "%d iterations of the full 1200x600 airfoil mesh (%.1f s of element "
+                         "loops), restated OpenMP backend (oracle)" % (iters, secs)}
+    line = {
+        "metric": "par_loop achieved HBM GB/s (airfoil chain)",
+        "value": round(value, 2), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "airfoil 1200x600 (720000 cells, 1438200 edges, 3600 boundary "
+                               "edges), permuted numbering, FP64, one outer iteration (9 "
+                               "par_loops) per step",
+                   "bytes_per_step": bpi, "global_batch": ws, "seq_len": 0,
+                   "parallelism": "replicas" if ws > 1 else "single",
+                   "l2": "flushed (256 MB write) before every step", "timing": "CUDA graph "
+                   "replay, CUDA events per step on the op2 stream, max over ranks"},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"kernel": "res_calc (all colour launches)", "bound": "hbm",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes": res_bytes, "avg_ms": round(res_avg, 4),
+                     "traffic": traffic},
+        "e2e": None if e2e_val is None else {
+            "value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d // e2e_iters),
+            "d2h_bytes_per_step": int(d2h // e2e_iters), "iterations": e2e_iters,
+            "ms": round(e2e_ms, 3)},
+        "clocks": clocks,
+        "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line))
+    d.close()
+    return 0
+
+
+def _step_loops(A):
+    """The bound loops of one iteration (for counting launches)."""
+    from pyop2_b200 import b200
+    out = []
+    for bl in b200.ParLoop._bound_cache.values():
+        if bl.spec.kernel_name in ("save_soln", "adt_calc", "res_calc", "bres_calc", "update"):
+            out.append(bl)
+    names = [bl.spec.kernel_name for bl in out]
+    mult = {"save_soln": 1, "adt_calc": 2, "res_calc": 2, "bres_calc": 2, "update": 2}
+    res = []
+    for bl, nm in zip(out, names):
+        res += [bl] * mult[nm]
+    return res
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--nx", type=int, default=NX, help="cells along x (default 1200)")
+    p.add_argument("--ny", type=int, default=NY, help="cells along y (default 600)")
+    p.add_argument("--part-size", type=int, default=0, help="plan partition size (0: backend default)")
+    p.add_argument("--block-size", type=int, default=0, help="threads per CTA (0: backend default)")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    args = p.parse_args(argv)
+    _set_mesh(args.nx, args.ny)
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank, local)
+    return run_gpu(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

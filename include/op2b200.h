@@ -44,6 +44,11 @@ int op2b_last_error(char *buf, size_t len);
  * global memory bytes, L2 bytes. */
 int op2b_device_info(int32_t *sm_count, int32_t *smem_optin, int32_t *cc_major,
                      int32_t *cc_minor, uint64_t *total_mem, uint64_t *l2_bytes);
+/* Maximum L2 fetch granularity of this process's context (32, 64 or 128
+ * bytes; a per-context limit, cudaLimitMaxL2FetchGranularity).  Indirect
+ * gathers of Dat rows of 8-32 bytes through permuted Maps fetch less unused
+ * data at 32.  No reference counterpart (PyCUDA used the default). */
+int op2b_set_l2_fetch_granularity(int32_t bytes);
 
 /* ------------------------------------------------------------------------
  * Device memory and transfers.  Replaces the PyCUDA gpuarray allocations and

@@ -24,6 +24,7 @@ _SIGS = {
     "op2b_version": [],
     "op2b_last_error": [C.c_char_p, C.c_size_t],
     "op2b_device_info": [i32p, i32p, i32p, i32p, u64p, u64p],
+    "op2b_set_l2_fetch_granularity": [i32],
     "op2b_malloc": [u64p, u64],
     "op2b_free": [u64],
     "op2b_host_alloc": [u64p, u64],

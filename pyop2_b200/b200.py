@@ -59,6 +59,9 @@ def _setup():
                   cc=(ma.value, mi.value), total_mem=tot.value, l2_bytes=l2.value)
     _state['err'] = DeviceBuffer(16)
     _state['err'].memset(0)
+    fetch = int(cfg.cfg['l2_fetch_granularity'])
+    if fetch:
+        call("op2b_set_l2_fetch_granularity", fetch)
 
 
 def _teardown():
@@ -107,9 +110,12 @@ class DeviceBuffer(object):
         self.ptr = p.value
 
     def __del__(self):
-        if getattr(self, "ptr", 0) and _state['init'] and _lib._lib is not None:
-            _lib._lib.op2b_free(self.ptr)
-            self.ptr = 0
+        try:
+            if self.ptr and _state['init'] and _lib._lib is not None:
+                _lib._lib.op2b_free(self.ptr)
+        except Exception:
+            pass
+        self.ptr = 0
 
     def from_host(self, arr):
         arr = np.ascontiguousarray(arr)
@@ -653,7 +659,7 @@ _MODULES = {}
 
 
 class _Module(object):
-    def __init__(self, source, fmad, name):
+    def __init__(self, source, fmad, name, stub):
         opts = codegen.nvrtc_options(fmad=fmad)
         digest = hashlib.sha256((source + "\0" + " ".join(opts)).encode()).hexdigest()
         cubin = _disk_cache_get(digest)
@@ -675,7 +681,7 @@ class _Module(object):
         call("op2b_module_load", cubin, C.byref(h))
         self.handle = h.value
         fn = C.c_uint64()
-        call("op2b_module_function", self.handle, b"op2b_stub", C.byref(fn))
+        call("op2b_module_function", self.handle, stub.encode(), C.byref(fn))
         self.fn = fn.value
         self.smem_set = 48 * 1024
         self.const_versions = {}
@@ -716,8 +722,8 @@ def _get_module(spec):
     key = spec.key()
     mod = _MODULES.get(key)
     if mod is None:
-        src, layout, _ = codegen.generate(spec)
-        mod = _Module(src, spec.fmad, spec.kernel_name)
+        src, layout, stub = codegen.generate(spec)
+        mod = _Module(src, spec.fmad, spec.kernel_name, stub)
         mod.layout = layout
         mod.source = src
         _MODULES[key] = mod
@@ -852,7 +858,8 @@ def loop_spec(loop, block_size=None, fmad=None):
                              zip(gbls, [s for s in specs if s.kind == "gbl"])],
                             consts, indirect,
                             [(st[0], st[1], st[2], st[3], tuple(st[4])) for st in stages],
-                            bs, bool(cfg.cfg['fmad'] if fmad is None else fmad))
+                            bs, bool(cfg.cfg['fmad'] if fmad is None else fmad),
+                            min_blocks=int(cfg.cfg['min_blocks_per_sm']))
     gspecs = [s for s in specs if s.kind == "gbl"]
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
@@ -1009,7 +1016,8 @@ class ParLoop(base.ParLoop):
                 k.append(("d", id(a.data), id(a.map), isinstance(a.idx, IterationIndex), ix,
                           a.access._mode))
         k.append(tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()))
-        k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad']))
+        k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
+                  cfg.cfg['min_blocks_per_sm']))
         return tuple(k)
 
     def compute(self):
@@ -1039,3 +1047,97 @@ class _MPIConfig(object):
 
 
 MPI = _MPIConfig()
+
+
+# ------------------------------------------------ events, graphs, L2 flush
+class Event(object):
+    """CUDA event on the op2 stream (device-side timing)."""
+
+    def __init__(self):
+        h = C.c_uint64()
+        call("op2b_event_create", C.byref(h))
+        self.handle = h.value
+
+    def record(self):
+        call("op2b_event_record", self.handle, 0)
+        return self
+
+    def synchronize(self):
+        call("op2b_event_sync", self.handle)
+
+    def elapsed_ms(self, later):
+        ms = C.c_float()
+        call("op2b_event_elapsed_ms", self.handle, later.handle, C.byref(ms))
+        return ms.value
+
+    def __del__(self):
+        try:
+            if self.handle and _state['init']:
+                _lib._lib.op2b_event_destroy(self.handle)
+        except Exception:
+            pass
+
+
+class Graph(object):
+    """A CUDA graph of par_loops recorded by :func:`capture`."""
+
+    def __init__(self):
+        self.handle = 0
+
+    def launch(self):
+        call("op2b_graph_launch", self.handle, 0)
+
+    def __del__(self):
+        try:
+            if self.handle and _state['init']:
+                _lib._lib.op2b_graph_destroy(self.handle)
+        except Exception:
+            pass
+
+
+class capture(object):
+    """Record the par_loops issued inside the block into a CUDA graph instead
+    of running them::
+
+        with b200.capture() as g:
+            op2.par_loop(...)
+        g.launch()
+
+    Every loop must have run once before (its stub, plan and device data
+    exist), and the block must not read results on the host."""
+
+    def __enter__(self):
+        self.graph = Graph()
+        call("op2b_graph_begin", 0)
+        return self.graph
+
+    def __exit__(self, exc_type, exc, tb):
+        h = C.c_uint64()
+        rc = _lib._lib.op2b_graph_end(0, C.byref(h))
+        if exc_type is None:
+            _lib.check(rc, "op2b_graph_end")
+            self.graph.handle = h.value
+        return False
+
+
+_FLUSH = {}
+
+
+def l2_flush():
+    """Overwrite a buffer twice the size of L2, evicting cached data."""
+    buf = _FLUSH.get('buf')
+    if buf is None:
+        buf = _FLUSH['buf'] = DeviceBuffer(max(2 * int(_state['l2_bytes']), 256 << 20))
+    buf.memset(_FLUSH.setdefault('v', 0) & 0xff)
+    _FLUSH['v'] += 1
+
+
+def _global_zero(self):
+    """Set the Global to zero on the device (no host round trip)."""
+    if self._state is DEVICE_UNALLOCATED:
+        self._device = DeviceBuffer(max(self._data.nbytes, 16))
+    self._device.memset(0, self._data.nbytes)
+    self._state = DEVICE
+
+
+Global.zero = _global_zero

@@ -68,7 +68,8 @@ class LoopSpec(object):
     """Everything the generator needs about one loop."""
 
     def __init__(self, kernel_name, kernel_code, extents, args, dats, maps, mats, gbls,
-                 consts, indirect, stages, block_size, fmad):
+                 consts, indirect, stages, block_size, fmad, min_blocks=0):
+        self.min_blocks = int(min_blocks)
         self.kernel_name = kernel_name
         self.kernel_code = kernel_code
         self.extents = tuple(extents)
@@ -88,7 +89,7 @@ class LoopSpec(object):
                 tuple(a.key() for a in self.args), tuple(self.dats), tuple(self.maps),
                 tuple(self.mats), tuple(self.gbls), tuple(self.consts), self.indirect,
                 tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
-                self.block_size, self.fmad)
+                self.block_size, self.fmad, self.min_blocks)
 
     @property
     def needs_coloring(self):
@@ -162,6 +163,19 @@ def _struct_decl(spec, layout):
     return "\n".join(lines)
 
 
+def _bounds(spec):
+    if spec.min_blocks:
+        return "__launch_bounds__(%d, %d)" % (spec.block_size, spec.min_blocks)
+    return "__launch_bounds__(%d)" % spec.block_size
+
+
+def stub_name(spec):
+    """Symbol of the stub: op2b_<user kernel name> (distinct per loop in
+    profiles)."""
+    import re
+    return "op2b_" + re.sub(r"[^A-Za-z0-9_]", "_", spec.kernel_name)
+
+
 def _kernel_source(spec):
     """User kernel as a device function.  Every function of the user code is
     compiled for the device (NVRTC -default-device) and the entry is forced
@@ -197,7 +211,7 @@ def generate(spec):
     w("#undef OP2_STRIDE")
     body = _indirect_body(spec) if spec.indirect else _direct_body(spec)
     w(body)
-    return "\n".join(out), layout, "op2b_stub"
+    return "\n".join(out), layout, stub_name(spec)
 
 
 # ------------------------------------------------------------------ helpers
@@ -255,7 +269,7 @@ def _kernel_call(spec, argexprs, indent):
 
 def _direct_body(spec):
     bs = spec.block_size
-    L = ["extern \"C\" __global__ void __launch_bounds__(%d) op2b_stub(const op2b_params p) {" % bs]
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
     _gbl_prologue(spec, L)
     L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
              " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
@@ -292,7 +306,7 @@ def _indirect_body(spec):
     bs = spec.block_size
     ninds = len(spec.stages)
     coloured = spec.needs_coloring
-    L = ["extern \"C\" __global__ void __launch_bounds__(%d) op2b_stub(const op2b_params p) {" % bs]
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
     L.append("  if ((int)blockIdx.x >= p.col_n) return;")
     L.append("  const int blk = p.blkmap[p.col_first + blockIdx.x];")
     L.append("  const int start = p.offset[blk];")

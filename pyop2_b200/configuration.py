@@ -10,7 +10,12 @@ keys of the B200 backend:
   (default False: every FP operation is rounded separately, like the host
   compiler on x86-64, so direct loops reproduce host results bit for bit);
 * ``cache_dir``: directory of the on-disk cubin cache;
-* ``validate_maps``: check Map values against their target Set on upload.
+* ``validate_maps``: check Map values against their target Set on upload;
+* ``l2_fetch_granularity``: per-context maximum L2 fetch granularity in bytes
+  (32 suits gathers of small Dat rows through permuted Maps; 0 keeps the
+  driver default);
+* ``min_blocks_per_sm``: second __launch_bounds__ argument of the stubs (0:
+  none), which caps registers per thread to raise occupancy.
 """
 
 import os
@@ -27,6 +32,8 @@ _defaults = {
                                 os.path.join('/tmp', 'op2b200-cache-%d' % os.getuid())),
     'validate_maps': True,
     'device': 0,
+    'l2_fetch_granularity': 32,
+    'min_blocks_per_sm': 0,
 }
 
 _config = dict(_defaults)

@@ -151,6 +151,14 @@ int op2b_device_info(int32_t *sm, int32_t *smem, int32_t *major, int32_t *minor,
   return OP2B_OK;
 }
 
+int op2b_set_l2_fetch_granularity(int32_t bytes) {
+  OP2B_REQUIRE_INIT();
+  if (bytes != 32 && bytes != 64 && bytes != 128)
+    return set_error(OP2B_ERR_ARG, "L2 fetch granularity %d (32, 64 or 128)", bytes);
+  OP2B_CUDA(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, (size_t)bytes));
+  return OP2B_OK;
+}
+
 // ---------------------------------------------------------------- memory
 int op2b_malloc(uint64_t *dptr, uint64_t bytes) {
   OP2B_REQUIRE_INIT();

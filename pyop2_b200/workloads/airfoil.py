@@ -129,8 +129,10 @@ class Airfoil(object):
     """The op2 objects of one airfoil problem."""
 
 
-def build(op2, nx, ny, seed=0, grid=None, consts=True):
-    """Declare the airfoil problem through ``op2`` (B200 op2 or the oracle)."""
+def build(op2, nx, ny, seed=0, grid=None, consts=True, q0=None, qold0=None, zeros=None):
+    """Declare the airfoil problem through ``op2`` (B200 op2 or the oracle).
+    ``q0``/``qold0``/``zeros`` optionally supply the host arrays (e.g. pinned
+    memory) of q, qold and of the zero-initialised adt/res."""
     g = grid if grid is not None else airfoil_grid(nx, ny, seed)
     A = Airfoil()
     A.grid = g
@@ -148,11 +150,13 @@ def build(op2, nx, ny, seed=0, grid=None, consts=True):
     A.pcell = op2.Map(A.cells, A.nodes, 4, g.pcell, "pcell")
     A.p_bound = op2.Dat(A.bedges, g.p_bound, np.int32, "p_bound")
     A.p_x = op2.Dat(A.nodes, g.x, np.float64, "p_x")
-    q0 = initial_q(g.ncells, seed)
+    if q0 is None:
+        q0 = initial_q(g.ncells, seed)
     A.p_q = op2.Dat(A.vcells, q0, np.float64, "p_q")
-    A.p_qold = op2.Dat(A.vcells, q0.copy(), np.float64, "p_qold")
-    A.p_adt = op2.Dat(A.cells, np.zeros(g.ncells), np.float64, "p_adt")
-    A.p_res = op2.Dat(A.vcells, np.zeros((g.ncells, 4)), np.float64, "p_res")
+    A.p_qold = op2.Dat(A.vcells, q0.copy() if qold0 is None else qold0, np.float64, "p_qold")
+    za, zr = zeros if zeros is not None else (np.zeros(g.ncells), np.zeros((g.ncells, 4)))
+    A.p_adt = op2.Dat(A.cells, za, np.float64, "p_adt")
+    A.p_res = op2.Dat(A.vcells, zr, np.float64, "p_res")
     if consts:
         A.consts = [op2.Const(1, GAM, "gam", np.float64), op2.Const(1, GM1, "gm1", np.float64),
                     op2.Const(1, CFL, "cfl", np.float64), op2.Const(1, EPS, "eps", np.float64),

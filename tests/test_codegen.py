@@ -92,7 +92,8 @@ def test_indirect_forms(host_op2, golden_matrices):
     for acc in (op2.WRITE, op2.RW, op2.READ):
         srcs.append(nvrtc_compile(spec_of(op2, op2.Kernel("void k(double *a[1], double *g) { }", "k"), el,
                                           b(en, acc), gl(op2.INC)))[0])
-    assert all("op2b_stub" in s for s in srcs)
+    assert all('extern "C" __global__' in s for s in srcs)
+    assert "op2b_mass(" in srcs[0] and "op2b_rhs_ffc_itspace(" in srcs[4]
     assert "op2b_csr_find" in srcs[0]
 
 
