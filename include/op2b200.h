@@ -191,6 +191,32 @@ int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx,
                        const int32_t *rows, int32_t nrows_zero, double diag,
                        int32_t elem_bytes, uint64_t stream);
 
+/* op2b_mat_zero_rows for callers that must not allocate device memory.
+ * No counterpart in the reference.
+ *
+ * op2b_mat_zero_rows copies the row list to device memory it allocates (from
+ * the stream-ordered pool) on every call.  Some callers cannot let the library
+ * allocate: a solver loop that applies boundary conditions every time step
+ * inside a process whose device memory is reserved up front by its host
+ * framework (a further cudaMalloc fails or is forbidden there), or code that
+ * must not risk the synchronisation or out-of-memory failure an allocation can
+ * bring in the middle of a time step.  This entry point takes the same inputs
+ * and outputs and allocates nothing: the row list goes into a fixed scratch
+ * array compiled into the library (OP2B_ZERO_ROWS_STATIC_MAX rows, 256 KiB,
+ * held on every GPU that loads the library until the process exits).
+ *  - More than OP2B_ZERO_ROWS_STATIC_MAX rows is rejected with OP2B_ERR_ARG
+ *    (split the list, or call op2b_mat_zero_rows).
+ *  - The first call on a device looks up the scratch array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls share the one scratch array, which keeps the last call's row
+ *    list: calls that overlap on the GPU (other streams, other threads) race
+ *    and must be serialised by the caller.  The call returns after its work
+ *    has finished on the stream. */
+#define OP2B_ZERO_ROWS_STATIC_MAX 65536
+int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_t colidx,
+                              const int32_t *rows, int32_t nrows_zero, double diag,
+                              int32_t elem_bytes, uint64_t stream);
+
 #ifdef __cplusplus
 }
 #endif

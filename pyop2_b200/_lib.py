@@ -70,6 +70,7 @@ _SIGS = {
     "op2b_sparsity_arrays": [u64, u64p, u64p, u64p],
     "op2b_sparsity_free": [u64],
     "op2b_mat_zero_rows": [u64, u64, u64, i32p, i32, C.c_double, i32, u64],
+    "op2b_mat_zero_rows_static": [u64, u64, u64, i32p, i32, C.c_double, i32, u64],
 }
 
 EXPORTED = tuple(sorted(_SIGS))

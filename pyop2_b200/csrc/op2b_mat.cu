@@ -6,6 +6,8 @@
 // the pattern stores one, becomes diag.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "op2b_internal.h"
@@ -25,9 +27,68 @@ __global__ void zero_rows_kernel(T *__restrict__ vals, const int32_t *__restrict
   }
 }
 
+// ---- scratch of op2b_mat_zero_rows_static: the row list lives in a fixed
+// device array instead of memory allocated per call.  Every GPU that loads
+// this library holds OP2B_ZERO_ROWS_STATIC_MAX * 4 bytes (256 KiB) for it
+// until the process exits.
+static __device__ __align__(256) int32_t g_zero_rows_scratch[OP2B_ZERO_ROWS_STATIC_MAX];
+
+// Device address of g_zero_rows_scratch per device.  In host code the array's
+// name is only a host-side stand-in, never a device address, so the address is
+// looked up with cudaGetSymbolAddress on the first call on each device.
+constexpr int kMaxDevices = 64;
+static int32_t *g_zero_rows_scratch_dev[kMaxDevices] = {nullptr};
+static std::mutex g_zero_rows_scratch_mutex;
+
+static int zero_rows_scratch(int32_t **out) {
+  int dev = 0;
+  OP2B_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return set_error(OP2B_ERR_STATE, "device %d", dev);
+  std::lock_guard<std::mutex> lock(g_zero_rows_scratch_mutex);
+  if (!g_zero_rows_scratch_dev[dev]) {
+    void *p = nullptr;
+    OP2B_CUDA(cudaGetSymbolAddress(&p, g_zero_rows_scratch));
+    g_zero_rows_scratch_dev[dev] = static_cast<int32_t *>(p);
+  }
+  *out = g_zero_rows_scratch_dev[dev];
+  return OP2B_OK;
+}
+
 }  // namespace op2b
 
 using namespace op2b;
+
+extern "C" int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_t colidx,
+                                         const int32_t *rows, int32_t nrows_zero, double diag,
+                                         int32_t elem_bytes, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (nrows_zero <= 0) return OP2B_OK;
+  if (nrows_zero > OP2B_ZERO_ROWS_STATIC_MAX)
+    return set_error(OP2B_ERR_ARG,
+                     "op2b_mat_zero_rows_static: %d rows exceed its fixed scratch of %d rows; "
+                     "use op2b_mat_zero_rows or split the list", nrows_zero,
+                     OP2B_ZERO_ROWS_STATIC_MAX);
+  if (elem_bytes != 8 && elem_bytes != 4)
+    return set_error(OP2B_ERR_ARG, "op2b_mat_zero_rows_static: elem_bytes %d", elem_bytes);
+  int32_t *d_rows = nullptr;
+  int rc = zero_rows_scratch(&d_rows);
+  if (rc) return rc;
+  cudaStream_t s = stream_of(stream);
+  // The whole list is overwritten before use: nothing in the scratch needs to
+  // start at zero.
+  OP2B_CUDA(cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * nrows_zero, cudaMemcpyHostToDevice, s));
+  const int grid = std::max(1, std::min(op2b_div_up(nrows_zero, 8), sm_count() * 8));
+  if (elem_bytes == 8)
+    zero_rows_kernel<double><<<grid, 256, 0, s>>>((double *)vals, (const int32_t *)rowptr,
+                                                  (const int32_t *)colidx, d_rows, nrows_zero, diag);
+  else
+    zero_rows_kernel<float><<<grid, 256, 0, s>>>((float *)vals, (const int32_t *)rowptr,
+                                                 (const int32_t *)colidx, d_rows, nrows_zero, (float)diag);
+  OP2B_CUDA(cudaGetLastError());
+  // The caller may release or reuse the host row list as soon as this returns.
+  OP2B_CUDA(cudaStreamSynchronize(s));
+  return OP2B_OK;
+}
 
 extern "C" int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx,
                                   const int32_t *rows, int32_t nrows_zero, double diag,
