@@ -245,10 +245,16 @@ def run_gpu(args, ws, rank, local):
         opts["partition_size"] = args.part_size
     if args.block_size:
         opts["block_size"] = args.block_size
+    if args.l2_fetch >= 0:
+        opts["l2_fetch_granularity"] = args.l2_fetch
+    if args.min_blocks >= 0:
+        opts["min_blocks_per_sm"] = args.min_blocks
+    if args.inc_mode:
+        opts["inc_mode"] = args.inc_mode
     op2.init(backend="b200", device=local, **opts)
     bytes_ = _bytes()
     bpi = bytes_["iteration"]
-    grid = airfoil_grid(NX, NY, SEED)
+    grid = airfoil_grid(NX, NY, SEED, permute=not args.no_permute)
 
     # ---------------- device-resident throughput (graph replay)
     A = airfoil.build(op2, NX, NY, SEED, grid=grid)
@@ -304,6 +310,22 @@ def run_gpu(args, ws, rank, local):
         e1.synchronize()
         res_ms.append(e0.elapsed_ms(e1))
     res_avg = statistics.mean(res_ms)
+    breakdown = {}
+    for name, fn in (("save_soln", lambda: airfoil.save_soln(op2, A)),
+                     ("adt_calc", lambda: airfoil.adt_calc(op2, A)),
+                     ("res_calc", lambda: airfoil.res_calc(op2, A)),
+                     ("bres_calc", lambda: airfoil.bres_calc(op2, A)),
+                     ("update", lambda: airfoil.update(op2, A, rms))):
+        ts = []
+        for _ in range(5):
+            b200.l2_flush()
+            e0 = b200.Event().record()
+            fn()
+            e1 = b200.Event().record()
+            e1.synchronize()
+            ts.append(e0.elapsed_ms(e1))
+        ms = statistics.median(ts)
+        breakdown[name] = {"ms": round(ms, 4), "GB/s": round(bytes_[name] / (ms * 1e-3) / 1e9, 1)}
     res_bytes = bytes_["res_calc"]
     peak, peak_kind = _peaks()
     achieved = res_bytes / (res_avg * 1e-3) / 1e9
@@ -380,6 +402,8 @@ def run_gpu(args, ws, rank, local):
             "d2h_bytes_per_step": int(d2h // e2e_iters), "iterations": e2e_iters,
             "ms": round(e2e_ms, 3)},
         "clocks": clocks,
+        "loops": breakdown,
+        "inc_mode": op2_cfg_inc_mode(),
         "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
     }
     if cpu is not None:
@@ -388,6 +412,11 @@ def run_gpu(args, ws, rank, local):
         print(json.dumps(line))
     d.close()
     return 0
+
+
+def op2_cfg_inc_mode():
+    from pyop2_b200 import configuration as cfg
+    return cfg.cfg['inc_mode']
 
 
 def _step_loops(A):
@@ -418,6 +447,13 @@ def main(argv=None):
     p.add_argument("--part-size", type=int, default=0, help="plan partition size (0: backend default)")
     p.add_argument("--block-size", type=int, default=0, help="threads per CTA (0: backend default)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    p.add_argument("--l2-fetch", type=int, default=-1,
+                   help="L2 fetch granularity in bytes (32/64/128; 0 driver default; -1 backend default)")
+    p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")
+    p.add_argument("--no-permute", action="store_true",
+                   help="structured (unpermuted) cell/node numbering instead of the random one")
+    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic"],
+                   help="INC conflict resolution of indirect loops (default: backend default)")
     args = p.parse_args(argv)
     _set_mesh(args.nx, args.ny)
     ws, rank, local = _dist()

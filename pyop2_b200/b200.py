@@ -860,6 +860,9 @@ def loop_spec(loop, block_size=None, fmad=None):
                             [(st[0], st[1], st[2], st[3], tuple(st[4])) for st in stages],
                             bs, bool(cfg.cfg['fmad'] if fmad is None else fmad),
                             min_blocks=int(cfg.cfg['min_blocks_per_sm']))
+    if indirect and cfg.cfg['inc_mode'] == 'atomic' and codegen.atomic_capable(spec):
+        spec.mode = "atomic"
+        indirect = False   # launched like a direct loop: no plan
     gspecs = [s for s in specs if s.kind == "gbl"]
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
@@ -1017,7 +1020,7 @@ class ParLoop(base.ParLoop):
                           a.access._mode))
         k.append(tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()))
         k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
-                  cfg.cfg['min_blocks_per_sm']))
+                  cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode']))
         return tuple(k)
 
     def compute(self):

@@ -68,8 +68,11 @@ class LoopSpec(object):
     """Everything the generator needs about one loop."""
 
     def __init__(self, kernel_name, kernel_code, extents, args, dats, maps, mats, gbls,
-                 consts, indirect, stages, block_size, fmad, min_blocks=0):
+                 consts, indirect, stages, block_size, fmad, min_blocks=0, mode=None):
         self.min_blocks = int(min_blocks)
+        # 'direct': no Map; 'plan': coloured blocks of a GPU plan; 'atomic':
+        # one grid-stride launch, INC args added with atomics
+        self.mode = mode or ("plan" if indirect else "direct")
         self.kernel_name = kernel_name
         self.kernel_code = kernel_code
         self.extents = tuple(extents)
@@ -89,7 +92,7 @@ class LoopSpec(object):
                 tuple(a.key() for a in self.args), tuple(self.dats), tuple(self.maps),
                 tuple(self.mats), tuple(self.gbls), tuple(self.consts), self.indirect,
                 tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
-                self.block_size, self.fmad, self.min_blocks)
+                self.block_size, self.fmad, self.min_blocks, self.mode)
 
     @property
     def needs_coloring(self):
@@ -106,7 +109,7 @@ class ParamLayout(object):
 
     def __init__(self, spec):
         f = []
-        if spec.indirect:
+        if spec.mode == "plan":
             f += ["blkmap", "offset", "nelems", "nthrcol", "thrcol", "ind_map", "ind_sizes",
                   "ind_offs", "loc_map"]
         for j in range(len(spec.dats)):
@@ -209,7 +212,7 @@ def generate(spec):
     w("#define OP2_STRIDE(a, idx) (a)[idx]")
     w(_mark_inline(spec.kernel_code, spec.kernel_name))
     w("#undef OP2_STRIDE")
-    body = _indirect_body(spec) if spec.indirect else _direct_body(spec)
+    body = {"plan": _indirect_body, "atomic": _atomic_body, "direct": _direct_body}[spec.mode](spec)
     w(body)
     return "\n".join(out), layout, stub_name(spec)
 
@@ -253,7 +256,13 @@ def _direct_row(a, n, e, lines_pre, lines_post, indent):
             lines_post.append("%sop2b_store_soa(p.d%d, %s, p.ds%d, a%d);" % (indent, j, e, j, n))
         return "a%d" % n
     if a.access == "WRITE":
-        return "p.d%d + (op2b_i64)(%s) * %d" % (j, e, c)
+        # The whole row is written back from registers with vector stores (as
+        # the reference CUDA backend's staged direct args, which wrote back the
+        # full row, cuda_direct_loop.jinja2:63-65); components the kernel does
+        # not write become 0.
+        lines_pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (indent, t, n, c, n))
+        lines_post.append("%sop2b_store(p.d%d + (op2b_i64)(%s) * %d, a%d);" % (indent, j, e, c, n))
+        return "a%d" % n
     lines_pre.append("%s__align__(16) %s a%d[%d];" % (indent, t, n, c))
     lines_pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + (op2b_i64)(%s) * %d);" %
                      (indent, t, c, _ro(a), n, j, e, c))
@@ -455,7 +464,110 @@ def _indirect_body(spec):
     return "\n".join(L)
 
 
-def _mat_addto(spec, n, a, ind):
+def _atomic_body(spec):
+    """Indirect loop without a plan: a grid-stride loop over all elements;
+    INC args (Dats and Mats) are added into global memory with atomic
+    reductions.  WRITE/RW indirect args are global pointers as in the
+    coloured form (OP2 leaves their conflicts to the user)."""
+    bs = spec.block_size
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
+    _gbl_prologue(spec, L)
+    L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
+             " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
+    ind = "    "
+    used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
+                       {a.cmslot for a in spec.args if a.kind == "mat"})
+    for k in used_maps:
+        ar = spec.maps[k]
+        L.append("%s__align__(16) int mr%d[%d];" % (ind, k, ar))
+        L.append("%sop2b_load<int, %d, true>(mr%d, p.m%d + e * %d);" % (ind, ar, k, k, ar))
+    pre, post, exprs, apply = [], [], [], []
+    for n, a in enumerate(spec.args):
+        t, c = a.ctype, a.cdim
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
+        elif a.kind == "direct":
+            exprs.append(_direct_row(a, n, "e", pre, post, ind))
+        elif a.kind == "ind":
+            row = "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, a.idx, c)
+            if a.access == "INC":
+                pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind, t, n, c, n))
+                apply.append("%sop2b_atomic_row(%s, a%d);" % (ind, row, n))
+                exprs.append("a%d" % n)
+            elif a.access == "READ":
+                pre.append("%s__align__(16) %s a%d[%d];" % (ind, t, n, c))
+                pre.append("%sop2b_load<%s, %d, %s>(a%d, %s);" % (ind, t, c, _ro(a), n, row))
+                exprs.append("a%d" % n)
+            else:
+                exprs.append(row)
+        elif a.kind in ("vec", "its"):
+            cnt = a.arity if a.kind == "vec" else a.ext
+            var = "i%d" % a.idx if a.kind == "its" else None
+            if a.access in ("READ", "INC"):
+                pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
+                for r in range(cnt):
+                    src = "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, r, c)
+                    if a.access == "READ":
+                        pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], %s);" % (ind, t, c, _ro(a), n, r, src))
+                    else:
+                        pre.append("%sop2b_zero(a%d[%d]);" % (ind, n, r))
+                        apply.append("%sop2b_atomic_row(%s, a%d[%d]);" % (ind, src, n, r))
+                if a.kind == "vec":
+                    pre.append("%s%s *a%d_v[%d] = {%s};" %
+                               (ind, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
+                    exprs.append("a%d_v" % n)
+                else:
+                    exprs.append("a%d[%s]" % (n, var))
+            else:
+                if a.kind == "vec":
+                    pre.append("%s%s *a%d_v[%d] = {%s};" % (
+                        ind, t, n, cnt, ", ".join("p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, r, c)
+                                                   for r in range(cnt))))
+                    exprs.append("a%d_v" % n)
+                else:
+                    exprs.append("p.d%d + (op2b_i64)mr%d[%s] * %d" % (a.slot, a.mslot, var, c))
+        elif a.kind == "mat":
+            e0, e1 = spec.extents[0], spec.extents[1]
+            if a.rm * a.cm == 1:
+                pre.append("%s%s A%d[%d][%d];" % (ind, t, n, e0, e1))
+                exprs.append("(%s (*)[1])&A%d[i0][i1]" % (t, n))
+            else:
+                pre.append("%s%s A%d[%d][%d][%d][%d];" % (ind, t, n, e0, e1, a.rm, a.cm))
+                exprs.append("A%d[i0][i1]" % n)
+            apply += _mat_addto(spec, n, a, ind, atomic=True)
+    L += pre
+    L += _itspace_open(spec, ind)
+    deep = ind + "  " * len(spec.extents)
+    for n, a in enumerate(spec.args):
+        if a.kind == "mat":
+            if a.rm * a.cm == 1:
+                L.append("%sA%d[i0][i1] = (%s)0;" % (deep, n, a.ctype))
+            else:
+                L.append("%sfor (int r = 0; r < %d; ++r) for (int c = 0; c < %d; ++c) A%d[i0][i1][r][c] = (%s)0;"
+                         % (deep, a.rm, a.cm, n, a.ctype))
+    L.append(_kernel_call(spec, exprs, deep))
+    L += _itspace_close(spec, ind)
+    L += post
+    L += apply
+    L.append("  }")
+    _gbl_epilogue(spec, L)
+    L.append("}")
+    return "\n".join(L)
+
+
+def atomic_capable(spec):
+    """True if every INC target of the loop has a native atomic add and no
+    Mat is written with WRITE (insertion needs the coloured form)."""
+    ok = {"double", "float", "int", "unsigned int", "unsigned long long", "long long"}
+    for a in spec.args:
+        if a.kind in ("ind", "vec", "its") and a.access == "INC" and a.ctype not in ok:
+            return False
+        if a.kind == "mat" and (a.access != "INC" or a.ctype not in ok):
+            return False
+    return True
+
+
+def _mat_addto(spec, n, a, ind, atomic=False):
     """Add / insert the local tensor of Mat arg n into the CSR values
     (pyop2/host.py:145-184: scalar fields add the whole block, vector fields
     add entry by entry and skip zero values when adding)."""
@@ -472,6 +584,8 @@ def _mat_addto(spec, n, a, ind):
         L.append("%s  if (pos < 0) op2b_flag_missing(p.err, row, colj);" % ind)
         if ins:
             L.append("%s  else p.mv%d[pos] = A%d[i0][i1];" % (ind, j, n))
+        elif atomic:
+            L.append("%s  else op2b_atomic_add(&p.mv%d[pos], A%d[i0][i1]);" % (ind, j, n))
         else:
             L.append("%s  else p.mv%d[pos] += A%d[i0][i1];" % (ind, j, n))
     else:
@@ -485,6 +599,8 @@ def _mat_addto(spec, n, a, ind):
         L.append("%s    if (pos < 0) op2b_flag_missing(p.err, row, colj);" % ind)
         if ins:
             L.append("%s    else p.mv%d[pos] = v;" % (ind, j))
+        elif atomic:
+            L.append("%s    else op2b_atomic_add(&p.mv%d[pos], v);" % (ind, j))
         else:
             L.append("%s    else p.mv%d[pos] += v;" % (ind, j))
         L.append("%s  }" % ind)

@@ -15,7 +15,11 @@ keys of the B200 backend:
   (32 suits gathers of small Dat rows through permuted Maps; 0 keeps the
   driver default);
 * ``min_blocks_per_sm``: second __launch_bounds__ argument of the stubs (0:
-  none), which caps registers per thread to raise occupancy.
+  none), which caps registers per thread to raise occupancy;
+* ``inc_mode``: how indirect loops resolve INC conflicts: ``'color'`` (plan
+  with block and thread colouring; deterministic, bit-identical from run to
+  run) or ``'atomic'`` (one launch, atomic adds; summation order varies
+  between runs within rounding).
 """
 
 import os
@@ -34,6 +38,7 @@ _defaults = {
     'device': 0,
     'l2_fetch_granularity': 32,
     'min_blocks_per_sm': 0,
+    'inc_mode': 'atomic',
 }
 
 _config = dict(_defaults)

@@ -104,6 +104,25 @@ __device__ __forceinline__ int op2b_csr_find(const int *__restrict__ rowptr,
   return (lo < end && colidx[lo] == col) ? lo : -1;
 }
 
+// Atomic increment for the atomic INC mode (no plan, no colouring).  The
+// result is unused, so the compiler emits a reduction (RED) to L2.
+__device__ __forceinline__ void op2b_atomic_add(double *a, double v) { atomicAdd(a, v); }
+__device__ __forceinline__ void op2b_atomic_add(float *a, float v) { atomicAdd(a, v); }
+__device__ __forceinline__ void op2b_atomic_add(int *a, int v) { atomicAdd(a, v); }
+__device__ __forceinline__ void op2b_atomic_add(unsigned *a, unsigned v) { atomicAdd(a, v); }
+__device__ __forceinline__ void op2b_atomic_add(unsigned long long *a, unsigned long long v) {
+  atomicAdd(a, v);
+}
+__device__ __forceinline__ void op2b_atomic_add(long long *a, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(a), (unsigned long long)v);
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void op2b_atomic_row(T *dst, const T (&v)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) op2b_atomic_add(dst + k, v[k]);
+}
+
 // Record the first Mat insertion outside the Sparsity (PETSc raises
 // NEW_NONZERO_ALLOCATION_ERR there); err[1..2] = offending (row, col).
 __device__ __forceinline__ void op2b_flag_missing(int *err, int row, int col) {

@@ -127,6 +127,44 @@ def test_airfoil_stubs(host_op2):
         c.remove_from_namespace()
 
 
+def test_atomic_mode_stubs(host_op2, golden_matrices):
+    """The atomic INC form of the indirect loops compiles (Dat INC through
+    maps, vec maps and iteration spaces; Mat INC)."""
+    op2 = host_op2
+    from pyop2_b200 import b200
+    from pyop2_b200 import configuration as cfg
+    el, nd, vnd = op2.Set(2), op2.Set(4), op2.Set(4, 2)
+    emap = np.asarray(golden_matrices["elem_node_map"], np.int32)
+    en = op2.Map(el, nd, 3, emap, "en_a")
+    evn = op2.Map(el, vnd, 3, emap, "evn_a")
+    coords, f = op2.Dat(vnd, np.zeros(8)), op2.Dat(nd, np.zeros(4))
+    b, bv = op2.Dat(nd, np.zeros(4)), op2.Dat(vnd, np.zeros(8))
+    mat = op2.Mat(op2.Sparsity((en, en)), np.float64)
+    vmat = op2.Mat(op2.Sparsity((evn, evn)), np.float64)
+    K = {k: op2.Kernel(v["code"], v["name"]) for k, v in golden_matrices["kernels"].items()}
+    cfg.configure(inc_mode="atomic")
+    try:
+        cases = [(K["mass"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.INC), coords(evn, op2.READ)),
+                 (K["mass_vector_ffc"], el(3, 3), vmat((evn[op2.i[0]], evn[op2.i[1]]), op2.INC),
+                  coords(evn, op2.READ)),
+                 (K["rhs"], el, b(en, op2.INC), coords(evn, op2.READ), f(en, op2.READ)),
+                 (K["rhs_ffc_itspace"], el(3), b(en[op2.i[0]], op2.INC), coords(evn, op2.READ),
+                  f(en, op2.READ)),
+                 (K["rhs_ffc_vector_itspace"], el(3), bv(evn[op2.i[0]], op2.INC), coords(evn, op2.READ),
+                  bv(evn, op2.READ))]
+        for k, it, *args in cases:
+            info = b200.loop_spec(b200.ParLoop(k, it, *args))
+            assert info["spec"].mode == "atomic"
+            src, layout, _ = nvrtc_compile(info["spec"])
+            assert "op2b_atomic" in src and "blkmap" not in layout.fields
+        # a Mat WRITE still needs the coloured form
+        info = b200.loop_spec(b200.ParLoop(K["kernel_set"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.WRITE),
+                                           op2.Global(1, 1.0, np.float64)(op2.READ)))
+        assert info["spec"].mode == "plan"
+    finally:
+        cfg.configure(inc_mode="color")
+
+
 def test_param_layout_offsets():
     spec = codegen.LoopSpec("k", "void k(double *a) {}", (), [], [("double", False)], [3], [], [], [],
                             True, [], 256, False)

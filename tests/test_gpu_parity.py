@@ -32,8 +32,18 @@ def _clear_consts(op2mod):
     seq._CONSTS.clear()
 
 
+@pytest.fixture(params=["atomic", "color"])
+def inc_mode(request):
+    """Run a test under both INC conflict strategies of indirect loops."""
+    from pyop2_b200 import configuration as cfg
+    old = cfg.cfg['inc_mode']
+    cfg.configure(inc_mode=request.param)
+    yield request.param
+    cfg.configure(inc_mode=old)
+
+
 @pytest.mark.parametrize("nx,ny,seed", [(24, 12, 0), (60, 30, 1)])
-def test_airfoil_chain_matches_oracle(op2, nx, ny, seed):
+def test_airfoil_chain_matches_oracle(op2, nx, ny, seed, inc_mode):
     _clear_consts(op2)
     grid = meshes.airfoil_grid(nx, ny, seed)
     G = airfoil.build(op2, nx, ny, seed, grid=grid)
@@ -67,7 +77,18 @@ def test_airfoil_chain_matches_oracle(op2, nx, ny, seed):
 
 
 def test_airfoil_results_repeatable(op2):
-    """Same inputs, same plan: bit-identical results on every run."""
+    """Coloured INC (inc_mode='color'): same inputs, same plan, bit-identical
+    results on every run."""
+    from pyop2_b200 import configuration as cfg
+    old = cfg.cfg['inc_mode']
+    cfg.configure(inc_mode='color')
+    try:
+        _repeatable(op2)
+    finally:
+        cfg.configure(inc_mode=old)
+
+
+def _repeatable(op2):
     _clear_consts(op2)
     grid = meshes.airfoil_grid(40, 20, 3)
     outs = []
@@ -131,7 +152,7 @@ def _p1(api, coords, elem, fvals):
 
 
 @pytest.mark.parametrize("n", [16, 100])
-def test_p1_mass_rhs_matches_oracle(op2, n):
+def test_p1_mass_rhs_matches_oracle(op2, n, inc_mode):
     coords, elem = meshes.square_p1(n)
     fvals = np.sin(np.pi * coords[:, 0]) * np.sin(np.pi * coords[:, 1])
     gm, gb, gsp = _p1(op2, coords, elem, fvals)
