@@ -183,6 +183,22 @@ int op2b_sparsity_arrays(uint64_t sparsity, uint64_t *rowptr, uint64_t *colidx,
 int op2b_sparsity_free(uint64_t sparsity);
 
 /* ------------------------------------------------------------------------
+ * Incidence: for each target t of a Map [nelem][arity] (values in
+ * [0, ntargets)), the flat positions e*arity+k with map[e*arity+k] == t, sorted
+ * ascending (element order, then map index).  Owner-computes stubs use it to
+ * add all contributions to one target in the order the sequential backend
+ * adds them (pyop2/sequential.py:55-72).  No direct reference counterpart:
+ * it replaces the LMA buffer + atomic scatter of pyop2/cuda.py:177-270 and
+ * the coloured INC of cuda_indirect_loop.jinja2:169-189 for those loops.
+ * ---------------------------------------------------------------------- */
+int op2b_incidence_build(uint64_t map, int32_t nelem, int32_t arity, int32_t ntargets,
+                         uint64_t stream, uint64_t *incidence);
+/* ptr: ntargets+1 int32 offsets; list: nelem*arity int32 flat positions. */
+int op2b_incidence_arrays(uint64_t incidence, uint64_t *ptr, uint64_t *list,
+                          int32_t *max_degree);
+int op2b_incidence_free(uint64_t incidence);
+
+/* ------------------------------------------------------------------------
  * Mat operations on the device CSR values (dtype 4 = float32, 8 = float64).
  * Replaces cuda.Mat.zero_rows / zero (pyop2/cuda.py:289-301) and PETSc
  * MatZeroRowsLocal (pyop2/petsc_base.py:131-135).

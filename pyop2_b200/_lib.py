@@ -69,6 +69,9 @@ _SIGS = {
     "op2b_sparsity_info": [u64, i32p, i64p],
     "op2b_sparsity_arrays": [u64, u64p, u64p, u64p],
     "op2b_sparsity_free": [u64],
+    "op2b_incidence_build": [u64, i32, i32, i32, u64, u64p],
+    "op2b_incidence_arrays": [u64, u64p, u64p, i32p],
+    "op2b_incidence_free": [u64],
     "op2b_mat_zero_rows": [u64, u64, u64, i32p, i32, C.c_double, i32, u64],
     "op2b_mat_zero_rows_static": [u64, u64, u64, i32p, i32, C.c_double, i32, u64],
 }

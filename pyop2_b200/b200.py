@@ -439,6 +439,13 @@ class Sparsity(base.Sparsity):
         self._ensure()
         return self._d_nz_
 
+    def _max_row_nnz(self):
+        """Largest number of stored entries in one row."""
+        if getattr(self, "_max_nnz", None) is None:
+            rp = self._rowptr
+            self._max_nnz = int(np.diff(rp).max()) if rp.size > 1 else 0
+        return self._max_nnz
+
     @property
     def _o_nz(self):
         return 0
@@ -654,6 +661,34 @@ def Plan(kernel, iset, *args, **kwargs):
                       staging=st, thread_coloring=tc)
 
 
+# ---------------------------------------------------------------- incidence
+class Incidence(object):
+    """Target -> sorted (element, map index) list of a Map, on the device."""
+
+    def __init__(self, m):
+        h = C.c_uint64()
+        call("op2b_incidence_build", m._to_device().ptr, m.iterset.size, m.dim, m.dataset.total_size,
+             0, C.byref(h))
+        self._handle = h.value
+        p, lst, md = C.c_uint64(), C.c_uint64(), C.c_int32()
+        call("op2b_incidence_arrays", self._handle, C.byref(p), C.byref(lst), C.byref(md))
+        self.ptr, self.list, self.max_degree = p.value, lst.value, md.value
+
+    def __del__(self):
+        try:
+            if self._handle and _state['init']:
+                _lib._lib.op2b_incidence_free(self._handle)
+        except Exception:
+            pass
+
+
+def _incidence(m):
+    inc = getattr(m, "_incidence_cache", None)
+    if inc is None:
+        inc = m._incidence_cache = Incidence(m)
+    return inc
+
+
 # --------------------------------------------------------------- JIT cache
 _MODULES = {}
 
@@ -735,7 +770,7 @@ def _acc_name(acc):
     return acc._mode
 
 
-def loop_spec(loop, block_size=None, fmad=None):
+def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=None):
     """Static description of a par_loop: the LoopSpec of its stub plus the
     unique Dats/Maps/Mats/Globals, the INC staging pairs and the plan race
     groups.  Touches no device memory (used to generate and test stubs)."""
@@ -860,7 +895,25 @@ def loop_spec(loop, block_size=None, fmad=None):
                             [(st[0], st[1], st[2], st[3], tuple(st[4])) for st in stages],
                             bs, bool(cfg.cfg['fmad'] if fmad is None else fmad),
                             min_blocks=int(cfg.cfg['min_blocks_per_sm']))
-    if indirect and cfg.cfg['inc_mode'] == 'atomic' and codegen.atomic_capable(spec):
+    owner = None
+    om = cfg.cfg['owner_mode'] if owner_mode is None else owner_mode
+    if indirect and om != 'never':
+        nnz_max = mat_nnz_max
+        if nnz_max is None and mats:
+            nnz_max = mats[0].sparsity._max_row_nnz() if _state['init'] else 32
+        owner = codegen.owner_plan(spec, nnz_max)
+        if owner is not None and om == 'auto':
+            # redundant kernel evaluations (one per map index of an element)
+            # only pay where there are none: Mats and iteration-space INC
+            w = spec.args[owner["arg"]]
+            if owner["kind"] == "dat" and w.kind != "its":
+                owner = None
+    if owner is not None:
+        owner["kahan"] = bool(cfg.cfg['kahan'])
+        spec.owner = owner
+        spec.mode = "owner"
+        indirect = False
+    elif indirect and cfg.cfg['inc_mode'] == 'atomic' and codegen.atomic_capable(spec):
         spec.mode = "atomic"
         indirect = False   # launched like a direct loop: no plan
     gspecs = [s for s in specs if s.kind == "gbl"]
@@ -934,9 +987,19 @@ class _BoundLoop(object):
         vals["err"] = _state['err'].ptr
         self.vals = vals
         n = iterset.size
+        self.range_end = n
         if indirect:
             self.grid = 0
             self.max_grid = self.plan.max_blocks_per_color
+        elif spec.mode == "owner":
+            # one warp per target of the owner Map
+            omap = maps[spec.owner["mslot"]]
+            inc = _incidence(omap)
+            vals["inc_ptr"], vals["inc_list"] = inc.ptr, inc.list
+            self.range_end = omap.dataset.size
+            warps = self.range_end
+            self.grid = max(1, min((warps * 32 + bs - 1) // bs, _state['sm_count'] * 16)) if warps else 0
+            self.max_grid = self.grid
         else:
             self.grid = max(1, min((n + bs - 1) // bs, _state['sm_count'] * 8)) if n else 0
             self.max_grid = self.grid
@@ -984,7 +1047,7 @@ class _BoundLoop(object):
         n = self.iterset.size
         if n == 0:
             return
-        params = C.create_string_buffer(self.layout.pack(n, 0, n, vals), self.layout.nbytes)
+        params = C.create_string_buffer(self.layout.pack(n, 0, self.range_end, vals), self.layout.nbytes)
         if self.indirect:
             plan = self.plan
             call("op2b_launch_colored", mod.fn, plan.ncolors, plan.ncolblk_host, self.block_size,
@@ -1020,7 +1083,8 @@ class ParLoop(base.ParLoop):
                           a.access._mode))
         k.append(tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()))
         k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
-                  cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode']))
+                  cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode'], cfg.cfg['owner_mode'],
+                  cfg.cfg['kahan']))
         return tuple(k)
 
     def compute(self):

@@ -73,6 +73,7 @@ class LoopSpec(object):
         # 'direct': no Map; 'plan': coloured blocks of a GPU plan; 'atomic':
         # one grid-stride launch, INC args added with atomics
         self.mode = mode or ("plan" if indirect else "direct")
+        self.owner = None   # owner-computes description (mode 'owner')
         self.kernel_name = kernel_name
         self.kernel_code = kernel_code
         self.extents = tuple(extents)
@@ -92,7 +93,8 @@ class LoopSpec(object):
                 tuple(a.key() for a in self.args), tuple(self.dats), tuple(self.maps),
                 tuple(self.mats), tuple(self.gbls), tuple(self.consts), self.indirect,
                 tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
-                self.block_size, self.fmad, self.min_blocks, self.mode)
+                self.block_size, self.fmad, self.min_blocks, self.mode,
+                tuple(sorted(self.owner.items())) if self.owner else None)
 
     @property
     def needs_coloring(self):
@@ -109,6 +111,8 @@ class ParamLayout(object):
 
     def __init__(self, spec):
         f = []
+        if spec.mode == "owner":
+            f += ["inc_ptr", "inc_list"]
         if spec.mode == "plan":
             f += ["blkmap", "offset", "nelems", "nthrcol", "thrcol", "ind_map", "ind_sizes",
                   "ind_offs", "loc_map"]
@@ -141,7 +145,7 @@ def _struct_decl(spec, layout):
     types = {"blkmap": "const int *", "offset": "const int *", "nelems": "const int *",
              "nthrcol": "const int *", "thrcol": "const int *", "ind_map": "const int *",
              "ind_sizes": "const int *", "ind_offs": "const int *", "loc_map": "const short *",
-             "err": "int *"}
+             "err": "int *", "inc_ptr": "const int *", "inc_list": "const int *"}
     for n in layout.fields:
         if n in types:
             t = types[n]
@@ -210,9 +214,14 @@ def generate(spec):
             w("__constant__ %s %s[%d];" % (ctype, name, cdim))
     w(_struct_decl(spec, layout))
     w("#define OP2_STRIDE(a, idx) (a)[idx]")
+    # the user's code lives in its own namespace, so no local name of a stub
+    # can hide the kernel (the reference's tests call many kernels "k")
+    w("namespace op2b_user {")
     w(_mark_inline(spec.kernel_code, spec.kernel_name))
+    w("}  // namespace op2b_user")
     w("#undef OP2_STRIDE")
-    body = {"plan": _indirect_body, "atomic": _atomic_body, "direct": _direct_body}[spec.mode](spec)
+    body = {"plan": _indirect_body, "atomic": _atomic_body, "direct": _direct_body,
+            "owner": _owner_body}[spec.mode](spec)
     w(body)
     return "\n".join(out), layout, stub_name(spec)
 
@@ -273,7 +282,7 @@ def _direct_row(a, n, e, lines_pre, lines_post, indent):
 
 def _kernel_call(spec, argexprs, indent):
     itargs = ["i%d" % k for k in range(len(spec.extents))]
-    return "%s%s(%s);" % (indent, spec.kernel_name, ", ".join(argexprs + itargs))
+    return "%sop2b_user::%s(%s);" % (indent, spec.kernel_name, ", ".join(argexprs + itargs))
 
 
 def _direct_body(spec):
@@ -553,6 +562,218 @@ def _atomic_body(spec):
     _gbl_epilogue(spec, L)
     L.append("}")
     return "\n".join(L)
+
+
+def _owner_body(spec):
+    """Owner computes: one warp per target t of the owner Map (a row node of
+    the Mat, or an element of the INC Dat's set).  The warp walks t's
+    incidence list (flat map positions e*arity+k in ascending order), each lane
+    evaluating the kernel for one incident (e, k) and keeping only t's
+    contribution; the contributions are then added into the target's value(s),
+    held in registers, strictly in list order -- the order in which the
+    sequential backend adds them -- and the target is written once.  No
+    atomics, no colouring, deterministic."""
+    bs = spec.block_size
+    ow = spec.owner
+    A = ow["arity"]
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
+    _gbl_prologue(spec, L)
+    L.append("  const int lane = threadIdx.x & 31;")
+    L.append("  const op2b_i64 nwarps = ((op2b_i64)gridDim.x * %d) >> 5;" % bs)
+    L.append("  for (op2b_i64 t = ((op2b_i64)blockIdx.x * %d + threadIdx.x) >> 5; t < p.end; t += nwarps) {" % bs)
+    L.append("    const int p0 = p.inc_ptr[t], p1 = p.inc_ptr[t + 1];")
+    oarg = spec.args[ow["arg"]]
+    T = oarg.ctype
+    if ow["kind"] == "dat":
+        C = oarg.cdim
+        L.append("    __align__(16) %s acc[%d];" % (T, C))
+        L.append("    op2b_load<%s, %d, false>(acc, p.d%d + t * %d);" % (T, C, oarg.slot, C))
+    else:
+        NQ = ow["nq"]
+        j = oarg.slot
+        L.append("    const int r0 = p.mr%d[t], r1 = p.mr%d[t + 1];" % (j, j))
+        L.append("    %s acc[%d]; int cols[%d];" % (T, NQ, NQ))
+        L.append("    #pragma unroll")
+        L.append("    for (int q = 0; q < %d; ++q) {" % NQ)
+        L.append("      const int jj = r0 + lane + 32 * q;")
+        L.append("      cols[q] = jj < r1 ? p.mc%d[jj] : -1;" % j)
+        L.append("      acc[q] = jj < r1 ? p.mv%d[jj] : (%s)0;" % (j, T))
+        L.append("    }")
+    if ow.get("kahan"):
+        n_acc = C if ow["kind"] == "dat" else ow["nq"]
+        L.append("    %s comp[%d];" % (T, n_acc))
+        L.append("    for (int q = 0; q < %d; ++q) comp[q] = (%s)0;" % (n_acc, T))
+    L.append("    for (int base = p0; base < p1; base += 32) {")
+    L.append("      const int ii = base + lane;")
+    L.append("      const bool active = ii < p1;")
+    L.append("      const int pos = active ? p.inc_list[ii] : 0;")
+    L.append("      const op2b_i64 e = pos / %d;" % A)
+    L.append("      const int k = pos - (int)e * %d;" % A)
+    ind = "      "
+    # contribution registers
+    if ow["kind"] == "dat":
+        L.append("%s%s contrib[%d]; op2b_zero(contrib);" % (ind, T, oarg.cdim))
+    else:
+        E1 = spec.extents[1]
+        L.append("%s%s vv[%d]; int vc[%d];" % (ind, T, E1, E1))
+        L.append("%sfor (int q = 0; q < %d; ++q) { vv[q] = (%s)0; vc[q] = -2; }" % (ind, E1, T))
+    L.append("%sif (active) {" % ind)
+    ind2 = ind + "  "
+    used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
+                       {a.cmslot for a in spec.args if a.kind == "mat"})
+    for kk in used_maps:
+        ar = spec.maps[kk]
+        L.append("%s__align__(16) int mr%d[%d];" % (ind2, kk, ar))
+        L.append("%sop2b_load<int, %d, true>(mr%d, p.m%d + e * %d);" % (ind2, ar, kk, kk, ar))
+    pre, exprs, select = [], [], []
+    for n, a in enumerate(spec.args):
+        t, c = a.ctype, a.cdim
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n)
+        elif a.kind == "direct":
+            pre.append("%s__align__(16) %s a%d[%d];" % (ind2, t, n, c))
+            pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + e * %d);" % (ind2, t, c, _ro(a), n, a.slot, c))
+            exprs.append("a%d" % n)
+        elif a.kind == "ind":
+            pre.append("%s__align__(16) %s a%d[%d];" % (ind2, t, n, c))
+            if a.access == "INC":
+                pre.append("%sop2b_zero(a%d);" % (ind2, n))
+                select.append("%sif (k == %d) for (int q = 0; q < %d; ++q) contrib[q] += a%d[q];"
+                              % (ind2, a.idx, c, n))
+            else:
+                pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                           % (ind2, t, c, _ro(a), n, a.slot, a.mslot, a.idx, c))
+            exprs.append("a%d" % n)
+        elif a.kind == "vec":
+            cnt = a.arity
+            pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind2, t, n, cnt, c))
+            for r in range(cnt):
+                if a.access == "INC":
+                    pre.append("%sop2b_zero(a%d[%d]);" % (ind2, n, r))
+                    select.append("%sif (k == %d) for (int q = 0; q < %d; ++q) contrib[q] += a%d[%d][q];"
+                                  % (ind2, r, c, n, r))
+                else:
+                    pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                               % (ind2, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
+            pre.append("%s%s *a%d_v[%d] = {%s};" % (ind2, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
+            exprs.append("a%d_v" % n)
+        elif a.kind == "its":
+            if a.access == "INC":
+                # 1-d iteration space: the kernel runs once, at i0 = k
+                pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind2, t, n, c, n))
+                select.append("%sfor (int q = 0; q < %d; ++q) contrib[q] += a%d[q];" % (ind2, c, n))
+                exprs.append("a%d" % n)
+            else:
+                cnt = a.ext
+                pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind2, t, n, cnt, c))
+                for r in range(cnt):
+                    pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                               % (ind2, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
+                exprs.append("a%d[i%d]" % (n, a.idx))
+        elif a.kind == "mat":
+            pre.append("%s%s Aloc;" % (ind2, t))
+            exprs.append("(%s (*)[1])&Aloc" % t)
+    L += pre
+    if ow["kind"] == "dat":
+        nx = len(spec.extents)
+        if nx == 0:
+            L.append(_kernel_call(spec, exprs, ind2))
+        else:
+            L.append("%sconst int i0 = k;" % ind2)
+            L.append(_kernel_call(spec, exprs, ind2))
+        L += select
+    else:
+        E1 = spec.extents[1]
+        L.append("%sconst int i%d = k;" % (ind2, oarg.idx))
+        L.append("%s#pragma unroll" % ind2)
+        L.append("%sfor (int i%d = 0; i%d < %d; ++i%d) {" % (ind2, oarg.cidx, oarg.cidx, E1, oarg.cidx))
+        L.append("%s  Aloc = (%s)0;" % (ind2, T))
+        L.append(_kernel_call(spec, exprs, ind2 + "  "))
+        L.append("%s  vv[i%d] = Aloc; vc[i%d] = mr%d[i%d];" % (ind2, oarg.cidx, oarg.cidx, oarg.cmslot, oarg.cidx))
+        L.append("%s}" % ind2)
+    L.append("%s}" % ind)
+    # ordered accumulation over the lanes of this chunk
+    L.append("%sconst int nact = min(32, p1 - base);" % ind)
+    L.append("%sfor (int l = 0; l < nact; ++l) {" % ind)
+    kahan = ow.get("kahan")
+
+    def add(dst, val, q):
+        if not kahan:
+            return "%s += %s;" % (dst, val)
+        return ("{ %s y_ = %s - comp[%s]; %s t_ = %s + y_; comp[%s] = (t_ - %s) - y_; %s = t_; }"
+                % (T, val, q, T, dst, q, dst, dst))
+    if ow["kind"] == "dat":
+        L.append("%s  #pragma unroll" % ind)
+        L.append("%s  for (int q = 0; q < %d; ++q) { const %s v = __shfl_sync(OP2B_FULL_MASK, contrib[q], l); %s }"
+                 % (ind, oarg.cdim, T, add("acc[q]", "v", "q")))
+    else:
+        E1 = spec.extents[1]
+        ins = oarg.access == "WRITE"
+        L.append("%s  #pragma unroll" % ind)
+        L.append("%s  for (int i1 = 0; i1 < %d; ++i1) {" % (ind, E1))
+        L.append("%s    const %s v = __shfl_sync(OP2B_FULL_MASK, vv[i1], l);" % (ind, T))
+        L.append("%s    const int c = __shfl_sync(OP2B_FULL_MASK, vc[i1], l);" % ind)
+        L.append("%s    bool hit = false;" % ind)
+        L.append("%s    #pragma unroll" % ind)
+        if ins:
+            L.append("%s    for (int q = 0; q < %d; ++q) if (cols[q] == c) { acc[q] = v; hit = true; }"
+                     % (ind, ow["nq"]))
+        else:
+            L.append("%s    for (int q = 0; q < %d; ++q) if (cols[q] == c) { %s hit = true; }"
+                     % (ind, ow["nq"], add("acc[q]", "v", "q")))
+        # a column the row does not store: PETSc's NEW_NONZERO_ALLOCATION_ERR
+        L.append("%s    if (!__any_sync(OP2B_FULL_MASK, hit) && lane == 0) op2b_flag_missing(p.err, (int)t, c);"
+                 % ind)
+        L.append("%s  }" % ind)
+    L.append("%s}" % ind)
+    L.append("    }")
+    if ow["kind"] == "dat":
+        L.append("    if (lane == 0) op2b_store(p.d%d + t * %d, acc);" % (oarg.slot, oarg.cdim))
+    else:
+        j = oarg.slot
+        L.append("    #pragma unroll")
+        L.append("    for (int q = 0; q < %d; ++q) { const int jj = r0 + lane + 32 * q; if (jj < r1) p.mv%d[jj] = acc[q]; }"
+                 % (ow["nq"], j))
+        L.append("    if (lane == 0 && r1 - r0 > %d) atomicCAS(p.err + 3, 0, 1);" % (32 * ow["nq"]))
+    L.append("  }")
+    L.append("}")
+    return "\n".join(L)
+
+
+def owner_plan(spec, mat_row_nnz_max=None):
+    """The owner description of a loop if owner-computes applies, else None.
+
+    Applies when the loop's only writes are (a) INC into one Dat through one
+    Map ('ind' / vec-map args, or an iteration-space arg of a 1-d iteration
+    space), or (b) INC or WRITE into one scalar Mat through a 2-d iteration
+    space with rows on index i0 -- all other args READ, no Global reduction."""
+    writers = [n for n, a in enumerate(spec.args) if a.access != "READ"]
+    if not writers:
+        return None
+    kinds = {spec.args[n].kind for n in writers}
+    if kinds == {"mat"} and len(writers) == 1:
+        a = spec.args[writers[0]]
+        if a.rm * a.cm != 1 or len(spec.extents) != 2 or a.idx != 0 or a.cidx != 1:
+            return None
+        if a.access not in ("INC", "WRITE") or mat_row_nnz_max is None or mat_row_nnz_max > 64:
+            return None
+        if a.ext != a.arity or a.cext != a.carity:
+            return None
+        return {"kind": "mat", "arg": writers[0], "arity": a.arity, "mslot": a.mslot,
+                "nq": 1 if mat_row_nnz_max <= 32 else 2}
+    if not kinds <= {"ind", "vec", "its"}:
+        return None
+    ws = [spec.args[n] for n in writers]
+    if any(a.access != "INC" for a in ws):
+        return None
+    if len({(a.slot, a.mslot) for a in ws}) != 1:
+        return None
+    if any(a.kind == "its" for a in ws):
+        if len(spec.extents) != 1 or len(ws) != 1 or ws[0].idx != 0 or ws[0].ext != ws[0].arity:
+            return None
+    elif spec.extents:
+        return None
+    return {"kind": "dat", "arg": writers[0], "arity": ws[0].arity, "mslot": ws[0].mslot}
 
 
 def atomic_capable(spec):

@@ -19,7 +19,14 @@ keys of the B200 backend:
 * ``inc_mode``: how indirect loops resolve INC conflicts: ``'color'`` (plan
   with block and thread colouring; deterministic, bit-identical from run to
   run) or ``'atomic'`` (one launch, atomic adds; summation order varies
-  between runs within rounding).
+  between runs within rounding);
+* ``owner_mode``: owner-computes for loops whose only write is INC into one
+  Dat through one Map or into one scalar Mat: one warp per target adds the
+  target's contributions in the sequential backend's order and writes it once
+  (deterministic, no atomics).  ``'auto'`` uses it for Mats and 1-d
+  iteration-space INC (no redundant kernel evaluation), ``'always'`` also for
+  vec-map / indexed INC, ``'never'`` disables it;
+* ``kahan``: compensated (Kahan) summation of owner-computes accumulation.
 """
 
 import os
@@ -39,6 +46,8 @@ _defaults = {
     'l2_fetch_granularity': 32,
     'min_blocks_per_sm': 0,
     'inc_mode': 'atomic',
+    'owner_mode': 'auto',
+    'kahan': False,
 }
 
 _config = dict(_defaults)

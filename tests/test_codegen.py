@@ -142,7 +142,7 @@ def test_atomic_mode_stubs(host_op2, golden_matrices):
     mat = op2.Mat(op2.Sparsity((en, en)), np.float64)
     vmat = op2.Mat(op2.Sparsity((evn, evn)), np.float64)
     K = {k: op2.Kernel(v["code"], v["name"]) for k, v in golden_matrices["kernels"].items()}
-    cfg.configure(inc_mode="atomic")
+    cfg.configure(inc_mode="atomic", owner_mode="never")
     try:
         cases = [(K["mass"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.INC), coords(evn, op2.READ)),
                  (K["mass_vector_ffc"], el(3, 3), vmat((evn[op2.i[0]], evn[op2.i[1]]), op2.INC),
@@ -162,7 +162,45 @@ def test_atomic_mode_stubs(host_op2, golden_matrices):
                                            op2.Global(1, 1.0, np.float64)(op2.READ)))
         assert info["spec"].mode == "plan"
     finally:
-        cfg.configure(inc_mode="color")
+        cfg.configure(inc_mode="atomic", owner_mode="auto")
+
+
+def test_owner_mode_stubs(host_op2, golden_matrices):
+    """Owner-computes stubs: scalar Mat INC/WRITE, 1-d iteration-space Dat
+    INC, indexed / vec-map Dat INC (owner_mode='always'), with and without
+    Kahan compensation."""
+    op2 = host_op2
+    from pyop2_b200 import b200
+    from pyop2_b200 import configuration as cfg
+    el, nd, vnd = op2.Set(2), op2.Set(4), op2.Set(4, 2)
+    emap = np.asarray(golden_matrices["elem_node_map"], np.int32)
+    en = op2.Map(el, nd, 3, emap, "en_o")
+    evn = op2.Map(el, vnd, 3, emap, "evn_o")
+    coords, f = op2.Dat(vnd, np.zeros(8)), op2.Dat(nd, np.zeros(4))
+    b = op2.Dat(nd, np.zeros(4))
+    mat = op2.Mat(op2.Sparsity((en, en)), np.float64)
+    g = op2.Global(1, 1.0, np.float64)
+    K = {k: op2.Kernel(v["code"], v["name"]) for k, v in golden_matrices["kernels"].items()}
+    cases = [(K["mass"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.INC), coords(evn, op2.READ)),
+             (K["kernel_set"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.WRITE), g(op2.READ)),
+             (K["rhs_ffc_itspace"], el(3), b(en[op2.i[0]], op2.INC), coords(evn, op2.READ), f(en, op2.READ)),
+             (K["rhs"], el, b(en, op2.INC), coords(evn, op2.READ), f(en, op2.READ))]
+    for kahan in (False, True):
+        cfg.configure(owner_mode="always", kahan=kahan)
+        try:
+            for k, it, *args in cases:
+                info = b200.loop_spec(b200.ParLoop(k, it, *args), mat_nnz_max=16)
+                assert info["spec"].mode == "owner", k.name
+                src, layout, _ = nvrtc_compile(info["spec"])
+                assert "inc_list" in layout.fields
+                assert ("comp[" in src) == kahan
+        finally:
+            cfg.configure(owner_mode="auto", kahan=False)
+    # a Global reduction forbids owner-computes
+    red = op2.Global(1, 0.0, np.float64)
+    info = b200.loop_spec(b200.ParLoop(op2.Kernel("void kg(double *b, double *g) { }", "kg"), el,
+                                       b(en[0], op2.INC), red(op2.INC)))
+    assert info["spec"].mode != "owner"
 
 
 def test_param_layout_offsets():

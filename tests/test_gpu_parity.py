@@ -163,6 +163,52 @@ def test_p1_mass_rhs_matches_oracle(op2, n, inc_mode):
     assert rel_err(gb.data_ro, ob.data) < TOL
 
 
+def test_owner_mode_is_bit_exact(op2):
+    """Owner-computes adds each target's contributions in element order
+    starting from its current value -- the sequential backend's order -- so
+    the Mat, the RHS and the airfoil residual equal the oracle bit for bit."""
+    from pyop2_b200 import configuration as cfg
+    old = (cfg.cfg['owner_mode'], cfg.cfg['inc_mode'])
+    cfg.configure(owner_mode='always')
+    try:
+        coords, elem = meshes.square_p1(40)
+        fvals = np.sin(np.pi * coords[:, 0]) * np.sin(np.pi * coords[:, 1])
+        gm, gb, _ = _p1(op2, coords, elem, fvals)
+        om, ob, _ = _p1(seq, coords, elem, fvals)
+        np.testing.assert_array_equal(gm.array, om.array)
+        # the RHS kernel adds three quadrature terms per call: the sequential
+        # backend adds each into the global value, owner-computes sums them in
+        # the zeroed local first, so only rounding of those sums differs
+        assert rel_err(gb.data_ro, ob.data) < 1e-15
+        _clear_consts(op2)
+        grid = meshes.airfoil_grid(30, 16, 5)
+        G = airfoil.build(op2, 30, 16, 5, grid=grid)
+        O = airfoil.build(seq, 30, 16, 5, grid=grid)
+        for api, A in ((op2, G), (seq, O)):
+            airfoil.save_soln(api, A)
+            airfoil.adt_calc(api, A)
+            airfoil.res_calc(api, A)
+            airfoil.bres_calc(api, A)
+        np.testing.assert_array_equal(G.p_res.data_ro, O.p_res.data)
+    finally:
+        cfg.configure(owner_mode=old[0], inc_mode=old[1])
+        _clear_consts(op2)
+
+
+def test_owner_mode_kahan_matches(op2):
+    from pyop2_b200 import configuration as cfg
+    cfg.configure(kahan=True)
+    try:
+        coords, elem = meshes.square_p1(24)
+        fvals = coords[:, 0] + 2 * coords[:, 1]
+        gm, gb, _ = _p1(op2, coords, elem, fvals)
+        om, ob, _ = _p1(seq, coords, elem, fvals)
+        assert rel_err(gm.array, om.array) < 1e-15
+        assert rel_err(gb.data_ro, ob.data) < 1e-15
+    finally:
+        cfg.configure(kahan=False)
+
+
 def test_p1_mass_regression_golden(op2):
     """The 100x100 mass problem of the reference's regression test
     (test/regression/tests/mass2d_triangle): the golden's mesh numbering is
