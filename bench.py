@@ -372,6 +372,10 @@ def run_gpu(args, ws, rank, local):
                sum(v.nbytes for v in host.values()) + e2e_iters * 2 * 8)
         d2h = e2e_iters * 2 * 8 + q_out.nbytes
 
+    assembly = None
+    if not args.no_assembly:
+        assembly = bench_assembly(op2, b200)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         gbs, iters, nthreads, secs = cpu_airfoil(seconds=args.cpu_seconds, max_iters=50)
@@ -403,6 +407,7 @@ def run_gpu(args, ws, rank, local):
             "ms": round(e2e_ms, 3)},
         "clocks": clocks,
         "loops": breakdown,
+        "mat_assembly": assembly,
         "inc_mode": op2_cfg_inc_mode(),
         "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
     }
@@ -417,6 +422,95 @@ def run_gpu(args, ws, rank, local):
 def op2_cfg_inc_mode():
     from pyop2_b200 import configuration as cfg
     return cfg.cfg['inc_mode']
+
+
+def _timed(fn, reps, b200, flush=True):
+    """Median device time (ms) of fn() over reps runs, L2 flushed before each."""
+    ts = []
+    for _ in range(reps):
+        if flush:
+            b200.l2_flush()
+        e0 = b200.Event().record()
+        fn()
+        e1 = b200.Event().record()
+        e1.synchronize()
+        ts.append(e0.elapsed_ms(e1))
+    return statistics.median(ts)
+
+
+def bench_assembly(op2, b200, reps=5):
+    """Mat assembly legs: P1 256x256 mass + RHS and P2 1024x1024
+    stiffness + mass in FP64 and in the precision form (FP32 element math and
+    geometry, FP64 Kahan-compensated accumulation)."""
+    from pyop2_b200 import base
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import fem
+    out = {}
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    # ---- P1
+    P = fem.build_p1(op2, 256)
+    t0 = time.time()
+    nz = P.sparsity.nz
+    sp_s = time.time() - t0
+    fem.assemble_p1(op2, P)
+    b200.synchronize()
+
+    def mass():
+        op2.par_loop(P.k_mass, P.elements(3, 3),
+                     P.mat((P.elem_node[op2.i[0]], P.elem_node[op2.i[1]]), op2.INC),
+                     P.coords(P.elem_vnode, op2.READ))
+
+    def rhs():
+        op2.par_loop(P.k_rhs, P.elements(3), P.b(P.elem_node[op2.i[0]], op2.INC),
+                     P.coords(P.elem_vnode, op2.READ), P.f(P.elem_node, op2.READ))
+    ms_m = _timed(mass, reps, b200)
+    ms_r = _timed(rhs, reps, b200)
+    bm = fem.assembly_bytes(P.n_elem, 3, P.n_nodes, nz)
+    br = fem.rhs_bytes(P.n_elem, P.n_nodes)
+    out["p1_256"] = {"nnz": nz, "elements": P.n_elem, "sparsity_build_s": round(sp_s, 4),
+                     "mass_ms": round(ms_m, 4), "mass_nnz_per_s": round(nz / (ms_m * 1e-3), 1),
+                     "mass_GBps": round(bm / (ms_m * 1e-3) / 1e9, 1),
+                     "rhs_ms": round(ms_r, 4), "rhs_GBps": round(br / (ms_r * 1e-3) / 1e9, 1),
+                     "mode": "atomic"}
+    del P
+    # ---- P2, FP64 and precision form
+    res = {}
+    vals = {}
+    # default form (atomic accumulation), then the deterministic owner-computes
+    # form that sums in the sequential backend's order, with Kahan for FP32
+    variants = (("f64", "never", False), ("f32", "never", False),
+                ("f64", "auto", False), ("f32", "auto", True), ("f32g", "auto", True))
+    for prec, mode, kahan in variants:
+        tag = prec + ("_owner" if mode == "auto" else "") + ("_kahan" if kahan else "")
+        cfg.configure(kahan=kahan, owner_mode=mode)
+        Q = fem.build_p2(op2, 1024, seed=0, precision=prec)
+        t0 = time.time()
+        nz = Q.sparsity.nz
+        sp_s = time.time() - t0
+        fem.assemble_p2(op2, Q)   # compile, incidence, warm-up: values once
+        b200.synchronize()
+        vals[tag] = (Q.K.array, Q.M.array)
+        ms = _timed(lambda: fem.assemble_p2(op2, Q), reps, b200)
+        nbytes = fem.assembly_bytes(Q.n_elem, 6, Q.n_dofs, nz, 4 if prec == "f32g" else 8, nmats=2)
+        res[tag] = {"nnz": nz, "elements": Q.n_elem, "sparsity_build_s": round(sp_s, 3),
+                    "K_plus_M_ms": round(ms, 3), "nnz_per_s": round(2 * nz / (ms * 1e-3), 1),
+                    "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "algorithmic_bytes": nbytes,
+                    "kahan": kahan, "element_math": "f64" if prec == "f64" else "f32",
+                    "coordinates": "f32" if prec == "f32g" else "f64",
+                    "mode": "owner-computes" if mode == "auto" else "atomic"}
+        del Q
+    cfg.configure(kahan=False, owner_mode="never")
+    for tag in vals:
+        if tag == "f64_owner":
+            continue
+        for i, nm in enumerate(("K", "M")):
+            a, b = vals[tag][i], vals["f64_owner"][i]
+            res[tag]["max_rel_err_" + nm] = float(np.abs(a - b).max() / np.abs(b).max())
+    res["error_reference"] = ("max|A - A_f64| / max|A_f64| against the FP64 owner-computes assembly "
+                              "of the same Mat, which equals the sequential oracle bit for bit")
+    out["p2_1024"] = res
+    return out
 
 
 def _step_loops(A):
@@ -447,6 +541,7 @@ def main(argv=None):
     p.add_argument("--part-size", type=int, default=0, help="plan partition size (0: backend default)")
     p.add_argument("--block-size", type=int, default=0, help="threads per CTA (0: backend default)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    p.add_argument("--no-assembly", action="store_true", help="skip the Mat assembly legs")
     p.add_argument("--l2-fetch", type=int, default=-1,
                    help="L2 fetch granularity in bytes (32/64/128; 0 driver default; -1 backend default)")
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")

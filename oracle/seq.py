@@ -373,7 +373,7 @@ def _generate(kernel, extents, args, consts, openmp):
            "int oracle_csr_addto_scalar(double*, const int*, const int*, double, int, int, int);",
            "int oracle_csr_addto_block(double*, const int*, const int*, const double*, int, const int*, int, const int*, int);"]
     src += const_decl
-    src += ["#define OP2_STRIDE(a, idx) a[idx]", "static inline " + kernel.code.strip(), "#undef OP2_STRIDE"]
+    src += ["#define OP2_STRIDE(a, idx) a[idx]", _static_inline(kernel.code, kernel.name), "#undef OP2_STRIDE"]
     if not openmp:
         src.append("""
 int wrap(int start, int end, void **args, void **consts) {
@@ -433,6 +433,16 @@ int wrap(int part_size, int ncolors, const int *blkmap, const int *ncolblk, cons
 }""" % ("\n  ".join(decl), "\n  ".join(const_init), "\n  ".join(red_decl),
        "\n    ".join(red_init), "\n      ".join(ltens), body, "\n  ".join(red_fin)))
     return "\n".join(src)
+
+
+def _static_inline(code, name):
+    """The kernel code with its entry function made `static inline` (the
+    reference compiled it `inline`, pyop2/host.py:230-239)."""
+    import re
+    m = re.search(r"(^|[;}\s])(void\s+%s\s*\()" % re.escape(name), code)
+    if not m:
+        return code
+    return code[:m.start(2)] + "static inline " + code[m.start(2):]
 
 
 _MODCACHE = {}

@@ -603,10 +603,22 @@ def _owner_body(spec):
         n_acc = C if ow["kind"] == "dat" else ow["nq"]
         L.append("    %s comp[%d];" % (T, n_acc))
         L.append("    for (int q = 0; q < %d; ++q) comp[q] = (%s)0;" % (n_acc, T))
-    L.append("    for (int base = p0; base < p1; base += 32) {")
-    L.append("      const int ii = base + lane;")
-    L.append("      const bool active = ii < p1;")
-    L.append("      const int pos = active ? p.inc_list[ii] : 0;")
+    if ow["kind"] == "dat":
+        # one lane per incident (element, map index)
+        L.append("    for (int base = p0; base < p1; base += 32) {")
+        L.append("      const int ii = base + lane;")
+        L.append("      const bool active = ii < p1;")
+        L.append("      const int pos = active ? p.inc_list[ii] : 0;")
+    else:
+        # one lane per kernel call: (incident (element, row index), column index)
+        E1 = spec.extents[1]
+        L.append("    const int ncall = (p1 - p0) * %d;" % E1)
+        L.append("    for (int base = 0; base < ncall; base += 32) {")
+        L.append("      const int ci = base + lane;")
+        L.append("      const bool active = ci < ncall;")
+        L.append("      const int ii = p0 + ci / %d;" % E1)
+        L.append("      const int call_i1 = ci - (ci / %d) * %d;" % (E1, E1))
+        L.append("      const int pos = active ? p.inc_list[ii] : 0;")
     L.append("      const op2b_i64 e = pos / %d;" % A)
     L.append("      const int k = pos - (int)e * %d;" % A)
     ind = "      "
@@ -614,9 +626,7 @@ def _owner_body(spec):
     if ow["kind"] == "dat":
         L.append("%s%s contrib[%d]; op2b_zero(contrib);" % (ind, T, oarg.cdim))
     else:
-        E1 = spec.extents[1]
-        L.append("%s%s vv[%d]; int vc[%d];" % (ind, T, E1, E1))
-        L.append("%sfor (int q = 0; q < %d; ++q) { vv[q] = (%s)0; vc[q] = -2; }" % (ind, E1, T))
+        L.append("%s%s vv = (%s)0; int vc = -2;" % (ind, T, T))
     L.append("%sif (active) {" % ind)
     ind2 = ind + "  "
     used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
@@ -683,17 +693,17 @@ def _owner_body(spec):
             L.append(_kernel_call(spec, exprs, ind2))
         L += select
     else:
-        E1 = spec.extents[1]
         L.append("%sconst int i%d = k;" % (ind2, oarg.idx))
-        L.append("%s#pragma unroll" % ind2)
-        L.append("%sfor (int i%d = 0; i%d < %d; ++i%d) {" % (ind2, oarg.cidx, oarg.cidx, E1, oarg.cidx))
-        L.append("%s  Aloc = (%s)0;" % (ind2, T))
-        L.append(_kernel_call(spec, exprs, ind2 + "  "))
-        L.append("%s  vv[i%d] = Aloc; vc[i%d] = mr%d[i%d];" % (ind2, oarg.cidx, oarg.cidx, oarg.cmslot, oarg.cidx))
-        L.append("%s}" % ind2)
+        L.append("%sconst int i%d = call_i1;" % (ind2, oarg.cidx))
+        L.append("%sAloc = (%s)0;" % (ind2, T))
+        L.append(_kernel_call(spec, exprs, ind2))
+        L.append("%svv = Aloc; vc = mr%d[i%d];" % (ind2, oarg.cmslot, oarg.cidx))
     L.append("%s}" % ind)
     # ordered accumulation over the lanes of this chunk
-    L.append("%sconst int nact = min(32, p1 - base);" % ind)
+    if ow["kind"] == "dat":
+        L.append("%sconst int nact = min(32, p1 - base);" % ind)
+    else:
+        L.append("%sconst int nact = min(32, ncall - base);" % ind)
     L.append("%sfor (int l = 0; l < nact; ++l) {" % ind)
     kahan = ow.get("kahan")
 
@@ -707,12 +717,10 @@ def _owner_body(spec):
         L.append("%s  for (int q = 0; q < %d; ++q) { const %s v = __shfl_sync(OP2B_FULL_MASK, contrib[q], l); %s }"
                  % (ind, oarg.cdim, T, add("acc[q]", "v", "q")))
     else:
-        E1 = spec.extents[1]
         ins = oarg.access == "WRITE"
-        L.append("%s  #pragma unroll" % ind)
-        L.append("%s  for (int i1 = 0; i1 < %d; ++i1) {" % (ind, E1))
-        L.append("%s    const %s v = __shfl_sync(OP2B_FULL_MASK, vv[i1], l);" % (ind, T))
-        L.append("%s    const int c = __shfl_sync(OP2B_FULL_MASK, vc[i1], l);" % ind)
+        L.append("%s  {" % ind)
+        L.append("%s    const %s v = __shfl_sync(OP2B_FULL_MASK, vv, l);" % (ind, T))
+        L.append("%s    const int c = __shfl_sync(OP2B_FULL_MASK, vc, l);" % ind)
         L.append("%s    bool hit = false;" % ind)
         L.append("%s    #pragma unroll" % ind)
         if ins:

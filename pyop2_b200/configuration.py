@@ -23,9 +23,12 @@ keys of the B200 backend:
 * ``owner_mode``: owner-computes for loops whose only write is INC into one
   Dat through one Map or into one scalar Mat: one warp per target adds the
   target's contributions in the sequential backend's order and writes it once
-  (deterministic, no atomics).  ``'auto'`` uses it for Mats and 1-d
-  iteration-space INC (no redundant kernel evaluation), ``'always'`` also for
-  vec-map / indexed INC, ``'never'`` disables it;
+  (deterministic, no atomics, bit-identical to the sequential backend's
+  order).  ``'auto'`` uses it for Mats and 1-d iteration-space INC (no
+  redundant kernel evaluation), ``'always'`` also for vec-map / indexed INC,
+  ``'never'`` (default) leaves those loops to ``inc_mode``.  It is slower than
+  the atomic form where kernels index tables with the iteration-space index
+  (the index becomes a run-time value per lane);
 * ``kahan``: compensated (Kahan) summation of owner-computes accumulation.
 """
 
@@ -46,7 +49,7 @@ _defaults = {
     'l2_fetch_granularity': 32,
     'min_blocks_per_sm': 0,
     'inc_mode': 'atomic',
-    'owner_mode': 'auto',
+    'owner_mode': 'never',
     'kahan': False,
 }
 

@@ -197,7 +197,7 @@ def test_owner_mode_is_bit_exact(op2):
 
 def test_owner_mode_kahan_matches(op2):
     from pyop2_b200 import configuration as cfg
-    cfg.configure(kahan=True)
+    cfg.configure(kahan=True, owner_mode='auto')
     try:
         coords, elem = meshes.square_p1(24)
         fvals = coords[:, 0] + 2 * coords[:, 1]
@@ -206,7 +206,7 @@ def test_owner_mode_kahan_matches(op2):
         assert rel_err(gm.array, om.array) < 1e-15
         assert rel_err(gb.data_ro, ob.data) < 1e-15
     finally:
-        cfg.configure(kahan=False)
+        cfg.configure(kahan=False, owner_mode='never')
 
 
 def test_p1_mass_regression_golden(op2):
