@@ -1,6 +1,6 @@
 """Benchmark of the B200 PyOP2 backend on the airfoil loop chain.
 
-Workload (BASELINE configs[1]): the airfoil finite-volume chain on a synthetic
+Workload: the airfoil finite-volume chain on a synthetic
 1200 x 600 quad mesh (720,000 cells, 1,438,200 interior edges, 3,600 boundary
 edges) with randomly permuted cell and node numbering, FP64.  One step = one
 outer iteration: save_soln, then twice (adt_calc, res_calc, bres_calc, update
@@ -153,15 +153,17 @@ def _bytes():
 
 
 def _traffic_from_profile():
-    """dram bytes (read+write) per res_calc launch from the committed ncu
-    summary, if one exists."""
-    p = os.path.join(HERE, "profiles", "ncu_metrics.json")
+    """DRAM bytes (read + write) per res_calc launch from the committed ncu
+    summary of that kernel, if one exists."""
+    p = os.path.join(HERE, "profiles", "res_calc_airfoil_1200x600.md")
     try:
         with open(p) as f:
-            d = json.load(f)
-        return d.get("res_calc_airfoil_1200x600", {}).get("dram_bytes_per_launch")
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1])
     except (OSError, ValueError):
-        return None
+        pass
+    return None
 
 
 def _peaks():
@@ -175,7 +177,16 @@ def _peaks():
 
 
 # ----------------------------------------------------------------- CPU leg
-def cpu_airfoil(seconds=20.0, max_iters=50, threads=None):
+def workload_config(ws):
+    """The workload both arms run (rank-independent description)."""
+    return {"workload": "airfoil 1200x600 (720000 cells, 1438200 edges, 3600 boundary "
+                        "edges), permuted numbering, FP64, one outer iteration (9 "
+                        "par_loops) per step",
+            "bytes_per_step": _bytes()["iteration"], "global_batch": ws, "seq_len": 0,
+            "parallelism": "replicas" if ws > 1 else "single"}
+
+
+def cpu_airfoil(seconds=20.0, max_iters=50, threads=None, warmup=1):
     """Restated OpenMP backend on the full mesh: iterations until ~seconds of
     element-loop time; returns (GB/s, iterations, threads, loop seconds)."""
     from oracle import seq
@@ -193,7 +204,8 @@ def cpu_airfoil(seconds=20.0, max_iters=50, threads=None):
         return orig(*a, openmp=True, part_size=1024, timer=lambda dt: loop_time.__setitem__(0, loop_time[0] + dt), **k)
     seq.par_loop = timed
     try:
-        airfoil.iteration(seq, A)  # compile + plan, not timed
+        for _ in range(max(1, warmup)):  # compile + plan, not timed
+            airfoil.iteration(seq, A)
         loop_time[0] = 0.0
         iters = 0
         while iters < max_iters and (loop_time[0] < seconds or iters == 0):
@@ -214,15 +226,15 @@ def run_reference(args, ws, rank, local):
     steps = max(1, args.steps)
     bpi = _bytes()["iteration"]
     # bounded: about 60 s of element-loop work in total
-    gbs, iters, nthreads, secs = cpu_airfoil(seconds=min(60.0, 2.0 * steps), max_iters=steps)
+    gbs, iters, nthreads, secs = cpu_airfoil(seconds=min(60.0, 2.0 * steps), max_iters=steps,
+                                             warmup=args.warmup)
     line = {"metric": "par_loop achieved HBM GB/s (airfoil chain)", "value": round(gbs, 3),
-            "unit": "GB/s", "n_gpus": ws, "steps": iters, "warmup": 1,
+            "unit": "GB/s", "n_gpus": ws, "steps": iters, "warmup": args.warmup,
             "ms_per_step": round(1e3 * secs / iters, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "airfoil 1200x600, permuted numbering, FP64, one outer "
-                                   "iteration per step", "global_batch": 1, "seq_len": 0,
-                       "parallelism": "replicas"},
+            "config": dict(workload_config(ws),
+                           timing="host wall clock around each element loop, rank 0 only"),
             "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads,
                              "kind": "port",
                              "sample": "%d airfoil iterations of the 1200x600 mesh, restated "
@@ -252,6 +264,12 @@ def run_gpu(args, ws, rank, local):
     if args.inc_mode:
         opts["inc_mode"] = args.inc_mode
     op2.init(backend="b200", device=local, **opts)
+    if args.assembly_only:
+        # the Mat assembly legs alone (profiling their kernels); not a bench line
+        if rank == 0:
+            print(json.dumps({"mat_assembly": bench_assembly(op2, b200)}))
+        d.close()
+        return 0
     bytes_ = _bytes()
     bpi = bytes_["iteration"]
     grid = airfoil_grid(NX, NY, SEED, permute=not args.no_permute)
@@ -300,36 +318,42 @@ def run_gpu(args, ws, rank, local):
     value = ws * bpi * args.steps / (total_ms * 1e-3) / 1e9
     final_rms = float(np.sqrt(rms.data[0] / grid.ncells))
 
-    # ---------------- roofline: res_calc alone, per launch
-    res_ms = []
-    for _ in range(max(3, min(args.steps, 20))):
-        b200.l2_flush()
-        e0 = b200.Event().record()
-        airfoil.res_calc(op2, A)
-        e1 = b200.Event().record()
-        e1.synchronize()
-        res_ms.append(e0.elapsed_ms(e1))
-    res_avg = statistics.mean(res_ms)
+    # ---------------- roofline: res_calc alone, per launch; and per-loop
+    # breakdown.  Each loop is replayed from its own CUDA graph right after an
+    # L2 flush, so no host-side launch cost falls between the events.
+    loop_fns = (("save_soln", lambda: airfoil.save_soln(op2, A)),
+                ("adt_calc", lambda: airfoil.adt_calc(op2, A)),
+                ("res_calc", lambda: airfoil.res_calc(op2, A)),
+                ("bres_calc", lambda: airfoil.bres_calc(op2, A)),
+                ("update", lambda: airfoil.update(op2, A, rms)))
     breakdown = {}
-    for name, fn in (("save_soln", lambda: airfoil.save_soln(op2, A)),
-                     ("adt_calc", lambda: airfoil.adt_calc(op2, A)),
-                     ("res_calc", lambda: airfoil.res_calc(op2, A)),
-                     ("bres_calc", lambda: airfoil.bres_calc(op2, A)),
-                     ("update", lambda: airfoil.update(op2, A, rms))):
+    res_avg = None
+    for name, fn in loop_fns:
+        with b200.capture() as g1:
+            fn()
+        reps = 20
+        for _ in range(3):
+            g1.launch()
         ts = []
-        for _ in range(5):
+        for _ in range(reps):
             b200.l2_flush()
             e0 = b200.Event().record()
-            fn()
+            g1.launch()
             e1 = b200.Event().record()
             e1.synchronize()
             ts.append(e0.elapsed_ms(e1))
+        g1.close()
         ms = statistics.median(ts)
+        if name == "res_calc":
+            res_avg = statistics.mean(ts)
         breakdown[name] = {"ms": round(ms, 4), "GB/s": round(bytes_[name] / (ms * 1e-3) / 1e9, 1)}
     res_bytes = bytes_["res_calc"]
     peak, peak_kind = _peaks()
     achieved = res_bytes / (res_avg * 1e-3) / 1e9
-    traffic = _traffic_from_profile()
+    # the committed capture covers the default workload in the default INC mode
+    default_run = ((NX, NY) == (1200, 600) and op2_cfg_inc_mode() == "atomic"
+                   and not args.no_permute and not args.block_size and not args.part_size)
+    traffic = _traffic_from_profile() if default_run else None
 
     e2e_val = e2e_ms = h2d = d2h = None
     e2e_iters = args.steps
@@ -388,15 +412,13 @@ def run_gpu(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "airfoil 1200x600 (720000 cells, 1438200 edges, 3600 boundary "
-                               "edges), permuted numbering, FP64, one outer iteration (9 "
-                               "par_loops) per step",
-                   "bytes_per_step": bpi, "global_batch": ws, "seq_len": 0,
-                   "parallelism": "replicas" if ws > 1 else "single",
-                   "l2": "flushed (256 MB write) before every step", "timing": "CUDA graph "
-                   "replay, CUDA events per step on the op2 stream, max over ranks"},
+        "config": dict(workload_config(ws),
+                       l2="flushed (256 MB write) before every step",
+                       timing="CUDA graph replay, CUDA events per step on the op2 stream, "
+                              "max over ranks"),
         "gpu_launches": launches * args.steps,
-        "roofline": {"kernel": "res_calc (all colour launches)", "bound": "hbm",
+        "roofline": {"kernel": "res_calc (%s)" % ("one atomic launch" if op2_cfg_inc_mode() == "atomic"
+                                                  else "all colour launches"), "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "algorithmic_bytes": res_bytes, "avg_ms": round(res_avg, 4),
@@ -439,9 +461,9 @@ def _timed(fn, reps, b200, flush=True):
 
 
 def bench_assembly(op2, b200, reps=5):
-    """Mat assembly legs: P1 256x256 mass + RHS (configs[0]) and P2 1024x1024
+    """Mat assembly legs: P1 256x256 mass + RHS and P2 1024x1024
     stiffness + mass in FP64 and in the precision form (FP32 element math and
-    geometry, FP64 Kahan-compensated accumulation) (configs[2])."""
+    geometry, FP64 Kahan-compensated accumulation)."""
     from pyop2_b200 import base
     from pyop2_b200 import configuration as cfg
     from pyop2_b200.workloads import fem
@@ -542,6 +564,8 @@ def main(argv=None):
     p.add_argument("--block-size", type=int, default=0, help="threads per CTA (0: backend default)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     p.add_argument("--no-assembly", action="store_true", help="skip the Mat assembly legs")
+    p.add_argument("--assembly-only", action="store_true",
+                   help="run only the Mat assembly legs and print their figures")
     p.add_argument("--l2-fetch", type=int, default=-1,
                    help="L2 fetch granularity in bytes (32/64/128; 0 driver default; -1 backend default)")
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")

@@ -1154,6 +1154,12 @@ class Graph(object):
     def launch(self):
         call("op2b_graph_launch", self.handle, 0)
 
+    def close(self):
+        """Destroy the executable graph now rather than at collection."""
+        if self.handle and _state['init']:
+            h, self.handle = self.handle, 0
+            call("op2b_graph_destroy", h)
+
     def __del__(self):
         try:
             if self.handle and _state['init']:

@@ -4,9 +4,9 @@ Kernels are written for this package in the form the reference's FFC
 kernels take (pyop2 test/unit/test_matrices.py:273-377): one local matrix
 entry per call through a 2-d iteration space, coordinates through a vec-map.
 
-* P1 (configs[0]): mass matrix with the 3-point rule (basis values 2/3, 1/6,
+* P1: mass matrix with the 3-point rule (basis values 2/3, 1/6,
   weights 1/6), RHS of f at the same points.
-* P2 (configs[2]): quadratic Lagrange basis, local order (v0, v1, v2, m12, m02,
+* P2: quadratic Lagrange basis, local order (v0, v1, v2, m12, m02,
   m01); stiffness with the degree-2 three-point rule (exact for products of
   linear gradients), mass with Dunavant's degree-4 six-point rule.  The FP64
   kernels compute in double; the precision form computes in float on float
@@ -135,7 +135,7 @@ class Problem(object):
 
 
 def build_p1(op2, n, coords=None, elem=None):
-    """P1 mass Mat + RHS Dat on the n x n square (configs[0]: n = 256)."""
+    """P1 mass Mat + RHS Dat on the n x n square."""
     if coords is None:
         coords, elem = square_p1(n)
     P = Problem()
@@ -164,7 +164,7 @@ def assemble_p1(op2, P):
 
 
 def build_p2(op2, n, seed=0, precision="f64", coords=None, elem=None):
-    """P2 stiffness + mass Mats on one Sparsity (configs[2]: n = 1024)."""
+    """P2 stiffness + mass Mats on one Sparsity."""
     if coords is None:
         coords, elem = square_p2(n, seed)
     P = Problem()
