@@ -548,6 +548,11 @@ class Solver(base.Solver):
         raise NotImplementedError("The linear solve is not part of the B200 backend's hot path")
 
 
+def solve(M, x, b):
+    """op2.solve (pyop2/op2.py: solve): not provided by this backend."""
+    Solver().solve(M, x, b)
+
+
 # ------------------------------------------------------------------- plans
 _PLAN_CACHE = {}
 
