@@ -270,6 +270,11 @@ def run_gpu(args, ws, rank, local):
             print(json.dumps({"mat_assembly": bench_assembly(op2, b200)}))
         d.close()
         return 0
+    if args.batching_only:
+        if rank == 0:
+            print(json.dumps({"batching": bench_batching(op2, b200, args.batch_meshes or 4096)}))
+        d.close()
+        return 0
     bytes_ = _bytes()
     bpi = bytes_["iteration"]
     grid = airfoil_grid(NX, NY, SEED, permute=not args.no_permute)
@@ -399,6 +404,9 @@ def run_gpu(args, ws, rank, local):
     assembly = None
     if not args.no_assembly:
         assembly = bench_assembly(op2, b200)
+    batching = None
+    if args.batch_meshes > 0:
+        batching = bench_batching(op2, b200, args.batch_meshes)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -430,6 +438,7 @@ def run_gpu(args, ws, rank, local):
         "clocks": clocks,
         "loops": breakdown,
         "mat_assembly": assembly,
+        "batching": batching,
         "inc_mode": op2_cfg_inc_mode(),
         "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
     }
@@ -458,6 +467,97 @@ def _timed(fn, reps, b200, flush=True):
         e1.synchronize()
         ts.append(e0.elapsed_ms(e1))
     return statistics.median(ts)
+
+
+def bench_batching(op2, b200, nmesh, reps=5, seed=0):
+    """Batching form: nmesh uneven P1 meshes (elements log-uniform in
+    [2^8, 2^16], random aspect ratio, permuted numbering), each with mass and
+    stiffness Mat assembly and an RHS INC loop.
+
+    * batched: the three loops of all meshes as three tuned BatchLoops (one
+      persistent launch each) recorded in one CUDA graph, replayed after an
+      L2 flush, CUDA events around the replay;
+    * plain: the same 3 x nmesh loops issued one by one through
+      op2.par_loop (objects already resident, stubs compiled), CUDA events
+      around the whole sequence (the device timeline, host gaps included).
+    Requests = meshes.  Parity: the batched Mats and RHS of sample meshes
+    against the plain path's."""
+    from pyop2_b200 import autotune
+    from pyop2_b200.workloads import batching
+    t0 = time.time()
+    shapes = batching.mesh_shapes(nmesh, seed)
+    probs = batching.build(op2, shapes, seed)
+    mass, stiff, rhs = batching.instances(op2, probs)
+    setup_s = time.time() - t0
+    elements = sum(P.n_elem for P in probs)
+    nbytes = sum(batching.bytes_per_mesh(P) for P in probs)
+    nnz = sum(int(P.sparsity.nz) for P in probs)
+    t1 = time.time()
+    loops, tuned = [], {}
+    for name, insts in (("mass", mass), ("stiffness", stiff), ("rhs", rhs)):
+        best, times = autotune.tune(insts, reps=3)
+        tuned[name] = {"best": best, "candidates_ms": times}
+        from pyop2_b200.batch import BatchLoop
+        loops.append(BatchLoop(insts, **best))
+    tune_s = time.time() - t1
+    for bl in loops:
+        bl.launch()
+    b200.synchronize()
+    with b200.capture() as g:
+        for bl in loops:
+            bl.launch(sync_host=False)
+    for _ in range(3):
+        g.launch()
+    ts = []
+    for _ in range(reps):
+        b200.l2_flush()
+        e0 = b200.Event().record()
+        g.launch()
+        e1 = b200.Event().record()
+        e1.synchronize()
+        ts.append(e0.elapsed_ms(e1))
+    batched_ms = statistics.median(ts)
+    # plain per-loop form: warm (stubs, bound loops), then timed
+    for P in probs:
+        batching.plain(op2, P)
+    b200.synchronize()
+    pts = []
+    for _ in range(2):
+        b200.l2_flush()
+        e0 = b200.Event().record()
+        for P in probs:
+            batching.plain(op2, P)
+        e1 = b200.Event().record()
+        e1.synchronize()
+        pts.append(e0.elapsed_ms(e1))
+    plain_ms = min(pts)
+    # parity on sample meshes: zero, batched graph once, keep; zero, plain
+    sample = sorted({0, nmesh // 2, nmesh - 1, int(np.argmax([P.n_elem for P in probs]))})
+    for P in probs:
+        P.mat.zero(); P.stiff.zero(); P.b.zero()
+    g.launch()
+    got = {i: (probs[i].mat.array.copy(), probs[i].stiff.array.copy(), probs[i].b.data_ro.copy())
+           for i in sample}
+    err = 0.0
+    for i in sample:
+        P = probs[i]
+        P.mat.zero(); P.stiff.zero(); P.b.zero()
+        batching.plain(op2, P)
+        for a, b in zip(got[i], (P.mat.array, P.stiff.array, P.b.data_ro)):
+            err = max(err, float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)))
+    g.close()
+    return {"meshes": nmesh, "elements": elements, "nnz_per_mat": nnz,
+            "loops_per_mesh": 3, "algorithmic_bytes": nbytes,
+            "batched_ms": round(batched_ms, 4),
+            "batched_req_per_s": round(nmesh / (batched_ms * 1e-3), 1),
+            "batched_GBps": round(nbytes / (batched_ms * 1e-3) / 1e9, 1),
+            "batched_launches": sum(bl.launches for bl in loops),
+            "plain_ms": round(plain_ms, 2),
+            "plain_req_per_s": round(nmesh / (plain_ms * 1e-3), 1),
+            "plain_launches": 3 * nmesh,
+            "speedup_req_per_s": round(plain_ms / batched_ms, 1),
+            "max_rel_err_vs_plain": err, "parity_sample_meshes": sample,
+            "autotune": tuned, "setup_s": round(setup_s, 1), "tune_s": round(tune_s, 1)}
 
 
 def bench_assembly(op2, b200, reps=5):
@@ -566,6 +666,10 @@ def main(argv=None):
     p.add_argument("--no-assembly", action="store_true", help="skip the Mat assembly legs")
     p.add_argument("--assembly-only", action="store_true",
                    help="run only the Mat assembly legs and print their figures")
+    p.add_argument("--batch-meshes", type=int, default=4096,
+                   help="meshes of the batching leg (0 skips it)")
+    p.add_argument("--batching-only", action="store_true",
+                   help="run only the batching leg and print its figures")
     p.add_argument("--l2-fetch", type=int, default=-1,
                    help="L2 fetch granularity in bytes (32/64/128; 0 driver default; -1 backend default)")
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")

@@ -113,6 +113,10 @@ int op2b_module_function(uint64_t module, const char *name, uint64_t *fn);
  * (Const._to_device, pyop2/cuda.py:314-320). */
 int op2b_module_global(uint64_t module, const char *name, uint64_t *dptr, uint64_t *bytes);
 int op2b_function_set_smem(uint64_t fn, int32_t bytes);
+/* Resident CTAs per SM of fn at the given block size and dynamic shared
+ * memory, for sizing persistent grids (batched loops).  No reference
+ * counterpart (the reference launched one CTA per plan block). */
+int op2b_function_occupancy(uint64_t fn, uint32_t block, uint32_t smem, int32_t *blocks_per_sm);
 /* Launch fn with ONE by-value parameter: the packed struct params[0..nbytes).
  * The generated stubs all take a single struct argument. */
 int op2b_launch(uint64_t fn, uint32_t grid, uint32_t block, uint32_t smem,
@@ -207,6 +211,15 @@ int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx,
                        const int32_t *rows, int32_t nrows_zero, double diag,
                        int32_t elem_bytes, uint64_t stream);
 
+/* Scatter-slot table of a scalar Mat assembled through the Map pair
+ * (rmap [nelem][ra], cmap [nelem][ca]): slots[(r*ca + c)*nelem + e] is the
+ * CSR position of (rmap[e][r], cmap[e][c]), or -1 where the Sparsity has no
+ * such entry.  slots holds nelem*ra*ca int32.  The assembly stubs read it
+ * instead of searching the row for every entry.  No direct reference
+ * counterpart: it replaces the per-entry row search of the LMA-to-CSR scatter
+ * (assets/cuda_matrix_support.jinja2:27-81) and PETSc's MatSetValues lookup. */
+int op2b_mat_slots_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64_t cmap,
+                         int64_t nelem, int32_t ra, int32_t ca, uint64_t slots, uint64_t stream);
 /* op2b_mat_zero_rows for callers that must not allocate device memory.
  * No counterpart in the reference.
  *

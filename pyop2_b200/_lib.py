@@ -57,6 +57,7 @@ _SIGS = {
     "op2b_module_function": [u64, charp, u64p],
     "op2b_module_global": [u64, charp, u64p, u64p],
     "op2b_function_set_smem": [u64, i32],
+    "op2b_function_occupancy": [u64, u32, u32, i32p],
     "op2b_launch": [u64, u32, u32, u32, u64, P, u64],
     "op2b_launch_colored": [u64, i32, i32p, u32, u32, u64, P, u64, u64],
     "op2b_plan_build": [i32, i32, i32, u64p, i32p, i32p, i32p, i32p, i32p,
@@ -73,6 +74,7 @@ _SIGS = {
     "op2b_incidence_arrays": [u64, u64p, u64p, i32p],
     "op2b_incidence_free": [u64],
     "op2b_mat_zero_rows": [u64, u64, u64, i32p, i32, C.c_double, i32, u64],
+    "op2b_mat_slots_build": [u64, u64, u64, u64, i64, i32, i32, u64, u64],
     "op2b_mat_zero_rows_static": [u64, u64, u64, i32p, i32, C.c_double, i32, u64],
 }
 

@@ -439,6 +439,22 @@ class Sparsity(base.Sparsity):
         self._ensure()
         return self._d_nz_
 
+    def _slot_table(self, rmap, cmap):
+        """Scatter-slot table of scalar assembly through (rmap, cmap): the
+        CSR position of every element's (r, c) entry, built on the device at
+        first use and kept with the Sparsity (op2b_mat_slots_build)."""
+        tables = self.__dict__.setdefault("_slot_tables", {})
+        key = (id(rmap), id(cmap))
+        hit = tables.get(key)
+        if hit is not None:
+            return hit[0]
+        n = rmap.iterset.size
+        buf = DeviceBuffer(max(1, n * rmap.dim * cmap.dim) * 4)
+        call("op2b_mat_slots_build", self._d_rowptr, self._d_colidx, rmap._to_device().ptr,
+             cmap._to_device().ptr, n, rmap.dim, cmap.dim, buf.ptr, 0)
+        tables[key] = (buf, rmap, cmap)
+        return buf
+
     def _max_row_nnz(self):
         """Largest number of stored entries in one row."""
         if getattr(self, "_max_nnz", None) is None:
@@ -720,11 +736,20 @@ class _Module(object):
         h = C.c_uint64()
         call("op2b_module_load", cubin, C.byref(h))
         self.handle = h.value
-        fn = C.c_uint64()
-        call("op2b_module_function", self.handle, stub.encode(), C.byref(fn))
-        self.fn = fn.value
+        self.fn = self.function(stub)
         self.smem_set = 48 * 1024
         self.const_versions = {}
+
+    def function(self, name):
+        fn = C.c_uint64()
+        call("op2b_module_function", self.handle, name.encode(), C.byref(fn))
+        return fn.value
+
+    def occupancy(self, fn, block, smem=0):
+        """Resident CTAs per SM of a function of this module."""
+        n = C.c_int32()
+        call("op2b_function_occupancy", fn, block, smem, C.byref(n))
+        return n.value
 
     def const_ptr(self, name):
         p, n = C.c_uint64(), C.c_uint64()
@@ -775,7 +800,30 @@ def _acc_name(acc):
     return acc._mode
 
 
-def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=None):
+def _slots_usable(specs):
+    """Scatter-slot tables serve a loop whose Mats are scalar and each
+    assembled through one (row Map, column Map) pair."""
+    pairs = {}
+    for s in specs:
+        if s.kind == "mat":
+            if s.rm * s.cm != 1:
+                return False
+            pairs.setdefault(s.slot, set()).add((s.mslot, s.cmslot))
+    return bool(pairs) and all(len(v) == 1 for v in pairs.values())
+
+
+def mat_slot_values(specs, maps, mats):
+    """Parameter values ms<j>: the scatter-slot table of each Mat slot."""
+    vals = {}
+    for s in specs:
+        if s.kind == "mat" and "ms%d" % s.slot not in vals:
+            m = mats[s.slot]
+            vals["ms%d" % s.slot] = m.sparsity._slot_table(maps[s.mslot], maps[s.cmslot]).ptr
+    return vals
+
+
+def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=None,
+              inc_mode=None, min_blocks=None):
     """Static description of a par_loop: the LoopSpec of its stub plus the
     unique Dats/Maps/Mats/Globals, the INC staging pairs and the plan race
     groups.  Touches no device memory (used to generate and test stubs)."""
@@ -899,7 +947,8 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
                             consts, indirect,
                             [(st[0], st[1], st[2], st[3], tuple(st[4])) for st in stages],
                             bs, bool(cfg.cfg['fmad'] if fmad is None else fmad),
-                            min_blocks=int(cfg.cfg['min_blocks_per_sm']))
+                            min_blocks=int(cfg.cfg['min_blocks_per_sm'] if min_blocks is None
+                                           else min_blocks))
     owner = None
     om = cfg.cfg['owner_mode'] if owner_mode is None else owner_mode
     if indirect and om != 'never':
@@ -918,13 +967,29 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
         spec.owner = owner
         spec.mode = "owner"
         indirect = False
-    elif indirect and cfg.cfg['inc_mode'] == 'atomic' and codegen.atomic_capable(spec):
+    elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'atomic' and codegen.atomic_capable(spec):
         spec.mode = "atomic"
         indirect = False   # launched like a direct loop: no plan
+        spec.mat_slots = bool(cfg.cfg['mat_slots']) and _slots_usable(specs)
     gspecs = [s for s in specs if s.kind == "gbl"]
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
                 iterset=iterset, block_size=bs)
+
+
+def _sync_consts(mod, consts):
+    """Copy Const values into the module's __constant__ symbols when they
+    changed since the module last saw them (Const._to_device,
+    pyop2/cuda.py:314-320)."""
+    for c in consts:
+        if mod.const_versions.get(c.name) != (id(c), c._version):
+            ptr, nbytes = mod.const_ptr(c.name)
+            arr = np.ascontiguousarray(c._data)
+            if arr.nbytes != nbytes:
+                raise RuntimeError("Const %s needs %d bytes, but only space for %d" %
+                                   (c.name, arr.nbytes, nbytes))
+            call("op2b_memcpy_h2d", ptr, arr.ctypes.data, arr.nbytes, 0)
+            mod.const_versions[c.name] = (id(c), c._version)
 
 
 class _BoundLoop(object):
@@ -989,6 +1054,8 @@ class _BoundLoop(object):
             vals["mv%d" % j] = m._device_values().ptr
             vals["mr%d" % j] = m.sparsity._d_rowptr
             vals["mc%d" % j] = m.sparsity._d_colidx
+        if spec.mat_slots:
+            vals.update(mat_slot_values(specs, maps, mats))
         vals["err"] = _state['err'].ptr
         self.vals = vals
         n = iterset.size
@@ -1040,15 +1107,7 @@ class _BoundLoop(object):
                 vals["gp%d" % j] = pp
                 vals["gc%d" % j] = cc
         mod = self.module
-        for c in self.consts:
-            if mod.const_versions.get(c.name) != (id(c), c._version):
-                ptr, nbytes = mod.const_ptr(c.name)
-                arr = np.ascontiguousarray(c._data)
-                if arr.nbytes != nbytes:
-                    raise RuntimeError("Const %s needs %d bytes, but only space for %d" %
-                                       (c.name, arr.nbytes, nbytes))
-                call("op2b_memcpy_h2d", ptr, arr.ctypes.data, arr.nbytes, 0)
-                mod.const_versions[c.name] = (id(c), c._version)
+        _sync_consts(mod, self.consts)
         n = self.iterset.size
         if n == 0:
             return
@@ -1089,7 +1148,7 @@ class ParLoop(base.ParLoop):
         k.append(tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()))
         k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
                   cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode'], cfg.cfg['owner_mode'],
-                  cfg.cfg['kahan']))
+                  cfg.cfg['kahan'], cfg.cfg['mat_slots']))
         return tuple(k)
 
     def compute(self):

@@ -1,0 +1,211 @@
+"""Batched par_loops: one loop signature over many independent instances.
+
+A :class:`LoopInstance` is one par_loop (a kernel, an iteration set and its
+arguments) whose objects stay resident on the device.  A :class:`BatchLoop`
+runs any number of instances that share a loop signature (same kernel, same
+argument kinds, types, arities and access modes; different Sets, Maps, Dats,
+Mats and Globals) in ONE persistent launch:
+
+* every instance is a *segment*; its parameter block (the same
+  ``op2b_params`` struct a single par_loop passes by value) is packed once, at
+  instance creation, and the blocks of a batch are copied to the device as
+  one array;
+* each segment is cut into tiles of ``block_size * elems_per_thread``
+  consecutive elements (no tile crosses a segment), and a grid of
+  ``resident CTAs per SM x SMs`` walks the tile list, so meshes of very
+  different sizes share the GPU evenly;
+* INC into Dats and Mats uses the atomic form; Global reductions are reduced
+  per tile and finalised per segment in tile order by a second kernel, so a
+  segment's Global does not depend on what else is in the batch.
+
+There is no counterpart in the reference: pyop2/cuda.py launched one
+par_loop at a time with a host synchronise after each (pyop2/cuda.py:656-658).
+"""
+
+import copy
+
+import numpy as np
+
+from . import b200, codegen
+from . import configuration as cfg
+from ._lib import call
+from .exceptions import DeviceError
+
+TILE_DTYPE = np.dtype([("seg", "<i4"), ("pad", "<i4"), ("first", "<i8")])
+
+
+def build_tiles(sizes, tile):
+    """Tile list of a batch: segment i of ``sizes[i]`` elements is cut into
+    ceil(sizes[i] / tile) tiles starting at 0, tile, 2*tile, ...  Returns the
+    tiles (TILE_DTYPE; one zero entry when there are none) and each segment's
+    first tile index (len(sizes) + 1 entries, the last = number of tiles)."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    if (sizes < 0).any() or tile < 1:
+        raise ValueError("bad segment sizes or tile")
+    nt = (sizes + tile - 1) // tile
+    tile_first = np.zeros(len(sizes) + 1, dtype=np.int64)
+    np.cumsum(nt, out=tile_first[1:])
+    ntiles = int(tile_first[-1])
+    tiles = np.zeros(max(ntiles, 1), dtype=TILE_DTYPE)
+    if ntiles:
+        seg = np.repeat(np.arange(len(sizes), dtype=np.int32), nt)
+        tiles["seg"][:ntiles] = seg
+        tiles["first"][:ntiles] = (np.arange(ntiles, dtype=np.int64) - tile_first[seg]) * tile
+    return tiles, tile_first
+
+
+def _bind(info):
+    """Parameter values (device addresses) of one loop instance."""
+    vals = {}
+    for k, m in enumerate(info['maps']):
+        vals["m%d" % k] = m._to_device().ptr
+    for j, m in enumerate(info['mats']):
+        vals["mv%d" % j] = m._device_values().ptr
+        vals["mr%d" % j] = m.sparsity._d_rowptr
+        vals["mc%d" % j] = m.sparsity._d_colidx
+    if info['spec'].mat_slots:
+        vals.update(b200.mat_slot_values(info['specs'], info['maps'], info['mats']))
+    for j, d in enumerate(info['dats']):
+        d._to_device()
+        vals["d%d" % j] = d._device.ptr
+        if d.soa:
+            vals["ds%d" % j] = d.dataset.total_size
+    for j, g in enumerate(info['gbls']):
+        g._to_device()
+        vals["g%d" % j] = g._device.ptr
+    vals["err"] = b200._state['err'].ptr
+    return vals
+
+
+class LoopInstance(object):
+    """One par_loop kept ready for batching: ``LoopInstance(kernel,
+    it_space, *args)`` with the arguments ``op2.par_loop`` takes."""
+
+    def __init__(self, kernel, it_space, *args):
+        self.loop = b200.ParLoop(kernel, it_space, *args)
+        info = b200.loop_spec(self.loop, owner_mode='never', inc_mode='atomic', min_blocks=0)
+        spec = info['spec']
+        if spec.mode not in ("direct", "atomic"):
+            raise NotImplementedError("batched loops need direct access or atomic INC "
+                                      "(kernel %s)" % kernel.name)
+        self.spec = spec
+        self.key = spec.key()
+        self.size = int(info['iterset'].size)
+        self.dats = info['dats']
+        self.gbls = info['gbls']
+        self.mats = info['mats']
+        specs = info['specs']
+        written = {id(a.data) for a, s in zip(self.loop.args, specs)
+                   if a._is_dat and s.access != "READ"}
+        self.written = [d for d in self.dats if id(d) in written]
+        self.reducing = [g for g, s in zip(self.gbls, [s for s in specs if s.kind == "gbl"])
+                         if s.access != "READ"]
+        self.vals = _bind(info)
+        layout = codegen.ParamLayout(spec)
+        self.params = layout.pack(self.size, 0, self.size, self.vals)
+
+    def sync(self):
+        """Upload Dats and Globals whose host copy is newer."""
+        for d in self.dats:
+            if d._state is b200.HOST:
+                d._to_device()
+        for g in self.gbls:
+            if g._state is b200.HOST:
+                g._to_device()
+
+    def mark(self):
+        """Record that the device copies of written data are now newer."""
+        for d in self.written:
+            d._state = b200.DEVICE
+        for g in self.reducing:
+            g._state = b200.DEVICE
+        for m in self.mats:
+            m._state = b200.DEVICE
+
+
+class BatchLoop(object):
+    """All ``instances`` (LoopInstance, one signature) in one launch.
+
+    ``block_size`` threads per CTA, ``elems_per_thread`` elements per thread
+    per tile, ``min_blocks`` the stub's __launch_bounds__ minimum CTAs per SM
+    (0: none), ``ctas_per_sm`` caps the persistent grid (0: all resident)."""
+
+    def __init__(self, instances, block_size=None, elems_per_thread=1, min_blocks=0,
+                 ctas_per_sm=0):
+        if not instances:
+            raise ValueError("a batch needs at least one instance")
+        self.instances = list(instances)
+        key = self.instances[0].key
+        for n, inst in enumerate(self.instances):
+            if inst.key != key:
+                raise ValueError("instance %d of the batch has a different loop signature" % n)
+        spec = copy.copy(self.instances[0].spec)
+        spec.block_size = int(block_size or cfg.cfg['block_size'])
+        spec.batch = int(elems_per_thread)
+        spec.min_blocks = int(min_blocks)
+        if spec.batch < 1:
+            raise ValueError("elems_per_thread must be >= 1")
+        self.spec = spec
+        self.config = dict(block_size=spec.block_size, elems_per_thread=spec.batch,
+                           min_blocks=spec.min_blocks, ctas_per_sm=int(ctas_per_sm))
+        self.module = b200._get_module(spec)
+        fin_name = codegen.batch_stub_names(spec)[1]
+        self.layout = codegen.BatchLayout(spec)
+        self.has_fin = len(self.layout.fields) > 5
+        self.fin = self.module.function(fin_name) if self.has_fin else 0
+        # segments and tiles
+        sizes = np.array([inst.size for inst in self.instances], dtype=np.int64)
+        tiles, tile_first = build_tiles(sizes, spec.block_size * spec.batch)
+        ntiles = int(tile_first[-1])
+        self.ntiles, self.nsegs = ntiles, len(sizes)
+        self.elements = int(sizes.sum())
+        self._segs = b200._upload(np.frombuffer(b"".join(i.params for i in self.instances),
+                                                dtype=np.uint8))
+        self._tiles = b200._upload(tiles)
+        self._tile_first = b200._upload(tile_first)
+        vals = dict(segs=self._segs.ptr, tiles=self._tiles.ptr, tile_first=self._tile_first.ptr,
+                    ntiles=ntiles, nsegs=self.nsegs)
+        self._gpart = []
+        for name in self.layout.fields[5:]:
+            ctype, cdim, _ = spec.gbls[int(name[5:])]
+            item = np.dtype(_CTYPES[ctype]).itemsize
+            buf = b200.DeviceBuffer(max(ntiles, 1) * cdim * item)
+            self._gpart.append(buf)
+            vals[name] = buf.ptr
+        self._params = self.layout.pack(vals)
+        occ = self.module.occupancy(self.module.fn, spec.block_size)
+        if occ < 1:
+            raise DeviceError("batched stub %s cannot be resident at block size %d"
+                              % (spec.kernel_name, spec.block_size))
+        if ctas_per_sm:
+            occ = min(occ, int(ctas_per_sm))
+        self.grid = int(min(ntiles, occ * b200._state['sm_count']))
+        self.fin_grid = (self.nsegs * 32 + 255) // 256
+        self.consts = b200.base.Const._definitions()
+
+    @property
+    def launches(self):
+        """Kernels one :meth:`launch` issues."""
+        return (1 if self.grid else 0) + (1 if self.has_fin and self.nsegs else 0)
+
+    def launch(self, sync_host=True):
+        """Run every instance (asynchronous on the op2 stream).  With
+        ``sync_host`` first upload data whose host copy is newer, and mark
+        written data as newer on the device afterwards."""
+        if sync_host:
+            for inst in self.instances:
+                inst.sync()
+        b200._sync_consts(self.module, self.consts)
+        if self.grid:
+            call("op2b_launch", self.module.fn, self.grid, self.spec.block_size, 0, 0,
+                 self._params, self.layout.nbytes)
+        if self.has_fin and self.nsegs:
+            call("op2b_launch", self.fin, self.fin_grid, 256, 0, 0, self._params, self.layout.nbytes)
+        if sync_host:
+            for inst in self.instances:
+                inst.mark()
+
+
+_CTYPES = {"double": np.float64, "float": np.float32, "int": np.int32, "unsigned int": np.uint32,
+           "long long": np.int64, "unsigned long long": np.uint64, "long": np.int64,
+           "unsigned long": np.uint64, "short": np.int16, "char": np.int8}

@@ -74,6 +74,11 @@ class LoopSpec(object):
         # one grid-stride launch, INC args added with atomics
         self.mode = mode or ("plan" if indirect else "direct")
         self.owner = None   # owner-computes description (mode 'owner')
+        # elements per thread of a batched launch (0: not batched); see _batch_body
+        self.batch = 0
+        # scalar Mats found through scatter-slot tables (op2b_mat_slots_build)
+        # instead of a row search per entry (atomic and batched forms)
+        self.mat_slots = False
         self.kernel_name = kernel_name
         self.kernel_code = kernel_code
         self.extents = tuple(extents)
@@ -94,7 +99,8 @@ class LoopSpec(object):
                 tuple(self.mats), tuple(self.gbls), tuple(self.consts), self.indirect,
                 tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
                 self.block_size, self.fmad, self.min_blocks, self.mode,
-                tuple(sorted(self.owner.items())) if self.owner else None)
+                tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
+                self.mat_slots)
 
     @property
     def needs_coloring(self):
@@ -124,6 +130,8 @@ class ParamLayout(object):
             f.append("m%d" % k)
         for j in range(len(spec.mats)):
             f += ["mv%d" % j, "mr%d" % j, "mc%d" % j]
+            if spec.mat_slots:
+                f.append("ms%d" % j)
         for j, g in enumerate(spec.gbls):
             f.append("g%d" % j)
             if g[2] != "READ":
@@ -220,6 +228,9 @@ def generate(spec):
     w(_mark_inline(spec.kernel_code, spec.kernel_name))
     w("}  // namespace op2b_user")
     w("#undef OP2_STRIDE")
+    if spec.batch:
+        w(_batch_body(spec))
+        return "\n".join(out), layout, batch_stub_names(spec)[0]
     body = {"plan": _indirect_body, "atomic": _atomic_body, "direct": _direct_body,
             "owner": _owner_body}[spec.mode](spec)
     w(body)
@@ -285,23 +296,29 @@ def _kernel_call(spec, argexprs, indent):
     return "%sop2b_user::%s(%s);" % (indent, spec.kernel_name, ", ".join(argexprs + itargs))
 
 
+def _direct_element(spec, ind):
+    """Lines computing element ``e`` of a direct loop."""
+    pre, post, exprs = [], [], []
+    for n, a in enumerate(spec.args):
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
+        else:
+            exprs.append(_direct_row(a, n, "e", pre, post, ind))
+    L = list(pre)
+    L += _itspace_open(spec, ind)
+    L.append(_kernel_call(spec, exprs, ind + "  " * len(spec.extents)))
+    L += _itspace_close(spec, ind)
+    L += post
+    return L
+
+
 def _direct_body(spec):
     bs = spec.block_size
     L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
     _gbl_prologue(spec, L)
     L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
              " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
-    pre, post, exprs = [], [], []
-    for n, a in enumerate(spec.args):
-        if a.kind == "gbl":
-            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
-        else:
-            exprs.append(_direct_row(a, n, "e", pre, post, "    "))
-    L += pre
-    L += _itspace_open(spec, "    ")
-    L.append(_kernel_call(spec, exprs, "    " + "  " * len(spec.extents)))
-    L += _itspace_close(spec, "    ")
-    L += post
+    L += _direct_element(spec, "    ")
     L.append("  }")
     _gbl_epilogue(spec, L)
     L.append("}")
@@ -483,7 +500,16 @@ def _atomic_body(spec):
     _gbl_prologue(spec, L)
     L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
              " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
-    ind = "    "
+    L += _atomic_element(spec, "    ")
+    L.append("  }")
+    _gbl_epilogue(spec, L)
+    L.append("}")
+    return "\n".join(L)
+
+
+def _atomic_element(spec, ind):
+    """Lines computing element ``e`` of an atomic-mode indirect loop."""
+    L = []
     used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
                        {a.cmslot for a in spec.args if a.kind == "mat"})
     for k in used_maps:
@@ -558,8 +584,101 @@ def _atomic_body(spec):
     L += _itspace_close(spec, ind)
     L += post
     L += apply
+    return L
+
+
+def batch_stub_names(spec):
+    """Symbols of a batched loop: the element kernel and the Global
+    finalisation kernel."""
+    base = stub_name(spec) + "_batch"
+    return base, base + "_fin"
+
+
+class BatchLayout(object):
+    """Field order of op2b_batch_params (all 8-byte fields): the per-segment
+    parameter blocks, the tile list, each segment's first tile (nsegs + 1
+    entries), the tile and segment counts, and one partials array per
+    reducing Global slot."""
+
+    def __init__(self, spec):
+        f = ["segs", "tiles", "tile_first", "ntiles", "nsegs"]
+        for j, g in enumerate(spec.gbls):
+            if g[2] != "READ":
+                f.append("gpart%d" % j)
+        self.fields = f
+        self.fmt = "<" + "Q" * len(f)
+        self.nbytes = struct.calcsize(self.fmt)
+
+    def pack(self, values):
+        return struct.pack(self.fmt, *[int(values.get(n, 0)) for n in self.fields])
+
+
+def _batch_body(spec):
+    """A batched loop: the same stub over many instances (segments) of one
+    loop signature, each with its own Sets, Maps, Dats, Mats and Globals.
+
+    The host splits every segment into tiles of ``block_size * batch``
+    consecutive elements (a tile never crosses a segment) and lists them; a
+    persistent grid walks the tile list, each CTA loading the tile's segment
+    parameter block and running the direct / atomic element code on the
+    tile's elements.  Global reductions are reduced per tile into a partials
+    array, and the finalisation kernel (one warp per segment) combines each
+    segment's partials in tile order: a segment's result depends only on its
+    own data and the tile size, never on the other segments in the batch."""
+    bs, ept = spec.block_size, spec.batch
+    names = batch_stub_names(spec)
+    layout = BatchLayout(spec)
+    L = ["struct op2b_batch_tile { int seg; int pad; op2b_i64 first; };",
+         "struct op2b_batch_params {", "  const op2b_params *segs;",
+         "  const op2b_batch_tile *tiles;", "  const op2b_i64 *tile_first;",
+         "  op2b_i64 ntiles, nsegs;"]
+    for n in layout.fields[5:]:
+        L.append("  %s *%s;" % (spec.gbls[int(n[5:])][0], n))
+    L.append("};")
+    elem = _direct_element if spec.mode == "direct" else _atomic_element
+    L.append("extern \"C\" __global__ void %s %s(const op2b_batch_params bp) {"
+             % (_bounds(spec), names[0]))
+    red = [(n, a) for n, a in enumerate(spec.args) if a.kind == "gbl" and a.access != "READ"]
+    for n, a in red:
+        L.append("  __shared__ %s red%d[32];" % (a.ctype, n))
+    L.append("  for (op2b_i64 t = blockIdx.x; t < bp.ntiles; t += gridDim.x) {")
+    L.append("    const op2b_batch_tile td = bp.tiles[t];")
+    L.append("    const op2b_params p = bp.segs[td.seg];")
+    pro = []
+    _gbl_prologue(spec, pro)
+    L += ["  " + x for x in pro]
+    L.append("#pragma unroll 1")
+    L.append("    for (int k = 0; k < %d; ++k) {" % ept)
+    L.append("      const op2b_i64 e = td.first + threadIdx.x + (op2b_i64)k * %d;" % bs)
+    L.append("      if (e < p.end) {")
+    L += elem(spec, "        ")
+    L.append("      }")
+    L.append("    }")
+    for n, a in red:
+        for c in range(a.cdim):
+            L.append("    { const %s v = op2b_block_reduce<%d>(r%d[%d], red%d);"
+                     % (a.ctype, _RED_OP[a.access], n, c, n))
+            L.append("      if (threadIdx.x == 0) bp.gpart%d[t * %d + %d] = v; }" % (a.slot, a.cdim, c))
     L.append("  }")
-    _gbl_epilogue(spec, L)
+    L.append("}")
+    # finalisation: one warp per segment, partials combined in tile order
+    L.append("extern \"C\" __global__ void __launch_bounds__(256) %s(const op2b_batch_params bp) {"
+             % names[1])
+    L.append("  const op2b_i64 s = ((op2b_i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;")
+    L.append("  const int lane = threadIdx.x & 31;")
+    L.append("  if (s >= bp.nsegs) return;")
+    L.append("  const op2b_params p = bp.segs[s];")
+    L.append("  const op2b_i64 t0 = bp.tile_first[s], t1 = bp.tile_first[s + 1];")
+    for n, a in red:
+        op = _RED_OP[a.access]
+        for c in range(a.cdim):
+            init = "(%s)0" % a.ctype if op == 0 else "p.g%d[%d]" % (a.slot, c)
+            L.append("  { %s acc = %s;" % (a.ctype, init))
+            L.append("    for (op2b_i64 t = t0 + lane; t < t1; t += 32)"
+                     " acc = op2b_combine<%d>(acc, bp.gpart%d[t * %d + %d]);" % (op, a.slot, a.cdim, c))
+            L.append("    acc = op2b_warp_reduce<%d>(acc);" % op)
+            L.append("    if (lane == 0) p.g%d[%d] = op2b_combine<%d>(p.g%d[%d], acc); }"
+                     % (a.slot, c, op, a.slot, c))
     L.append("}")
     return "\n".join(L)
 
@@ -809,7 +928,11 @@ def _mat_addto(spec, n, a, ind, atomic=False):
     ci = "i%d" % a.cidx
     if a.rm * a.cm == 1:
         L.append("%s  const int row = mr%d[%s], colj = mr%d[%s];" % (ind, a.mslot, ri, a.cmslot, ci))
-        L.append("%s  const int pos = op2b_csr_find(p.mr%d, p.mc%d, row, colj);" % (ind, j, j))
+        if spec.mat_slots and atomic:
+            L.append("%s  const int pos = __ldg(p.ms%d + (op2b_i64)(%s * %d + %s) * p.set_size + e);"
+                     % (ind, j, ri, a.carity, ci))
+        else:
+            L.append("%s  const int pos = op2b_csr_find(p.mr%d, p.mc%d, row, colj);" % (ind, j, j))
         L.append("%s  if (pos < 0) op2b_flag_missing(p.err, row, colj);" % ind)
         if ins:
             L.append("%s  else p.mv%d[pos] = A%d[i0][i1];" % (ind, j, n))

@@ -29,7 +29,11 @@ keys of the B200 backend:
   ``'never'`` (default) leaves those loops to ``inc_mode``.  It is slower than
   the atomic form where kernels index tables with the iteration-space index
   (the index becomes a run-time value per lane);
-* ``kahan``: compensated (Kahan) summation of owner-computes accumulation.
+* ``kahan``: compensated (Kahan) summation of owner-computes accumulation;
+* ``mat_slots``: assemble scalar Mats in the atomic form through a cached
+  scatter-slot table (the CSR position of every element's local entries,
+  built once per Sparsity and Map pair: nelem x arity^2 int32 of device
+  memory) instead of searching the CSR row for every entry.
 """
 
 import os
@@ -51,6 +55,7 @@ _defaults = {
     'inc_mode': 'atomic',
     'owner_mode': 'never',
     'kahan': False,
+    'mat_slots': True,
 }
 
 _config = dict(_defaults)

@@ -455,6 +455,16 @@ int op2b_function_set_smem(uint64_t fn, int32_t bytes) {
   return OP2B_OK;
 }
 
+int op2b_function_occupancy(uint64_t fn, uint32_t block, uint32_t smem, int32_t *blocks_per_sm) {
+  OP2B_REQUIRE_INIT();
+  if (!blocks_per_sm || block == 0) return set_error(OP2B_ERR_ARG, "bad occupancy query");
+  int n = 0;
+  OP2B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, reinterpret_cast<const void *>(fn),
+                                                          static_cast<int>(block), smem));
+  *blocks_per_sm = n;
+  return OP2B_OK;
+}
+
 int op2b_launch(uint64_t fn, uint32_t grid, uint32_t block, uint32_t smem, uint64_t stream,
                 const void *params, uint64_t nbytes) {
   OP2B_REQUIRE_INIT();

@@ -53,6 +53,20 @@ void p1_rhs(double *b, double *x[2], double **f, int j) {
 
 # P2 basis on the reference triangle with barycentrics l0 = 1-s-t, l1 = s,
 # l2 = t: vertices li(2li-1), midpoints 4 la lb.  REAL is double or float.
+P1_STIFF = """
+void p1_stiff(double A[1][1], double *x[2], int j, int k) {
+  double a00 = x[1][0] - x[0][0], a01 = x[2][0] - x[0][0];
+  double a10 = x[1][1] - x[0][1], a11 = x[2][1] - x[0][1];
+  double det = a00 * a11 - a01 * a10;
+  const double rg[3][2] = {{-1.0, -1.0}, {1.0, 0.0}, {0.0, 1.0}};
+  double gj0 = (a11 * rg[j][0] - a10 * rg[j][1]) / det;
+  double gj1 = (a00 * rg[j][1] - a01 * rg[j][0]) / det;
+  double gk0 = (a11 * rg[k][0] - a10 * rg[k][1]) / det;
+  double gk1 = (a00 * rg[k][1] - a01 * rg[k][0]) / det;
+  A[0][0] += 0.5 * fabs(det) * (gj0 * gk0 + gj1 * gk1);
+}
+"""
+
 _P2_COMMON = """
 static __inline__ void p2_basis_%(S)s(REAL s, REAL t, REAL phi[6], REAL ds[6], REAL dt[6]) {
   const REAL l0 = (REAL)1 - s - t, l1 = s, l2 = t;
@@ -134,7 +148,7 @@ class Problem(object):
     pass
 
 
-def build_p1(op2, n, coords=None, elem=None):
+def build_p1(op2, n, coords=None, elem=None, stiffness=False):
     """P1 mass Mat + RHS Dat on the n x n square."""
     if coords is None:
         coords, elem = square_p1(n)
@@ -151,8 +165,17 @@ def build_p1(op2, n, coords=None, elem=None):
     P.b = op2.Dat(P.nodes, np.zeros(len(coords)), np.float64, "b")
     P.k_mass = op2.Kernel(P1_MASS, "p1_mass")
     P.k_rhs = op2.Kernel(P1_RHS, "p1_rhs")
+    if stiffness:
+        P.stiff = op2.Mat(P.sparsity, np.float64, "stiffness")
+        P.k_stiff = op2.Kernel(P1_STIFF, "p1_stiff")
     P.n_elem, P.n_nodes = len(elem), len(coords)
     return P
+
+
+def assemble_p1_stiffness(op2, P):
+    op2.par_loop(P.k_stiff, P.elements(3, 3),
+                 P.stiff((P.elem_node[op2.i[0]], P.elem_node[op2.i[1]]), op2.INC),
+                 P.coords(P.elem_vnode, op2.READ))
 
 
 def assemble_p1(op2, P):

@@ -37,6 +37,31 @@ def square_p1(n):
     return coords, elem
 
 
+def rect_p1(nx, ny, seed=None):
+    """nx x ny quads of side h = 1 / max(nx, ny), each split into two
+    triangles; node numbering randomly permuted from ``seed`` (None keeps
+    the structured numbering).  Returns coords [(nx+1)(ny+1), 2] f64 and
+    elem_node [2 nx ny, 3] i32 (counter-clockwise)."""
+    mx, my = nx + 1, ny + 1
+    h = 1.0 / max(nx, ny)
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    v00 = (i * my + j).ravel()
+    v10 = ((i + 1) * my + j).ravel()
+    v11 = ((i + 1) * my + j + 1).ravel()
+    v01 = (i * my + j + 1).ravel()
+    elem = np.empty((2 * nx * ny, 3), dtype=np.int64)
+    elem[0::2] = np.stack([v00, v10, v11], axis=1)
+    elem[1::2] = np.stack([v00, v11, v01], axis=1)
+    xi, yj = np.meshgrid(np.arange(mx), np.arange(my), indexing="ij")
+    coords = np.stack([xi.ravel() * h, yj.ravel() * h], axis=1).astype(np.float64)
+    if seed is not None:
+        perm = np.random.default_rng(seed).permutation(mx * my)
+        new_coords = np.empty_like(coords)
+        new_coords[perm] = coords
+        coords, elem = new_coords, perm[elem]
+    return coords, elem.astype(np.int32)
+
+
 def square_p2(n, seed=0, jitter=0.1):
     """Returns coords [(2n+1)^2, 2] f64 and elem_dof [2 n^2, 6] i32 with the
     local order (v0, v1, v2, m12, m02, m01): vertices then the midpoint of the

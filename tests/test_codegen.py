@@ -211,3 +211,69 @@ def test_param_layout_offsets():
     assert L.nbytes == 32 + 8 * len(L.fields)
     packed = L.pack(100, 0, 100, {"d0": 0x1000, "m0": 0x2000})
     assert len(packed) == L.nbytes
+
+
+def _batched(spec, ept=2):
+    import copy
+    from pyop2_b200 import b200
+    s = copy.copy(spec)
+    s.batch = ept
+    return s
+
+
+def test_batched_forms(host_op2):
+    """Batched stubs (one launch over many instances): direct loops with
+    Global INC / MIN / MAX, atomic indirect INC into Dats and a Mat."""
+    from pyop2_b200 import b200
+    op2 = host_op2
+    s1, s2 = op2.Set(10, 1), op2.Set(10, 2)
+    x = op2.Dat(s1, np.zeros(10), np.float64)
+    y = op2.Dat(s2, np.zeros(20), np.float64)
+    g = op2.Global(1, 0.0, np.float64)
+    g3 = op2.Global(3, (0.0, 0.0, 0.0), np.float64)
+    k = op2.Kernel("void k(double *a, double *g) { g[0] += a[0]; }", "k")
+    for acc in (op2.INC, op2.MIN, op2.MAX, op2.READ):
+        spec = b200.loop_spec(b200.ParLoop(k, s1, x(op2.IdentityMap, op2.READ), g(acc)),
+                              inc_mode='atomic', owner_mode='never')["spec"]
+        src, _, _ = nvrtc_compile(_batched(spec))
+        assert "op2b_k_batch" in src and "op2b_k_batch_fin" in src
+    spec = b200.loop_spec(b200.ParLoop(op2.Kernel("void k3(double *a, double *g) { }", "k3"), s2,
+                                       y(op2.IdentityMap, op2.RW), g3(op2.INC)),
+                          inc_mode='atomic', owner_mode='never')["spec"]
+    nvrtc_compile(_batched(spec, 4))
+    # indirect: vec-map READ, itspace INC, Mat INC
+    e = op2.Set(4, 1)
+    n = op2.Set(6, 1)
+    vn = op2.Set(6, 2)
+    em = op2.Map(e, n, 3, np.array([0, 1, 2, 1, 2, 3, 2, 3, 4, 3, 4, 5], np.int32))
+    evm = op2.Map(e, vn, 3, np.array([0, 1, 2, 1, 2, 3, 2, 3, 4, 3, 4, 5], np.int32))
+    xy = op2.Dat(vn, np.zeros(12), np.float64)
+    b = op2.Dat(n, np.zeros(6), np.float64)
+    sp = op2.Sparsity((em, em))
+    mat = op2.Mat(sp, np.float64)
+    km = op2.Kernel("void km(double A[1][1], double *x[2], int j, int k) { A[0][0] += x[j][0] * x[k][1]; }", "km")
+    spec = b200.loop_spec(b200.ParLoop(km, e(3, 3), mat((em[op2.i[0]], em[op2.i[1]]), op2.INC),
+                                       xy(evm, op2.READ)), inc_mode='atomic', owner_mode='never',
+                          mat_nnz_max=8)["spec"]
+    assert spec.mode == "atomic"
+    src, _, _ = nvrtc_compile(_batched(spec, 1))
+    assert "op2b_km_batch_fin" in src
+    kr = op2.Kernel("void kr(double *b, double *x[2], int j) { b[0] += x[j][0]; }", "kr")
+    spec = b200.loop_spec(b200.ParLoop(kr, e(3), b(em[op2.i[0]], op2.INC), xy(evm, op2.READ)),
+                          inc_mode='atomic', owner_mode='never')["spec"]
+    nvrtc_compile(_batched(spec, 2))
+
+
+def test_batch_layout_fields(host_op2):
+    from pyop2_b200 import b200
+    op2 = host_op2
+    s1 = op2.Set(10, 1)
+    x = op2.Dat(s1, np.zeros(10), np.float64)
+    g = op2.Global(1, 0.0, np.float64)
+    h = op2.Global(1, 0.0, np.float64)
+    k = op2.Kernel("void k(double *a, double *g, double *h) { }", "k")
+    spec = b200.loop_spec(b200.ParLoop(k, s1, x(op2.IdentityMap, op2.READ), g(op2.INC), h(op2.READ)),
+                          inc_mode='atomic', owner_mode='never')["spec"]
+    lay = codegen.BatchLayout(spec)
+    assert lay.fields == ["segs", "tiles", "tile_first", "ntiles", "nsegs", "gpart0"]
+    assert lay.nbytes == 48

@@ -195,3 +195,36 @@ def test_insert_outside_sparsity_raises(op2):
         loop.args[0]._map = [m1, m3]
         loop.compute()
         matx.array
+
+
+def test_slot_table_matches_row_search(op2):
+    """The scatter-slot table holds, for every element's (r, c) entry, the
+    CSR position a row search finds; assembly through it equals assembly by
+    search within the INC tolerance."""
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import fem, meshes
+    coords, elem = meshes.rect_p1(9, 5, seed=4)
+    P = fem.build_p1(op2, 0, coords=coords, elem=elem, stiffness=True)
+    sp = P.sparsity
+    buf = sp._slot_table(P.elem_node, P.elem_node)
+    n = len(elem)
+    got = np.empty(n * 9, dtype=np.int32)
+    buf.to_host(got)
+    rp, ci = sp.rowptr, sp.colidx
+    for e in range(n):
+        for r in range(3):
+            for c in range(3):
+                row, col = elem[e, r], elem[e, c]
+                seg = ci[rp[row]:rp[row + 1]]
+                want = rp[row] + int(np.searchsorted(seg, col))
+                assert got[(r * 3 + c) * n + e] == want
+    vals = {}
+    for slots in (True, False):
+        cfg.configure(mat_slots=slots)
+        try:
+            P.stiff.zero()
+            fem.assemble_p1_stiffness(op2, P)
+            vals[slots] = P.stiff.array.copy()
+        finally:
+            cfg.configure(mat_slots=True)
+    assert np.abs(vals[True] - vals[False]).max() <= 1e-12 * np.abs(vals[False]).max()
