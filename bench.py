@@ -275,6 +275,12 @@ def run_gpu(args, ws, rank, local):
             print(json.dumps({"batching": bench_batching(op2, b200, args.batch_meshes or 4096)}))
         d.close()
         return 0
+    if args.serving_only:
+        if rank == 0:
+            print(json.dumps({"serving": bench_serving(op2, b200, args.serve_requests or 3000,
+                                                       args.serve_rate)}))
+        d.close()
+        return 0
     bytes_ = _bytes()
     bpi = bytes_["iteration"]
     grid = airfoil_grid(NX, NY, SEED, permute=not args.no_permute)
@@ -407,6 +413,9 @@ def run_gpu(args, ws, rank, local):
     batching = None
     if args.batch_meshes > 0:
         batching = bench_batching(op2, b200, args.batch_meshes)
+    serving = None
+    if args.serve_requests > 0:
+        serving = bench_serving(op2, b200, args.serve_requests, args.serve_rate)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -439,6 +448,7 @@ def run_gpu(args, ws, rank, local):
         "loops": breakdown,
         "mat_assembly": assembly,
         "batching": batching,
+        "serving": serving,
         "inc_mode": op2_cfg_inc_mode(),
         "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
     }
@@ -560,6 +570,93 @@ def bench_batching(op2, b200, nmesh, reps=5, seed=0):
             "autotune": tuned, "setup_s": round(setup_s, 1), "tune_s": round(tune_s, 1)}
 
 
+def bench_serving(op2, b200, nreq, rate, seed=0, n_p1=16, n_quad=16):
+    """Serving form: a Poisson trace (``rate`` requests/s, ``nreq`` requests)
+    mixing P1 assembly requests (meshes of 10^3..10^6 triangles) and
+    10-iteration airfoil-style chains (10^4..10^6 cells) on a pool of
+    resident meshes, 120 GB HBM admission budget.  The continuous-batching
+    engine and the plain per-request drop-in serve the same trace in real
+    time (latency = result on the host - arrival); then both serve it with
+    every request released at once (capacity).  Parity: every request's
+    results, engine against plain."""
+    from pyop2_b200 import autotune, base, serve
+    from pyop2_b200.workloads import serving
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    consts = serving.declare_consts(op2)
+    pool = serving.mesh_pool(n_p1, n_quad, seed)
+    store = serve.MeshStore(budget=120e9)
+    serving.register(store, op2, pool, seed)
+    t0 = time.time()
+    for mid in sorted(pool):
+        store.load(mid)
+    resident_s = time.time() - t0
+    jobs = serving.trace(nreq, rate, pool, seed)
+    warm = serving.trace(64, 1e6, pool, seed + 1)
+    serve.Engine(store).run(serving.clone_trace(warm, False), realtime=False)
+    serve.PlainServer(op2, store).run(serving.clone_trace(warm[:16], False), realtime=False)
+    t1 = time.time()
+    configs = {}
+    kinds = {"p1": (("p1_src", "t_src"), ("p1_mass", "t_mass"), ("p1_rhs", "t_rhs")),
+             "quad": (("q_init", "t_init"), ("save_soln", "t_save"), ("adt_calc", "t_adt"),
+                      ("res_calc", "t_res"), ("bres_calc", "t_bres"), ("update", "t_update"))}
+    for mkind, loops in kinds.items():
+        meshes = [store.get(m) for m in sorted(pool) if pool[m][0] == mkind]
+        for name, attr in loops:
+            configs[name], _ = autotune.tune([getattr(m, attr) for m in meshes], reps=2)
+    tune_s = time.time() - t1
+    b200.synchronize()
+    # results reach the consumer as views of pinned host memory; every 16th
+    # request's results are kept for the parity check
+    kept = {"engine": {}, "plain": {}}
+
+    def consumer(which):
+        def take(job, views):
+            if job.rid % 16 == 0:
+                kept[which][job.rid] = {k: np.array(v, dtype=np.float64).reshape(-1)
+                                        for k, v in views.items()}
+        return take
+
+    # capacity first: it also fills the pinned-buffer pool the timed runs reuse
+    cap_e = serve.Engine(store, configs=configs, consumer=lambda j, v: None, timing=True)
+    s_cap_eng = serve.summary(cap_e.run(serving.clone_trace(jobs, False), realtime=False), 0.0)
+    s_cap_eng["gpu_busy_fraction"] = round(cap_e.gpu_busy_ms() / (s_cap_eng["span_s"] * 1e3), 3)
+    eng = serve.Engine(store, configs=configs, consumer=consumer("engine"))
+    done = eng.run(serving.clone_trace(jobs), realtime=True)
+    s_eng = serve.summary(done)
+    s_eng.update(steps=eng.steps, launches=eng.launches,
+                 mean_batch=round(float(np.mean(eng.batch_sizes)), 2),
+                 peak_hbm_gb=round(eng.peak_used / 1e9, 3))
+    plain = serve.PlainServer(op2, store, consumer=consumer("plain")).run(
+        serving.clone_trace(jobs), realtime=True)
+    s_plain = serve.summary(plain)
+    sub = jobs[:max(1, len(jobs) // 4)]
+    s_cap_plain = serve.summary(serve.PlainServer(op2, store, consumer=lambda j, v: None).run(
+        serving.clone_trace(sub, False), realtime=False), 0.0)
+    err = {"p1": 0.0, "quad": 0.0}
+    kinds_by_id = {j.rid: j.kind for j in jobs}
+    for rid, pres in kept["plain"].items():
+        eres = kept["engine"][rid]
+        for k in pres:
+            a, b = eres[k], pres[k]
+            den = max(float(np.abs(b).max()), 1e-300)
+            err[kinds_by_id[rid]] = max(err[kinds_by_id[rid]], float(np.abs(a - b).max()) / den)
+    del consts
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    return {"trace": {"requests": nreq, "rate_per_s": rate, "p1_meshes": n_p1,
+                      "quad_meshes": n_quad, "iters_per_chain": 10, "hbm_budget_gb": 120,
+                      "p1_triangles": [int(2 * v[1] * v[2]) for v in pool.values() if v[0] == "p1"],
+                      "quad_cells": [int(v[1] * v[2]) for v in pool.values() if v[0] == "quad"]},
+            "engine": s_eng, "plain": s_plain,
+            "req_per_s_ratio": round(s_eng["req_per_s"] / s_plain["req_per_s"], 2),
+            "p99_ratio_plain_over_engine": round(s_plain["p99_ms"] / s_eng["p99_ms"], 2),
+            "capacity_engine": s_cap_eng, "capacity_plain": s_cap_plain,
+            "capacity_ratio": round(s_cap_eng["req_per_s"] / s_cap_plain["req_per_s"], 2),
+            "max_rel_err_engine_vs_plain": err, "autotuned": configs,
+            "resident_setup_s": round(resident_s, 1), "tune_s": round(tune_s, 1)}
+
+
 def bench_assembly(op2, b200, reps=5):
     """Mat assembly legs: P1 256x256 mass + RHS and P2 1024x1024
     stiffness + mass in FP64 and in the precision form (FP32 element math and
@@ -670,6 +767,12 @@ def main(argv=None):
                    help="meshes of the batching leg (0 skips it)")
     p.add_argument("--batching-only", action="store_true",
                    help="run only the batching leg and print its figures")
+    p.add_argument("--serve-requests", type=int, default=3000,
+                   help="requests of the serving leg (0 skips it)")
+    p.add_argument("--serve-rate", type=float, default=2000.0,
+                   help="mean Poisson arrival rate of the serving leg (requests/s)")
+    p.add_argument("--serving-only", action="store_true",
+                   help="run only the serving leg and print its figures")
     p.add_argument("--l2-fetch", type=int, default=-1,
                    help="L2 fetch granularity in bytes (32/64/128; 0 driver default; -1 backend default)")
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")

@@ -62,6 +62,10 @@ int op2b_host_alloc(uint64_t *hptr, uint64_t bytes);   /* pinned host memory */
 int op2b_host_free(uint64_t hptr);
 int op2b_memcpy_h2d(uint64_t dst, const void *src, uint64_t bytes, uint64_t stream);
 int op2b_memcpy_d2h(void *dst, uint64_t src, uint64_t bytes, uint64_t stream);
+/* Device-to-host copy that returns at once (stream-ordered; complete when an
+ * event recorded after it completes).  dst must be pinned host memory
+ * (op2b_host_alloc) for the copy to be asynchronous. */
+int op2b_memcpy_d2h_async(void *dst, uint64_t src, uint64_t bytes, uint64_t stream);
 int op2b_memcpy_d2d(uint64_t dst, uint64_t src, uint64_t bytes, uint64_t stream);
 int op2b_memset(uint64_t dst, int value, uint64_t bytes, uint64_t stream);
 /* AoS <-> SoA reorder on the device, [n][dim] <-> [dim][n] with elements of
@@ -90,6 +94,9 @@ int op2b_event_create(uint64_t *event);
 int op2b_event_destroy(uint64_t event);
 int op2b_event_record(uint64_t event, uint64_t stream);
 int op2b_event_sync(uint64_t event);
+/* Non-blocking: *done = 1 if all work before the event's record has
+ * completed, else 0 (cudaEventQuery). */
+int op2b_event_query(uint64_t event, int32_t *done);
 int op2b_event_elapsed_ms(uint64_t start, uint64_t stop, float *ms);
 int op2b_stream_wait_event(uint64_t stream, uint64_t event);
 int op2b_graph_begin(uint64_t stream);

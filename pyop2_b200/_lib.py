@@ -31,6 +31,7 @@ _SIGS = {
     "op2b_host_free": [u64],
     "op2b_memcpy_h2d": [u64, P, u64, u64],
     "op2b_memcpy_d2h": [P, u64, u64, u64],
+    "op2b_memcpy_d2h_async": [P, u64, u64, u64],
     "op2b_memcpy_d2d": [u64, u64, u64, u64],
     "op2b_memset": [u64, C.c_int, u64, u64],
     "op2b_transpose": [u64, u64, i64, i32, i32, i32, u64],
@@ -44,6 +45,7 @@ _SIGS = {
     "op2b_event_destroy": [u64],
     "op2b_event_record": [u64, u64],
     "op2b_event_sync": [u64],
+    "op2b_event_query": [u64, i32p],
     "op2b_event_elapsed_ms": [u64, u64, C.POINTER(C.c_float)],
     "op2b_stream_wait_event": [u64, u64],
     "op2b_graph_begin": [u64],

@@ -1012,9 +1012,16 @@ class _BoundLoop(object):
         self.dats, self.maps, self.mats = dats, maps, mats
         self.gbl_specs = [s for s in specs if s.kind == "gbl"]
         self.dat_access = {}
+        direct_write = {}
         for a, s in zip(args, specs):
             if a._is_dat:
                 self.dat_access.setdefault(id(a.data), []).append(s.access)
+                ok = (s.kind == "direct" and s.access == "WRITE"
+                      and a.data.dataset.total_size == iterset.size)
+                direct_write[id(a.data)] = direct_write.get(id(a.data), True) and ok
+        # Dats the loop only writes, row by row over the whole set: a fresh
+        # device copy needs no upload of the host values first
+        self.write_only = {k for k, v in direct_write.items() if v}
         self.refs = [weakref.ref(o) for o in dats + maps + mats]
         self.consts = base.Const._definitions()
         self.block_size = info['block_size']
@@ -1090,7 +1097,9 @@ class _BoundLoop(object):
     def run(self, loop):
         vals = self.vals
         for j, d in enumerate(self.dats):
-            modes = self.dat_access[id(d)]
+            if d._state is DEVICE_UNALLOCATED and id(d) in self.write_only:
+                d._allocate_device()
+                d._state = DEVICE
             d._allocate_device()
             if d._state is HOST:
                 d._to_device()
@@ -1195,6 +1204,12 @@ class Event(object):
 
     def synchronize(self):
         call("op2b_event_sync", self.handle)
+
+    def query(self):
+        """True once the work recorded before this event has completed."""
+        d = C.c_int32()
+        call("op2b_event_query", self.handle, C.byref(d))
+        return bool(d.value)
 
     def elapsed_ms(self, later):
         ms = C.c_float()

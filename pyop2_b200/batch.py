@@ -23,6 +23,7 @@ par_loop at a time with a host synchronise after each (pyop2/cuda.py:656-658).
 """
 
 import copy
+import struct
 
 import numpy as np
 
@@ -32,6 +33,10 @@ from ._lib import call
 from .exceptions import DeviceError
 
 TILE_DTYPE = np.dtype([("seg", "<i4"), ("pad", "<i4"), ("first", "<i8")])
+
+# (loop signature, block size, elements per thread, min blocks) ->
+# (module, BatchLayout, has finalisation, finalisation function, CTAs per SM)
+_COMPILED = {}
 
 
 def build_tiles(sizes, tile):
@@ -54,55 +59,130 @@ def build_tiles(sizes, tile):
     return tiles, tile_first
 
 
-def _bind(info):
+def _fields(info):
+    """The pointer fields of a loop instance and the object behind each:
+    [(field, kind, obj)]; kind 'slots' holds (Mat, row Map, column Map)."""
+    f = []
+    spec = info['spec']
+    for k, m in enumerate(info['maps']):
+        f.append(("m%d" % k, "map", m))
+    for j, m in enumerate(info['mats']):
+        f.append(("mv%d" % j, "mat", m))
+    if spec.mat_slots:
+        seen = set()
+        for s in info['specs']:
+            if s.kind == "mat" and s.slot not in seen:
+                seen.add(s.slot)
+                f.append(("ms%d" % s.slot, "slots",
+                          (info['mats'][s.slot], info['maps'][s.mslot], info['maps'][s.cmslot])))
+    for j, d in enumerate(info['dats']):
+        f.append(("d%d" % j, "dat", d))
+    for j, g in enumerate(info['gbls']):
+        f.append(("g%d" % j, "gbl", g))
+    return f
+
+
+def _bind(fields):
     """Parameter values (device addresses) of one loop instance."""
     vals = {}
-    for k, m in enumerate(info['maps']):
-        vals["m%d" % k] = m._to_device().ptr
-    for j, m in enumerate(info['mats']):
-        vals["mv%d" % j] = m._device_values().ptr
-        vals["mr%d" % j] = m.sparsity._d_rowptr
-        vals["mc%d" % j] = m.sparsity._d_colidx
-    if info['spec'].mat_slots:
-        vals.update(b200.mat_slot_values(info['specs'], info['maps'], info['mats']))
-    for j, d in enumerate(info['dats']):
-        d._to_device()
-        vals["d%d" % j] = d._device.ptr
-        if d.soa:
-            vals["ds%d" % j] = d.dataset.total_size
-    for j, g in enumerate(info['gbls']):
-        g._to_device()
-        vals["g%d" % j] = g._device.ptr
+    for name, kind, o in fields:
+        if kind == "map":
+            vals[name] = o._to_device().ptr
+        elif kind == "mat":
+            j = name[2:]
+            vals[name] = o._device_values().ptr
+            vals["mr" + j] = o.sparsity._d_rowptr
+            vals["mc" + j] = o.sparsity._d_colidx
+        elif kind == "slots":
+            m, rmap, cmap = o
+            vals[name] = m.sparsity._slot_table(rmap, cmap).ptr
+        elif kind == "dat":
+            o._to_device()
+            vals[name] = o._device.ptr
+            if o.soa:
+                vals["ds" + name[1:]] = o.dataset.total_size
+        else:
+            o._to_device()
+            vals[name] = o._device.ptr
     vals["err"] = b200._state['err'].ptr
     return vals
 
 
 class LoopInstance(object):
     """One par_loop kept ready for batching: ``LoopInstance(kernel,
-    it_space, *args)`` with the arguments ``op2.par_loop`` takes."""
+    it_space, *args)`` with the arguments ``op2.par_loop`` takes.
+
+    :meth:`like` makes the same loop over other objects (another mesh, other
+    Dats) without re-deriving the loop signature."""
 
     def __init__(self, kernel, it_space, *args):
-        self.loop = b200.ParLoop(kernel, it_space, *args)
-        info = b200.loop_spec(self.loop, owner_mode='never', inc_mode='atomic', min_blocks=0)
+        loop = b200.ParLoop(kernel, it_space, *args)
+        info = b200.loop_spec(loop, owner_mode='never', inc_mode='atomic', min_blocks=0)
         spec = info['spec']
         if spec.mode not in ("direct", "atomic"):
             raise NotImplementedError("batched loops need direct access or atomic INC "
                                       "(kernel %s)" % kernel.name)
         self.spec = spec
         self.key = spec.key()
-        self.size = int(info['iterset'].size)
-        self.dats = info['dats']
-        self.gbls = info['gbls']
-        self.mats = info['mats']
+        self.iterset = info['iterset']
         specs = info['specs']
-        written = {id(a.data) for a, s in zip(self.loop.args, specs)
+        written = {id(a.data) for a, s in zip(loop.args, specs)
                    if a._is_dat and s.access != "READ"}
+        self.dats = list(info['dats'])
+        self.gbls = list(info['gbls'])
+        self.mats = list(info['mats'])
         self.written = [d for d in self.dats if id(d) in written]
         self.reducing = [g for g, s in zip(self.gbls, [s for s in specs if s.kind == "gbl"])
                          if s.access != "READ"]
-        self.vals = _bind(info)
-        layout = codegen.ParamLayout(spec)
-        self.params = layout.pack(self.size, 0, self.size, self.vals)
+        self.fields = _fields(info)
+        self._finish()
+
+    def _finish(self):
+        self.size = int(self.iterset.size)
+        self.vals = _bind(self.fields)
+        self.params = codegen.ParamLayout(self.spec).pack(self.size, 0, self.size, self.vals)
+
+    def like(self, subs):
+        """The same loop with objects replaced: ``subs`` maps each object of
+        this instance (iteration Set, Maps, Dats, Mats, Globals) to its
+        replacement; objects not listed are shared.  Replacements must have
+        the types, dims and arities of the originals."""
+        new = object.__new__(LoopInstance)
+        new.spec, new.key = self.spec, self.key
+        by_id = {id(k): v for k, v in subs.items()}   # Maps compare by structure
+        r = lambda o: by_id.get(id(o), o)  # noqa: E731
+        new.iterset = r(self.iterset)
+        new.dats = [r(d) for d in self.dats]
+        new.gbls = [r(g) for g in self.gbls]
+        new.mats = [r(m) for m in self.mats]
+        new.written = [r(d) for d in self.written]
+        new.reducing = [r(g) for g in self.reducing]
+        new.fields = [(n, k, tuple(r(x) for x in o) if k == "slots" else r(o))
+                      for n, k, o in self.fields]
+        for (n, k, o), (_, _, o2) in zip(self.fields, new.fields):
+            if k in ("dat", "gbl") and (o.dtype != o2.dtype or o.cdim != o2.cdim):
+                raise ValueError("replacement for %s differs in type or dim" % n)
+            if k == "map" and o.dim != o2.dim:
+                raise ValueError("replacement for %s differs in arity" % n)
+        new._finish()
+        return new
+
+    def patch(self, ptrs):
+        """A :class:`PatchedInstance` of this loop whose arguments bound to
+        the objects in ``ptrs`` (object -> device address) read and write the
+        given addresses instead: raw device memory of the same layout (e.g.
+        a request's arena).  Maps, Sparsity and sizes are shared."""
+        layout = codegen.ParamLayout(self.spec)
+        buf = bytearray(self.params)
+        by_id = {id(k): v for k, v in ptrs.items()}
+        hit = 0
+        for name, kind, o in self.fields:
+            if kind in ("dat", "gbl", "mat") and id(o) in by_id:
+                struct.pack_into("<Q", buf, layout.offset(name), int(by_id[id(o)]))
+                hit += 1
+        if hit == 0:
+            raise ValueError("none of the objects to patch is an argument of the loop")
+        return PatchedInstance(self, bytes(buf))
 
     def sync(self):
         """Upload Dats and Globals whose host copy is newer."""
@@ -121,6 +201,24 @@ class LoopInstance(object):
             g._state = b200.DEVICE
         for m in self.mats:
             m._state = b200.DEVICE
+
+
+class PatchedInstance(object):
+    """A loop instance made by :meth:`LoopInstance.patch`: the template's
+    signature with its own parameter block.  Its data lives in raw device
+    memory owned by the caller, so there is no host copy to synchronise."""
+
+    __slots__ = ("spec", "key", "size", "params")
+
+    def __init__(self, template, params):
+        self.spec, self.key, self.size = template.spec, template.key, template.size
+        self.params = params
+
+    def sync(self):
+        pass
+
+    def mark(self):
+        pass
 
 
 class BatchLoop(object):
@@ -148,22 +246,33 @@ class BatchLoop(object):
         self.spec = spec
         self.config = dict(block_size=spec.block_size, elems_per_thread=spec.batch,
                            min_blocks=spec.min_blocks, ctas_per_sm=int(ctas_per_sm))
-        self.module = b200._get_module(spec)
-        fin_name = codegen.batch_stub_names(spec)[1]
-        self.layout = codegen.BatchLayout(spec)
-        self.has_fin = len(self.layout.fields) > 5
-        self.fin = self.module.function(fin_name) if self.has_fin else 0
+        ckey = (key, spec.block_size, spec.batch, spec.min_blocks)
+        hit = _COMPILED.get(ckey)
+        if hit is None:
+            module = b200._get_module(spec)
+            layout = codegen.BatchLayout(spec)
+            has_fin = len(layout.fields) > 5
+            fin = module.function(codegen.batch_stub_names(spec)[1]) if has_fin else 0
+            occ = module.occupancy(module.fn, spec.block_size)
+            hit = _COMPILED[ckey] = (module, layout, has_fin, fin, occ)
+        self.module, self.layout, self.has_fin, self.fin, occ = hit
         # segments and tiles
         sizes = np.array([inst.size for inst in self.instances], dtype=np.int64)
         tiles, tile_first = build_tiles(sizes, spec.block_size * spec.batch)
         ntiles = int(tile_first[-1])
         self.ntiles, self.nsegs = ntiles, len(sizes)
         self.elements = int(sizes.sum())
-        self._segs = b200._upload(np.frombuffer(b"".join(i.params for i in self.instances),
-                                                dtype=np.uint8))
-        self._tiles = b200._upload(tiles)
-        self._tile_first = b200._upload(tile_first)
-        vals = dict(segs=self._segs.ptr, tiles=self._tiles.ptr, tile_first=self._tile_first.ptr,
+        # one upload: parameter blocks | tiles | first tile per segment
+        segs = b"".join(i.params for i in self.instances)
+        o_tiles = (len(segs) + 15) // 16 * 16
+        o_first = o_tiles + tiles.nbytes
+        host = np.zeros(o_first + tile_first.nbytes, dtype=np.uint8)
+        host[:len(segs)] = np.frombuffer(segs, dtype=np.uint8)
+        host[o_tiles:o_first] = tiles.view(np.uint8)
+        host[o_first:] = tile_first.view(np.uint8)
+        self._meta = b200._upload(host)
+        base = self._meta.ptr
+        vals = dict(segs=base, tiles=base + o_tiles, tile_first=base + o_first,
                     ntiles=ntiles, nsegs=self.nsegs)
         self._gpart = []
         for name in self.layout.fields[5:]:
@@ -173,7 +282,6 @@ class BatchLoop(object):
             self._gpart.append(buf)
             vals[name] = buf.ptr
         self._params = self.layout.pack(vals)
-        occ = self.module.occupancy(self.module.fn, spec.block_size)
         if occ < 1:
             raise DeviceError("batched stub %s cannot be resident at block size %d"
                               % (spec.kernel_name, spec.block_size))

@@ -146,6 +146,10 @@ class ParamLayout(object):
         return struct.pack(self.fmt, set_size, 0, 0, start, end,
                            *[int(values.get(n, 0)) for n in self.fields])
 
+    def offset(self, name):
+        """Byte offset of a field in the packed block."""
+        return struct.calcsize(self.HEADER) + 8 * self.index[name]
+
 
 def _struct_decl(spec, layout):
     lines = ["struct op2b_params {", "  op2b_i64 set_size;", "  int col_first, col_n;",

@@ -208,6 +208,14 @@ int op2b_memcpy_d2h(void *dst, uint64_t src, uint64_t bytes, uint64_t stream) {
   return OP2B_OK;
 }
 
+int op2b_memcpy_d2h_async(void *dst, uint64_t src, uint64_t bytes, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (!bytes) return OP2B_OK;
+  OP2B_CUDA(cudaMemcpyAsync(dst, reinterpret_cast<const void *>(src), bytes,
+                            cudaMemcpyDeviceToHost, stream_of(stream)));
+  return OP2B_OK;
+}
+
 int op2b_memcpy_d2d(uint64_t dst, uint64_t src, uint64_t bytes, uint64_t stream) {
   OP2B_REQUIRE_INIT();
   if (!bytes) return OP2B_OK;
@@ -321,6 +329,19 @@ int op2b_event_record(uint64_t event, uint64_t stream) {
 int op2b_event_sync(uint64_t event) {
   OP2B_REQUIRE_INIT();
   OP2B_CUDA(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(event)));
+  return OP2B_OK;
+}
+
+int op2b_event_query(uint64_t event, int32_t *done) {
+  OP2B_REQUIRE_INIT();
+  if (!done) return set_error(OP2B_ERR_ARG, "op2b_event_query: null out pointer");
+  cudaError_t e = cudaEventQuery(reinterpret_cast<cudaEvent_t>(event));
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return OP2B_OK;
+  }
+  OP2B_CUDA(e);
+  *done = 1;
   return OP2B_OK;
 }
 

@@ -58,5 +58,7 @@ def rel_err(a, b):
     """Normwise relative error max|a-b| / max(max|b|, tiny)."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
+    assert a.size == b.size, "compared arrays differ in size: %s vs %s" % (a.shape, b.shape)
+    a, b = a.reshape(-1), b.reshape(-1)
     scale = max(np.abs(b).max() if b.size else 0.0, 1e-300)
     return float(np.abs(a - b).max() / scale) if a.size else 0.0
