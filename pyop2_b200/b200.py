@@ -455,6 +455,23 @@ class Sparsity(base.Sparsity):
         tables[key] = (buf, rmap, cmap)
         return buf
 
+    def _mat_incidence(self, rmap, cmap):
+        """CSR position -> the (element, r, c) local entries that add to it,
+        in element order (op2b_mat_incidence_build), kept with the
+        Sparsity."""
+        tables = self.__dict__.setdefault("_mat_incidences", {})
+        key = (id(rmap), id(cmap))
+        hit = tables.get(key)
+        if hit is not None:
+            return hit[0]
+        h = C.c_uint64()
+        call("op2b_mat_incidence_build", self._d_rowptr, self._d_colidx, rmap._to_device().ptr,
+             cmap._to_device().ptr, rmap.iterset.size, rmap.dim, cmap.dim, self._d_nz, 0,
+             C.byref(h))
+        inc = Incidence(handle=h.value)
+        tables[key] = (inc, rmap, cmap)
+        return inc
+
     def _max_row_nnz(self):
         """Largest number of stored entries in one row."""
         if getattr(self, "_max_nnz", None) is None:
@@ -684,13 +701,17 @@ def Plan(kernel, iset, *args, **kwargs):
 
 # ---------------------------------------------------------------- incidence
 class Incidence(object):
-    """Target -> sorted (element, map index) list of a Map, on the device."""
+    """Target -> sorted (element, map index) list of a Map, on the device;
+    or, given a handle from op2b_mat_incidence_build, CSR position -> sorted
+    local entries of a Mat assembly."""
 
-    def __init__(self, m):
-        h = C.c_uint64()
-        call("op2b_incidence_build", m._to_device().ptr, m.iterset.size, m.dim, m.dataset.total_size,
-             0, C.byref(h))
-        self._handle = h.value
+    def __init__(self, m=None, handle=None):
+        if handle is None:
+            h = C.c_uint64()
+            call("op2b_incidence_build", m._to_device().ptr, m.iterset.size, m.dim,
+                 m.dataset.total_size, 0, C.byref(h))
+            handle = h.value
+        self._handle = handle
         p, lst, md = C.c_uint64(), C.c_uint64(), C.c_int32()
         call("op2b_incidence_arrays", self._handle, C.byref(p), C.byref(lst), C.byref(md))
         self.ptr, self.list, self.max_degree = p.value, lst.value, md.value
@@ -967,6 +988,9 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
         spec.owner = owner
         spec.mode = "owner"
         indirect = False
+    elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'lma' and codegen.lma_capable(spec):
+        spec.mode = "lma"
+        indirect = False   # launched like a direct loop, then reduced per target
     elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'atomic' and codegen.atomic_capable(spec):
         spec.mode = "atomic"
         indirect = False   # launched like a direct loop: no plan
@@ -1070,6 +1094,29 @@ class _BoundLoop(object):
         if indirect:
             self.grid = 0
             self.max_grid = self.plan.max_blocks_per_color
+        elif spec.mode == "lma":
+            # two-phase INC: contribution arrays (phase 1, the stub) and the
+            # incidences their reduction walks (phase 2, op2b_lma_reduce)
+            self.lma = []
+            self.kahan = bool(cfg.cfg['kahan'])
+            for j, m in enumerate(mats):
+                s = next(a for a in specs if a.kind == "mat" and a.slot == j)
+                rmap, cmap = maps[s.mslot], maps[s.cmslot]
+                buf = DeviceBuffer(max(1, n * rmap.dim * cmap.dim) * 8)
+                vals["lm%d" % j] = buf.ptr
+                inc = m.sparsity._mat_incidence(rmap, cmap)
+                self.lma.append((buf, inc, m, 1, m.sparsity._d_nz, rmap.dim * cmap.dim,
+                                 (1 << (rmap.dim * cmap.dim)) - 1))
+            for k, st in enumerate(stages):
+                d, mp = dats[st[0]], maps[st[1]]
+                buf = DeviceBuffer(max(1, n * mp.dim * st[3]) * 8)
+                vals["ld%d" % k] = buf.ptr
+                mask = 0
+                for ix in st[4]:
+                    mask |= 1 << ix
+                self.lma.append((buf, _incidence(mp), d, st[3], mp.dataset.size, mp.dim, mask))
+            self.grid = max(1, min((n + bs - 1) // bs, _state['sm_count'] * 8)) if n else 0
+            self.max_grid = self.grid
         elif spec.mode == "owner":
             # one warp per target of the owner Map
             omap = maps[spec.owner["mslot"]]
@@ -1127,6 +1174,12 @@ class _BoundLoop(object):
                  self.smem, 0, params, self.layout.nbytes, codegen.ParamLayout.COL_OFFSET)
         else:
             call("op2b_launch", mod.fn, self.grid, self.block_size, 0, 0, params, self.layout.nbytes)
+        if self.spec.mode == "lma":
+            kahan = int(self.kahan)
+            for buf, inc, target, cdim, ntargets, arity, mask in self.lma:
+                out = target._device_values().ptr if isinstance(target, Mat) else target._device.ptr
+                call("op2b_lma_reduce", out, cdim, inc.ptr, inc.list, ntargets, buf.ptr, n,
+                     arity, mask, kahan, 0)
         for j, d in enumerate(self.dats):
             if any(m != "READ" for m in self.dat_access[id(d)]):
                 d._state = DEVICE

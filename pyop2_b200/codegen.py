@@ -132,6 +132,10 @@ class ParamLayout(object):
             f += ["mv%d" % j, "mr%d" % j, "mc%d" % j]
             if spec.mat_slots:
                 f.append("ms%d" % j)
+            if spec.mode == "lma":
+                f.append("lm%d" % j)
+        if spec.mode == "lma":
+            f += ["ld%d" % k for k in range(len(spec.stages))]
         for j, g in enumerate(spec.gbls):
             f.append("g%d" % j)
             if g[2] != "READ":
@@ -167,6 +171,10 @@ def _struct_decl(spec, layout):
             t = "%s *" % spec.dats[int(n[1:])][0]
         elif n.startswith("mv"):
             t = "%s *" % spec.mats[int(n[2:])]
+        elif n.startswith("lm"):
+            t = "%s *" % spec.mats[int(n[2:])]
+        elif n.startswith("ld"):
+            t = "%s *" % spec.stages[int(n[2:])][2]
         elif n.startswith("mr") or n.startswith("mc") or n.startswith("m"):
             t = "const int *"
         elif n.startswith("gp"):
@@ -235,8 +243,8 @@ def generate(spec):
     if spec.batch:
         w(_batch_body(spec))
         return "\n".join(out), layout, batch_stub_names(spec)[0]
-    body = {"plan": _indirect_body, "atomic": _atomic_body, "direct": _direct_body,
-            "owner": _owner_body}[spec.mode](spec)
+    body = {"plan": _indirect_body, "atomic": _atomic_body, "lma": _atomic_body,
+            "direct": _direct_body, "owner": _owner_body}[spec.mode](spec)
     w(body)
     return "\n".join(out), layout, stub_name(spec)
 
@@ -511,8 +519,19 @@ def _atomic_body(spec):
     return "\n".join(L)
 
 
+def _inc_sink(spec, a, n, k, src, val, ind):
+    """Add the INC row ``val`` of arg n (map position k, row address src):
+    an atomic add, or in the two-phase form a store to the contribution array
+    of the arg's (Dat, Map) pair."""
+    if spec.mode == "lma":
+        return "%sop2b_store(p.ld%d + ((op2b_i64)%d * p.set_size + e) * %d, %s);" % (
+            ind, a.stage, k, a.cdim, val)
+    return "%sop2b_atomic_row(%s, %s);" % (ind, src, val)
+
+
 def _atomic_element(spec, ind):
-    """Lines computing element ``e`` of an atomic-mode indirect loop."""
+    """Lines computing element ``e`` of an atomic-mode (or two-phase)
+    indirect loop."""
     L = []
     used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
                        {a.cmslot for a in spec.args if a.kind == "mat"})
@@ -531,7 +550,7 @@ def _atomic_element(spec, ind):
             row = "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, a.idx, c)
             if a.access == "INC":
                 pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind, t, n, c, n))
-                apply.append("%sop2b_atomic_row(%s, a%d);" % (ind, row, n))
+                apply.append(_inc_sink(spec, a, n, a.idx, row, "a%d" % n, ind))
                 exprs.append("a%d" % n)
             elif a.access == "READ":
                 pre.append("%s__align__(16) %s a%d[%d];" % (ind, t, n, c))
@@ -550,7 +569,7 @@ def _atomic_element(spec, ind):
                         pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], %s);" % (ind, t, c, _ro(a), n, r, src))
                     else:
                         pre.append("%sop2b_zero(a%d[%d]);" % (ind, n, r))
-                        apply.append("%sop2b_atomic_row(%s, a%d[%d]);" % (ind, src, n, r))
+                        apply.append(_inc_sink(spec, a, n, r, src, "a%d[%d]" % (n, r), ind))
                 if a.kind == "vec":
                     pre.append("%s%s *a%d_v[%d] = {%s};" %
                                (ind, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
@@ -573,7 +592,7 @@ def _atomic_element(spec, ind):
             else:
                 pre.append("%s%s A%d[%d][%d][%d][%d];" % (ind, t, n, e0, e1, a.rm, a.cm))
                 exprs.append("A%d[i0][i1]" % n)
-            apply += _mat_addto(spec, n, a, ind, atomic=True)
+            apply += _mat_addto(spec, n, a, ind, atomic=True, lma=spec.mode == "lma")
     L += pre
     L += _itspace_open(spec, ind)
     deep = ind + "  " * len(spec.extents)
@@ -907,6 +926,29 @@ def owner_plan(spec, mat_row_nnz_max=None):
     return {"kind": "dat", "arg": writers[0], "arity": ws[0].arity, "mslot": ws[0].mslot}
 
 
+def lma_capable(spec):
+    """True if the two-phase form can run the loop: every INC goes to a
+    float64 Dat (row of 1 to 4 values) through a Map of arity <= 64 with
+    each map position at most once per (Dat, Map) pair, or to a scalar
+    float64 Mat over its full local tensor; no Mat WRITE and no Global
+    reduction ordering issue (Globals reduce as usual)."""
+    if not any(a.kind == "mat" or (a.kind in ("ind", "vec", "its") and a.access == "INC")
+               for a in spec.args):
+        return False
+    for st in spec.stages:
+        if st[2] != "double" or not 1 <= st[3] <= 4 or len(set(st[4])) != len(st[4]):
+            return False
+        if spec.maps[st[1]] > 64:
+            return False
+    for a in spec.args:
+        if a.kind == "mat":
+            if (a.access != "INC" or a.ctype != "double" or a.rm * a.cm != 1
+                    or (spec.extents[a.idx], spec.extents[a.cidx]) != (a.arity, a.carity)
+                    or a.arity * a.carity > 64):
+                return False
+    return True
+
+
 def atomic_capable(spec):
     """True if every INC target of the loop has a native atomic add and no
     Mat is written with WRITE (insertion needs the coloured form)."""
@@ -919,7 +961,7 @@ def atomic_capable(spec):
     return True
 
 
-def _mat_addto(spec, n, a, ind, atomic=False):
+def _mat_addto(spec, n, a, ind, atomic=False, lma=False):
     """Add / insert the local tensor of Mat arg n into the CSR values
     (pyop2/host.py:145-184: scalar fields add the whole block, vector fields
     add entry by entry and skip zero values when adding)."""
@@ -930,6 +972,13 @@ def _mat_addto(spec, n, a, ind, atomic=False):
     L.append("%sfor (int i0 = 0; i0 < %d; ++i0) for (int i1 = 0; i1 < %d; ++i1) {" % (ind, e0, e1))
     ri = "i%d" % a.idx
     ci = "i%d" % a.cidx
+    if lma:
+        # two-phase form: the local entry goes to the contribution array at
+        # k = r * ca + c; op2b_lma_reduce adds it to its CSR slot
+        L.append("%s  p.lm%d[((op2b_i64)(%s * %d + %s)) * p.set_size + e] = A%d[i0][i1];"
+                 % (ind, j, ri, a.carity, ci, n))
+        L.append("%s}" % ind)
+        return L
     if a.rm * a.cm == 1:
         L.append("%s  const int row = mr%d[%s], colj = mr%d[%s];" % (ind, a.mslot, ri, a.cmslot, ci))
         if spec.mat_slots and atomic:

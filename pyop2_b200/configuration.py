@@ -18,8 +18,12 @@ keys of the B200 backend:
   none), which caps registers per thread to raise occupancy;
 * ``inc_mode``: how indirect loops resolve INC conflicts: ``'color'`` (plan
   with block and thread colouring; deterministic, bit-identical from run to
-  run) or ``'atomic'`` (one launch, atomic adds; summation order varies
-  between runs within rounding);
+  run), ``'atomic'`` (one launch, atomic adds; summation order varies
+  between runs within rounding) or ``'lma'`` (two phases: the stub stores
+  every contribution, then each target adds its contributions in element
+  order -- the sequential backend's order -- optionally Kahan-compensated;
+  deterministic and independent of the launch configuration; loops it cannot
+  run fall back to ``'color'``);
 * ``owner_mode``: owner-computes for loops whose only write is INC into one
   Dat through one Map or into one scalar Mat: one warp per target adds the
   target's contributions in the sequential backend's order and writes it once
@@ -29,7 +33,8 @@ keys of the B200 backend:
   ``'never'`` (default) leaves those loops to ``inc_mode``.  It is slower than
   the atomic form where kernels index tables with the iteration-space index
   (the index becomes a run-time value per lane);
-* ``kahan``: compensated (Kahan) summation of owner-computes accumulation;
+* ``kahan``: compensated (Kahan) summation of owner-computes and two-phase
+  (``inc_mode='lma'``) accumulation;
 * ``mat_slots``: assemble scalar Mats in the atomic form through a cached
   scatter-slot table (the CSR position of every element's local entries,
   built once per Sparsity and Map pair: nelem x arity^2 int32 of device

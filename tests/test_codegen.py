@@ -277,3 +277,40 @@ def test_batch_layout_fields(host_op2):
     lay = codegen.BatchLayout(spec)
     assert lay.fields == ["segs", "tiles", "tile_first", "ntiles", "nsegs", "gpart0"]
     assert lay.nbytes == 48
+
+
+def test_two_phase_forms(host_op2):
+    """Two-phase (inc_mode='lma') stubs: Mat INC, vec-map and indexed Dat INC
+    write contribution arrays instead of adding."""
+    from pyop2_b200 import b200
+    op2 = host_op2
+    e = op2.Set(4, 1)
+    n = op2.Set(6, 1)
+    vn = op2.Set(6, 2)
+    em = op2.Map(e, n, 3, np.array([0, 1, 2, 1, 2, 3, 2, 3, 4, 3, 4, 5], np.int32))
+    evm = op2.Map(e, vn, 3, np.array([0, 1, 2, 1, 2, 3, 2, 3, 4, 3, 4, 5], np.int32))
+    xy = op2.Dat(vn, np.zeros(12), np.float64)
+    b = op2.Dat(n, np.zeros(6), np.float64)
+    mat = op2.Mat(op2.Sparsity((em, em)), np.float64)
+    km = op2.Kernel("void km(double A[1][1], double *x[2], int j, int k) { A[0][0] += x[j][0]; }", "km")
+    spec = b200.loop_spec(b200.ParLoop(km, e(3, 3), mat((em[op2.i[0]], em[op2.i[1]]), op2.INC),
+                                       xy(evm, op2.READ)), inc_mode='lma', owner_mode='never',
+                          mat_nnz_max=8)["spec"]
+    assert spec.mode == "lma"
+    src, layout, _ = nvrtc_compile(spec)
+    assert "p.lm0[" in src and "lm0" in layout.fields and "op2b_atomic" not in src.split("op2b_user")[-1]
+    kv = op2.Kernel("void kv(double *b[1], double *x[2]) { b[0][0] += x[0][0]; b[2][0] += 1.0; }", "kv")
+    spec = b200.loop_spec(b200.ParLoop(kv, e, b(em, op2.INC), xy(evm, op2.READ)),
+                          inc_mode='lma', owner_mode='never')["spec"]
+    assert spec.mode == "lma"
+    src, layout, _ = nvrtc_compile(spec)
+    assert "p.ld0" in src and "ld0" in layout.fields
+    ki = op2.Kernel("void ki(double *b0, double *b1) { *b0 += 1.0; *b1 += 2.0; }", "ki")
+    spec = b200.loop_spec(b200.ParLoop(ki, e, b(em[0], op2.INC), b(em[2], op2.INC)),
+                          inc_mode='lma', owner_mode='never')["spec"]
+    assert spec.mode == "lma"
+    nvrtc_compile(spec)
+    # the same map index twice in one loop: no two-phase form
+    spec = b200.loop_spec(b200.ParLoop(ki, e, b(em[0], op2.INC), b(em[0], op2.INC)),
+                          inc_mode='lma', owner_mode='never')["spec"]
+    assert spec.mode == "plan"

@@ -32,7 +32,7 @@ def _clear_consts(op2mod):
     seq._CONSTS.clear()
 
 
-@pytest.fixture(params=["atomic", "color"])
+@pytest.fixture(params=["atomic", "color", "lma"])
 def inc_mode(request):
     """Run a test under both INC conflict strategies of indirect loops."""
     from pyop2_b200 import configuration as cfg
@@ -226,3 +226,62 @@ def test_p1_mass_regression_golden(op2):
     assert np.abs(vals - golden).max() < 1e-12 * np.abs(golden).max()
     assert abs(gm.array.sum() - float(z["mat_sum"])) < 1e-12
     assert abs(gb.data_ro.sum() - float(z["b_sum"])) < 1e-12
+
+
+def test_two_phase_is_bit_exact_and_launch_independent(op2):
+    """inc_mode='lma' adds each target's contributions in element order
+    starting from its current value -- the sequential backend's order -- so
+    the Mat and the airfoil residual equal the oracle bit for bit, and the
+    result does not depend on the block size."""
+    from pyop2_b200 import configuration as cfg
+    old = (cfg.cfg['inc_mode'], cfg.cfg['block_size'])
+    try:
+        mats = []
+        for bs in (128, 512):
+            cfg.configure(inc_mode='lma', block_size=bs)
+            coords, elem = meshes.square_p1(40)
+            fvals = np.sin(np.pi * coords[:, 0]) * np.sin(np.pi * coords[:, 1])
+            gm, gb, _ = _p1(op2, coords, elem, fvals)
+            mats.append((gm.array.copy(), gb.data_ro.copy()))
+        om, ob, _ = _p1(seq, coords, elem, fvals)
+        np.testing.assert_array_equal(mats[0][0], om.array)
+        np.testing.assert_array_equal(mats[0][0], mats[1][0])
+        np.testing.assert_array_equal(mats[0][1], mats[1][1])
+        assert rel_err(mats[0][1], ob.data) < 1e-15
+        _clear_consts(op2)
+        grid = meshes.airfoil_grid(30, 16, 5)
+        G = airfoil.build(op2, 30, 16, 5, grid=grid)
+        O = airfoil.build(seq, 30, 16, 5, grid=grid)
+        for api, A in ((op2, G), (seq, O)):
+            airfoil.save_soln(api, A)
+            airfoil.adt_calc(api, A)
+            airfoil.res_calc(api, A)
+            airfoil.bres_calc(api, A)
+        np.testing.assert_array_equal(G.p_res.data_ro, O.p_res.data)
+    finally:
+        cfg.configure(inc_mode=old[0], block_size=old[1])
+        _clear_consts(op2)
+
+
+def test_two_phase_kahan_precision_form(op2):
+    """FP32 element kernels with FP64 Kahan accumulation (inc_mode='lma',
+    kahan=True): the P2 stiffness and mass Mats within the FP32 element
+    error of the FP64 oracle, and equal to the uncompensated sum within
+    rounding."""
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import fem
+    old = (cfg.cfg['inc_mode'], cfg.cfg['kahan'])
+    try:
+        out = {}
+        for kahan in (True, False):
+            cfg.configure(inc_mode='lma', kahan=kahan)
+            P = fem.build_p2(op2, 12, seed=3, precision="f32")
+            fem.assemble_p2(op2, P)
+            out[kahan] = (P.K.array.copy(), P.M.array.copy())
+        Q = fem.build_p2(seq, 12, seed=3, precision="f64")
+        fem.assemble_p2(seq, Q)
+        assert rel_err(out[True][0], Q.K.array) < 1e-5
+        assert rel_err(out[True][1], Q.M.array) < 1e-5
+        assert rel_err(out[True][0], out[False][0]) < 1e-14
+    finally:
+        cfg.configure(inc_mode=old[0], kahan=old[1])
