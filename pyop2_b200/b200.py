@@ -20,6 +20,7 @@ HOST (host copy newer), DEVICE (device copy newer), BOTH.
 import ctypes as C
 import hashlib
 import os
+import struct
 import weakref
 
 import numpy as np
@@ -1141,33 +1142,63 @@ class _BoundLoop(object):
                 objs.append(a.data)
         return all(r() is not None for r in self.refs)
 
-    def run(self, loop):
+    def _prepare(self, loop):
+        """First run: device copies of the Dats, the full parameter block in a
+        persistent buffer, and the bookkeeping later runs need."""
         vals = self.vals
         for j, d in enumerate(self.dats):
             if d._state is DEVICE_UNALLOCATED and id(d) in self.write_only:
                 d._allocate_device()
                 d._state = DEVICE
-            d._allocate_device()
-            if d._state is HOST:
-                d._to_device()
+            d._to_device()
             vals["d%d" % j] = d._device.ptr
             if d.soa:
                 vals["ds%d" % j] = d.dataset.total_size
-            maybe_setflags(d._data, write=False)
+        gargs = [k for k, a in enumerate(loop.args) if a._is_global]
+        # (field offset of the pointer, arg index, reducing?, offsets of partials/counter)
+        self._gbl = []
         for j, s in enumerate(self.gbl_specs):
-            g = loop.args[[k for k, a in enumerate(loop.args) if a._is_global][j]].data
+            red = s.access != "READ"
+            self._gbl.append((self.layout.offset("g%d" % j), gargs[j], red,
+                              self.layout.offset("gp%d" % j) if red else 0,
+                              self.layout.offset("gc%d" % j) if red else 0))
+        self._gptr = [None] * len(self._gbl)
+        self._written = [d for d in self.dats if any(m != "READ" for m in self.dat_access[id(d)])]
+        self._reducing = [k for k, (_, _, red, _, _) in enumerate(self._gbl) if red]
+        n = self.iterset.size
+        self._buf = C.create_string_buffer(self.layout.pack(n, 0, self.range_end, vals),
+                                           self.layout.nbytes)
+
+    def run(self, loop):
+        if getattr(self, "_buf", None) is None:
+            self._prepare(loop)
+        for d in self.dats:
+            st = d._state
+            if st is HOST:
+                d._to_device()
+            elif st is DEVICE_UNALLOCATED:
+                raise DeviceError("Dat %s lost its device copy" % d.name)
+        buf = self._buf
+        args = loop.args
+        for k, (off, ai, red, offp, offc) in enumerate(self._gbl):
+            g = args[ai].data
             g._to_device()
-            vals["g%d" % j] = g._device.ptr
-            if s.access != "READ":
-                pp, cc = g._reduction_buffers(self.max_grid)
-                vals["gp%d" % j] = pp
-                vals["gc%d" % j] = cc
+            # the Global, and its reduction scratch (which another loop with a
+            # larger grid may have reallocated), as this loop's block holds them
+            ptrs = (g._device.ptr,) + (g._reduction_buffers(self.max_grid) if red else ())
+            if ptrs != self._gptr[k]:
+                struct.pack_into("<Q", buf, off, ptrs[0])
+                if red:
+                    struct.pack_into("<Q", buf, offp, ptrs[1])
+                    struct.pack_into("<Q", buf, offc, ptrs[2])
+                self._gptr[k] = ptrs
         mod = self.module
-        _sync_consts(mod, self.consts)
+        if self.consts:
+            _sync_consts(mod, self.consts)
         n = self.iterset.size
         if n == 0:
             return
-        params = C.create_string_buffer(self.layout.pack(n, 0, self.range_end, vals), self.layout.nbytes)
+        params = buf
         if self.indirect:
             plan = self.plan
             call("op2b_launch_colored", mod.fn, plan.ncolors, plan.ncolblk_host, self.block_size,
@@ -1180,15 +1211,29 @@ class _BoundLoop(object):
                 out = target._device_values().ptr if isinstance(target, Mat) else target._device.ptr
                 call("op2b_lma_reduce", out, cdim, inc.ptr, inc.list, ntargets, buf.ptr, n,
                      arity, mask, kahan, 0)
-        for j, d in enumerate(self.dats):
-            if any(m != "READ" for m in self.dat_access[id(d)]):
-                d._state = DEVICE
-        for j, s in enumerate(self.gbl_specs):
-            if s.access != "READ":
-                g = loop.args[[k for k, a in enumerate(loop.args) if a._is_global][j]].data
-                g._state = DEVICE
+        for d in self._written:
+            d._state = DEVICE
+            maybe_setflags(d._data, write=False)
+        for k in self._reducing:
+            args[self._gbl[k][1]].data._state = DEVICE
         for m in self.mats:
             m._state = DEVICE
+
+
+_ENV = {"gen": None, "key": None}
+
+
+def _env_key():
+    """The part of a loop's cache key that the Consts and the configuration
+    give, recomputed only when either changed."""
+    gen = (cfg.generation(), base.Const._generation)
+    if _ENV["gen"] != gen:
+        _ENV["key"] = (tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()),
+                       (cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
+                        cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode'], cfg.cfg['owner_mode'],
+                        cfg.cfg['kahan'], cfg.cfg['mat_slots']))
+        _ENV["gen"] = gen
+    return _ENV["key"]
 
 
 class ParLoop(base.ParLoop):
@@ -1207,10 +1252,7 @@ class ParLoop(base.ParLoop):
                 ix = a.idx.index if isinstance(a.idx, IterationIndex) else a.idx
                 k.append(("d", id(a.data), id(a.map), isinstance(a.idx, IterationIndex), ix,
                           a.access._mode))
-        k.append(tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()))
-        k.append((cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
-                  cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode'], cfg.cfg['owner_mode'],
-                  cfg.cfg['kahan'], cfg.cfg['mat_slots']))
+        k.append(_env_key())
         return tuple(k)
 
     def compute(self):

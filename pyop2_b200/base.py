@@ -483,6 +483,7 @@ class Const(DataCarrier):
 
     _defs = set()
     _globalcount = 0
+    _generation = 0     # changes whenever the set of definitions changes
 
     @validate_type(('name', str, NameTypeError))
     def __init__(self, dim, data=None, name=None, dtype=None):
@@ -496,6 +497,7 @@ class Const(DataCarrier):
                 "OP2 Constants are globally scoped, %s is already in use" % self._name)
         Const._defs.add(self)
         Const._globalcount += 1
+        Const._generation += 1
 
     @property
     def data(self):
@@ -521,6 +523,7 @@ class Const(DataCarrier):
     def remove_from_namespace(self):
         """Remove this Const from the namespace (the name may be reused)."""
         Const._defs.discard(self)
+        Const._generation += 1
 
     def _format_declaration(self):
         d = {'type': self.ctype, 'name': self.name, 'dim': self.cdim}

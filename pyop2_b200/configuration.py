@@ -66,16 +66,26 @@ _defaults = {
 _config = dict(_defaults)
 
 
+_generation = [0]
+
+
+def generation():
+    """Changes whenever the configuration may have changed (cache keys)."""
+    return _generation[0]
+
+
 def configure(**kwargs):
     for k, v in kwargs.items():
         if k == 'log_level' and v is None:
             continue
         _config[k] = v
+    _generation[0] += 1
 
 
 def reset():
     _config.clear()
     _config.update(_defaults)
+    _generation[0] += 1
 
 
 def __getitem__(key):  # pragma: no cover - module-level item access shim

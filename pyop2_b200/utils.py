@@ -55,28 +55,35 @@ class _validate_base(object):
         varnames = code.co_varnames[:code.co_argcount]
         defaults = f.__defaults__ or ()
         where = "%s:%d" % (code.co_filename, code.co_firstlineno + 1)
+        # positions resolved once: (name, position, index into defaults or -1)
+        plan = []
+        for argname, cond, exception in self._checks:
+            if argname in varnames:
+                i = varnames.index(argname)
+                di = i - len(varnames) + len(defaults)
+                plan.append((argname, i, di, cond, exception))
+        check = self.check_arg
 
         @functools.wraps(f)
         def wrapper(*args, **kwargs):
-            for argname, cond, exception in self._checks:
-                try:
-                    i = varnames.index(argname)
-                except ValueError:
-                    continue
-                if argname in kwargs:
-                    arg = kwargs[argname]
-                elif i < len(args):
+            n = len(args)
+            for argname, i, di, cond, exception in plan:
+                if i < n:
                     arg = args[i]
+                elif kwargs and argname in kwargs:
+                    arg = kwargs[argname]
                 else:
                     continue
-                di = i - len(varnames) + len(defaults)
                 if di >= 0:
+                    d = defaults[di]
+                    if arg is d:
+                        continue
                     try:
-                        if arg is defaults[di] or (not isinstance(arg, np.ndarray) and arg == defaults[di]):
+                        if not isinstance(arg, np.ndarray) and arg == d:
                             continue
                     except Exception:
                         pass
-                self.check_arg(arg, cond, exception, where)
+                check(arg, cond, exception, where)
             return f(*args, **kwargs)
         return wrapper
 
