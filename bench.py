@@ -781,7 +781,7 @@ def main(argv=None):
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")
     p.add_argument("--no-permute", action="store_true",
                    help="structured (unpermuted) cell/node numbering instead of the random one")
-    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic"],
+    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic", "lma"],
                    help="INC conflict resolution of indirect loops (default: backend default)")
     args = p.parse_args(argv)
     _set_mesh(args.nx, args.ny)

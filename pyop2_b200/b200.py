@@ -105,6 +105,9 @@ class DeviceBuffer(object):
     __slots__ = ("ptr", "nbytes", "__weakref__")
 
     def __init__(self, nbytes):
+        if _state.get('capturing'):
+            raise DeviceError("device memory requested while recording a CUDA graph: run every "
+                              "loop (and create its Globals) once before capture()")
         self.nbytes = int(nbytes)
         p = C.c_uint64()
         call("op2b_malloc", C.byref(p), max(self.nbytes, 16))
@@ -1356,9 +1359,11 @@ class capture(object):
     def __enter__(self):
         self.graph = Graph()
         call("op2b_graph_begin", 0)
+        _state['capturing'] = True
         return self.graph
 
     def __exit__(self, exc_type, exc, tb):
+        _state['capturing'] = False
         h = C.c_uint64()
         rc = _lib._lib.op2b_graph_end(0, C.byref(h))
         if exc_type is None:

@@ -601,3 +601,27 @@ class TestConstant:
         op2.par_loop(k, cset, dat(op2.IdentityMap, op2.WRITE))
         c.remove_from_namespace()
         assert all(dat.data == 11)
+
+
+class TestCapture:
+    """Loops recorded into a CUDA graph (b200.capture) replay the recorded
+    work; a Global first used inside the recording is refused."""
+
+    def test_replay_and_fresh_global_refused(self, op2):
+        from pyop2_b200 import b200
+        from pyop2_b200.exceptions import DeviceError
+        s = op2.Set(1000)
+        x = op2.Dat(s, np.arange(1000, dtype=np.float64), np.float64)
+        g = op2.Global(1, 0.0, np.float64)
+        k = op2.Kernel("void kc(double *x, double *g) { x[0] += 1.0; g[0] += x[0]; }", "kc")
+        op2.par_loop(k, s, x(op2.IdentityMap, op2.RW), g(op2.INC))
+        with b200.capture() as graph:
+            op2.par_loop(k, s, x(op2.IdentityMap, op2.RW), g(op2.INC))
+        graph.launch()
+        graph.launch()
+        np.testing.assert_array_equal(x.data_ro.reshape(-1), np.arange(1000) + 3.0)
+        fresh = op2.Global(1, 0.0, np.float64)
+        with pytest.raises(DeviceError):
+            with b200.capture():
+                op2.par_loop(k, s, x(op2.IdentityMap, op2.RW), fresh(op2.INC))
+        graph.close()
