@@ -62,6 +62,12 @@ int op2b_host_alloc(uint64_t *hptr, uint64_t bytes);   /* pinned host memory */
 int op2b_host_free(uint64_t hptr);
 int op2b_memcpy_h2d(uint64_t dst, const void *src, uint64_t bytes, uint64_t stream);
 int op2b_memcpy_d2h(void *dst, uint64_t src, uint64_t bytes, uint64_t stream);
+/* Host-to-device copy of at most 256 bytes carried in the launch parameters
+ * of a one-block kernel: asynchronous from any host memory (the bytes are
+ * captured at the call), so uploading a Global's value never waits for the
+ * stream as a pageable-memory copy does.  No reference counterpart (PyCUDA
+ * copied Globals with synchronous memcpy_htod, pyop2/cuda.py:325-340). */
+int op2b_memcpy_h2d_small(uint64_t dst, const void *src, uint64_t bytes, uint64_t stream);
 /* Device-to-host copy that returns at once (stream-ordered; complete when an
  * event recorded after it completes).  dst must be pinned host memory
  * (op2b_host_alloc) for the copy to be asynchronous. */

@@ -32,6 +32,7 @@ _SIGS = {
     "op2b_memcpy_h2d": [u64, P, u64, u64],
     "op2b_memcpy_d2h": [P, u64, u64, u64],
     "op2b_memcpy_d2h_async": [P, u64, u64, u64],
+    "op2b_memcpy_h2d_small": [u64, P, u64, u64],
     "op2b_memcpy_d2d": [u64, u64, u64, u64],
     "op2b_memset": [u64, C.c_int, u64, u64],
     "op2b_transpose": [u64, u64, i64, i32, i32, i32, u64],

@@ -312,8 +312,6 @@ class Global(DeviceDataMixin, base.Global):
         base.Global.__init__(self, dim, data, dtype, name)
         self._state = DEVICE_UNALLOCATED
         self._device = None
-        self._partials = None
-        self._counter = None
 
     @property
     def data(self):
@@ -342,23 +340,18 @@ class Global(DeviceDataMixin, base.Global):
             self._device = DeviceBuffer(max(self._data.nbytes, 16))
             self._state = HOST
         if self._state is HOST:
-            self._device.from_host(self._data)
+            data = np.ascontiguousarray(self._data)
+            if data.nbytes <= 256:
+                # carried in launch parameters: does not wait for the stream
+                call("op2b_memcpy_h2d_small", self._device.ptr, data.ctypes.data, data.nbytes, 0)
+            else:
+                self._device.from_host(data)
             self._state = BOTH
 
     def _from_device(self):
         if self._state is DEVICE:
             self._device.to_host(self._data)
             self._state = BOTH
-
-    def _reduction_buffers(self, nblocks):
-        """Per-CTA partials and the arrival counter of op2b_reduce (scratch)."""
-        need = max(1, nblocks) * self.cdim * self.dtype.itemsize
-        if self._partials is None or self._partials.nbytes < need:
-            self._partials = DeviceBuffer(need)
-        if self._counter is None:
-            self._counter = DeviceBuffer(16)
-            self._counter.memset(0)
-        return self._partials.ptr, self._counter.ptr
 
 
 _MAP_DEVICE = weakref.WeakValueDictionary()
@@ -1158,16 +1151,24 @@ class _BoundLoop(object):
             if d.soa:
                 vals["ds%d" % j] = d.dataset.total_size
         gargs = [k for k, a in enumerate(loop.args) if a._is_global]
-        # (field offset of the pointer, arg index, reducing?, offsets of partials/counter)
+        # (field offset of the Global's pointer, arg index, reducing?)
         self._gbl = []
+        # reduction scratch belongs to the loop, not to the Global: launches of
+        # one stream never overlap, and the last CTA leaves the counter at 0
+        self._scratch = []
         for j, s in enumerate(self.gbl_specs):
             red = s.access != "READ"
-            self._gbl.append((self.layout.offset("g%d" % j), gargs[j], red,
-                              self.layout.offset("gp%d" % j) if red else 0,
-                              self.layout.offset("gc%d" % j) if red else 0))
+            self._gbl.append((self.layout.offset("g%d" % j), gargs[j], red))
+            if red:
+                g = loop.args[gargs[j]].data
+                part = DeviceBuffer(max(1, self.max_grid) * g.cdim * g.dtype.itemsize)
+                cnt = DeviceBuffer(16)
+                cnt.memset(0)
+                self._scratch += [part, cnt]
+                vals["gp%d" % j], vals["gc%d" % j] = part.ptr, cnt.ptr
         self._gptr = [None] * len(self._gbl)
         self._written = [d for d in self.dats if any(m != "READ" for m in self.dat_access[id(d)])]
-        self._reducing = [k for k, (_, _, red, _, _) in enumerate(self._gbl) if red]
+        self._reducing = [k for k, (_, _, red) in enumerate(self._gbl) if red]
         n = self.iterset.size
         self._buf = C.create_string_buffer(self.layout.pack(n, 0, self.range_end, vals),
                                            self.layout.nbytes)
@@ -1183,18 +1184,13 @@ class _BoundLoop(object):
                 raise DeviceError("Dat %s lost its device copy" % d.name)
         buf = self._buf
         args = loop.args
-        for k, (off, ai, red, offp, offc) in enumerate(self._gbl):
+        for k, (off, ai, red) in enumerate(self._gbl):
             g = args[ai].data
             g._to_device()
-            # the Global, and its reduction scratch (which another loop with a
-            # larger grid may have reallocated), as this loop's block holds them
-            ptrs = (g._device.ptr,) + (g._reduction_buffers(self.max_grid) if red else ())
-            if ptrs != self._gptr[k]:
-                struct.pack_into("<Q", buf, off, ptrs[0])
-                if red:
-                    struct.pack_into("<Q", buf, offp, ptrs[1])
-                    struct.pack_into("<Q", buf, offc, ptrs[2])
-                self._gptr[k] = ptrs
+            ptr = g._device.ptr
+            if ptr != self._gptr[k]:
+                struct.pack_into("<Q", buf, off, ptr)
+                self._gptr[k] = ptr
         mod = self.module
         if self.consts:
             _sync_consts(mod, self.consts)

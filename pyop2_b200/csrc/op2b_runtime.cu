@@ -71,6 +71,16 @@ __global__ void transpose_kernel(T *__restrict__ dst, const T *__restrict__ src,
   }
 }
 
+// Host bytes carried by value in the launch parameters: a small upload that
+// needs no staging buffer and never waits for the stream.
+struct SmallBytes {
+  unsigned char b[256];
+};
+
+__global__ void small_copy_kernel(unsigned char *__restrict__ dst, SmallBytes v, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = v.b[i];
+}
+
 // Writes the smallest offending position (or INT64_MAX) to *bad.
 __global__ void map_validate_kernel(const int32_t *__restrict__ map, int64_t n, int32_t to_size,
                                     unsigned long long *bad) {
@@ -206,6 +216,19 @@ int op2b_memcpy_d2h(void *dst, uint64_t src, uint64_t bytes, uint64_t stream) {
                             cudaMemcpyDeviceToHost, s));
   OP2B_CUDA(cudaStreamSynchronize(s));
   return OP2B_OK;
+}
+
+int op2b_memcpy_h2d_small(uint64_t dst, const void *src, uint64_t bytes, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (bytes > sizeof(SmallBytes::b))
+    return set_error(OP2B_ERR_ARG, "op2b_memcpy_h2d_small: %llu bytes (at most %zu)",
+                     (unsigned long long)bytes, sizeof(SmallBytes::b));
+  if (!bytes) return OP2B_OK;
+  SmallBytes v;
+  std::memcpy(v.b, src, bytes);
+  small_copy_kernel<<<1, 64, 0, stream_of(stream)>>>(reinterpret_cast<unsigned char *>(dst), v,
+                                                    static_cast<int>(bytes));
+  return check_cuda(cudaGetLastError(), "small_copy_kernel");
 }
 
 int op2b_memcpy_d2h_async(void *dst, uint64_t src, uint64_t bytes, uint64_t stream) {
