@@ -617,7 +617,10 @@ def bench_serving(op2, b200, nreq, rate, seed=0, n_p1=16, n_quad=16):
                                         for k, v in views.items()}
         return take
 
-    # capacity first: it also fills the pinned-buffer pool the timed runs reuse
+    # one untimed pass over the trace fills the pinned-buffer pool the timed
+    # runs reuse (page-locking host memory is a one-off cost)
+    serve.Engine(store, configs=configs, consumer=lambda j, v: None).run(
+        serving.clone_trace(jobs, False), realtime=False)
     cap_e = serve.Engine(store, configs=configs, consumer=lambda j, v: None, timing=True)
     s_cap_eng = serve.summary(cap_e.run(serving.clone_trace(jobs, False), realtime=False), 0.0)
     s_cap_eng["gpu_busy_fraction"] = round(cap_e.gpu_busy_ms() / (s_cap_eng["span_s"] * 1e3), 3)
