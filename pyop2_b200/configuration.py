@@ -38,7 +38,9 @@ keys of the B200 backend:
 * ``mat_slots``: assemble scalar Mats in the atomic form through a cached
   scatter-slot table (the CSR position of every element's local entries,
   built once per Sparsity and Map pair: nelem x arity^2 int32 of device
-  memory) instead of searching the CSR row for every entry.
+  memory) instead of searching the CSR row for every entry;
+* ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
+  admits meshes and requests against by default.
 """
 
 import os
@@ -61,6 +63,7 @@ _defaults = {
     'owner_mode': 'never',
     'kahan': False,
     'mat_slots': True,
+    'hbm_budget_gb': 120.0,
 }
 
 _config = dict(_defaults)

@@ -223,6 +223,10 @@ class Job(object):
         self.t_admit = self.t_done = None
         self.result = None
         self.stage = 0
+        # 'done', 'rejected' (admission queue full) or 'cancelled'; a caller
+        # sets ``cancelled`` to withdraw the request (see Engine.run)
+        self.status = None
+        self.cancelled = False
 
     @property
     def latency(self):
@@ -359,7 +363,10 @@ class MeshStore(object):
     """Resident meshes against an HBM budget (bytes), LRU eviction of meshes
     no admitted request uses."""
 
-    def __init__(self, budget):
+    def __init__(self, budget=None):
+        if budget is None:
+            from . import configuration as cfg
+            budget = float(cfg.cfg['hbm_budget_gb']) * 1e9
         self.budget = int(budget)
         self.used = 0
         self.meshes = collections.OrderedDict()
@@ -418,9 +425,12 @@ class Engine(object):
     memory, valid during the call (default: :func:`keep_results`)."""
 
     def __init__(self, store, max_inflight=2, max_admit=64, configs=None, consumer=None,
-                 pool=None, timing=False):
+                 pool=None, timing=False, max_waiting=None):
         self.store = store
         self.max_inflight, self.max_admit = max_inflight, max_admit
+        # bound of the admission queue: a request arriving to a full queue is
+        # rejected (status 'rejected') instead of waiting
+        self.max_waiting = max_waiting
         self.configs = dict(configs or {})
         self.consumer = consumer or keep_results
         self.pool = pool if pool is not None else POOL
@@ -450,7 +460,17 @@ class Engine(object):
         while pending or waiting or active or inflight:
             now = clock()
             while pending and pending[0].arrival <= now:
-                waiting.append(pending.popleft())
+                job = pending.popleft()
+                if job.cancelled:
+                    self._retire(job, "cancelled", t0, done)
+                elif self.max_waiting is not None and len(waiting) >= self.max_waiting:
+                    self._retire(job, "rejected", t0, done)
+                else:
+                    waiting.append(job)
+            if any(j.cancelled for j in waiting):
+                for j in [j for j in waiting if j.cancelled]:
+                    self._retire(j, "cancelled", t0, done)
+                waiting = collections.deque(j for j in waiting if not j.cancelled)
             # completions first: they return memory to the budget
             while inflight and inflight[0][0].query():
                 self._complete(inflight.popleft()[1], t0, done)
@@ -472,6 +492,15 @@ class Engine(object):
                 active.append(job)
                 admitted += 1
             self.peak_used = max(self.peak_used, self.store.used)
+            if any(j.cancelled for j in active):
+                # withdrawn between steps: its launched work completes in
+                # stream order before the arena's stream-ordered free
+                for j in [j for j in active if j.cancelled]:
+                    j._mesh.refs -= 1
+                    self.store.release(j._mesh.request_bytes())
+                    j._mesh = j.arena = j.steps = None
+                    self._retire(j, "cancelled", t0, done)
+                active = [j for j in active if not j.cancelled]
             if active and len(inflight) < self.max_inflight:
                 finishing = self._step(active)
                 ev = b200.Event().record()
@@ -523,11 +552,19 @@ class Engine(object):
         t = time.perf_counter() - t0
         for job in jobs:
             job.t_done = t
+            job.status = "done"
             job.deliver(self.pool, self.consumer)
             job._mesh.refs -= 1
             self.store.release(job._mesh.request_bytes())
             job._mesh = None
             done.append(job)
+
+    @staticmethod
+    def _retire(job, status, t0, done):
+        """A request that leaves without a result (rejected or cancelled)."""
+        job.status = status
+        job.t_done = time.perf_counter() - t0
+        done.append(job)
 
 
 class PlainServer(object):
@@ -552,17 +589,22 @@ class PlainServer(object):
             job.t_admit = time.perf_counter() - t0
             views = job.run_plain(self.op2, mesh)
             job.t_done = time.perf_counter() - t0
+            job.status = "done"
             self.consumer(job, views)
             done.append(job)
         return done
 
 
 def summary(jobs, t_first=None):
-    """p50 / p99 latency (ms) and requests/s of a served trace."""
+    """p50 / p99 latency (ms) and requests/s of the completed requests of a
+    served trace, with the counts of rejected and cancelled ones."""
+    dropped = collections.Counter(j.status for j in jobs if j.status not in (None, "done"))
+    jobs = [j for j in jobs if j.status in (None, "done")]
     lat = np.array([j.latency for j in jobs]) * 1e3
     t_first = min(j.arrival for j in jobs) if t_first is None else t_first
     span = max(j.t_done for j in jobs) - t_first
     out = {"requests": len(jobs), "req_per_s": round(len(jobs) / span, 1),
+           "rejected": dropped.get("rejected", 0), "cancelled": dropped.get("cancelled", 0),
            "p50_ms": round(float(np.percentile(lat, 50)), 3),
            "p99_ms": round(float(np.percentile(lat, 99)), 3),
            "mean_ms": round(float(lat.mean()), 3), "span_s": round(span, 4)}

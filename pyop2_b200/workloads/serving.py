@@ -83,8 +83,9 @@ def clone_trace(jobs, realtime=True):
         c = object.__new__(type(j))
         c.__dict__.update({k: v for k, v in j.__dict__.items()
                            if k in ("rid", "arrival", "mesh_id", "seed", "iters")})
-        c.t_admit = c.t_done = c.result = None
+        c.t_admit = c.t_done = c.result = c.status = None
         c.stage = 0
+        c.cancelled = False
         if not realtime:
             c.arrival = 0.0
         out.append(c)

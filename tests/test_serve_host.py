@@ -157,3 +157,52 @@ def test_engine_admission_and_completion_logic(monkeypatch, steps, slots):
     assert tight.used == sum(m.nbytes for m in tight.meshes.values())
     if slots > 1:
         assert max(_Batch.sizes) > 1
+
+
+def _fake_engine_env(monkeypatch, budget_slots=100):
+    from pyop2_b200 import serve
+    monkeypatch.setattr(serve, "BatchLoop", _Batch)
+    monkeypatch.setattr(serve.b200, "Event", _Event)
+    sizes = {"m%d" % i: 100 + 37 * i for i in range(5)}
+    store = MeshStore(10 ** 9)
+    for m, n in sizes.items():
+        store.register(m, lambda m=m, n=n: _Mesh(m, n, 10 + n // 10), n)
+    for m in sizes:
+        store.load(m)
+    return serve, store, sorted(sizes)
+
+
+def test_full_admission_queue_rejects(monkeypatch):
+    """Requests arriving to a full admission queue are rejected, not queued;
+    the others complete and summary() counts both."""
+    serve, store, meshes = _fake_engine_env(monkeypatch)
+    jobs = _fake_jobs(30, meshes, (3, 4), seed=1)
+    eng = serve.Engine(store, max_admit=2, max_waiting=5)
+    done = eng.run(jobs, realtime=False)
+    st = [j.status for j in done]
+    # all 30 arrive at once: 5 fit the queue, the other 25 are turned away
+    assert len(done) == 30 and st.count("rejected") == 25 and st.count("done") == 5
+    s = serve.summary(done, t_first=0.0)
+    assert s["requests"] == 5 and s["rejected"] == 25
+    assert store.used == sum(m.nbytes for m in store.meshes.values())
+
+
+def test_cancelled_requests_leave_and_return_memory(monkeypatch):
+    """Cancelled before arrival, while waiting, or between steps: the request
+    leaves with status 'cancelled', no result, and its memory back."""
+    serve, store, meshes = _fake_engine_env(monkeypatch)
+    jobs = _fake_jobs(20, meshes, (6, 7), seed=2)
+    jobs[0].cancelled = True                      # before it arrives
+
+    def consumer(job, views):
+        job.result = views
+        for j in jobs[10:15]:                     # withdrawn while others run
+            j.cancelled = True
+    eng = serve.Engine(store, max_admit=4, consumer=consumer)
+    done = eng.run(jobs, realtime=False)
+    by = {j.rid: j for j in done}
+    assert len(by) == 20 and by[0].status == "cancelled" and by[0].result is None
+    assert all(by[r].status == "cancelled" and by[r].result is None for r in range(10, 15))
+    assert sum(j.status == "done" for j in done) == 14
+    assert store.used == sum(m.nbytes for m in store.meshes.values())
+    assert all(m.refs == 0 for m in store.meshes.values())
