@@ -217,25 +217,36 @@ int op2b_incidence_free(uint64_t incidence);
 
 /* ------------------------------------------------------------------------
  * Two-phase deterministic INC.  A generated stub writes every element's INC
- * contribution to a contribution array lma[(k * nelem + e) * cdim + comp]
- * (k: map position of a Dat INC, or r * ca + c of a Mat's local entry);
+ * contribution to a tiled contribution array: element e, position k (of K)
+ * at row ((e / 32) * K + k) * 32 + e % 32, cdim values per row (k: map
+ * position of a Dat INC, or r * ca + c of a Mat's local entry);
  * op2b_lma_reduce then adds, for each target t, the contributions listed by
- * t's incidence (flat positions e * arity + k, increasing) to out[t] in that
- * order -- the order pyop2/sequential.py:55-72 adds them -- optionally with
- * compensated (Kahan) summation.  Positions whose k is not set in kmask are
- * skipped.  out and lma are float64; cdim is 1 to 4; arity at most 64.
- * Replaces the LMA buffer + atomic scatter of pyop2/cuda.py:177-270 and the
- * coloured INC of cuda_indirect_loop.jinja2:169-189 where the result must not
- * depend on scheduling.
+ * t's incidence (increasing element order) to out[t] in that order -- the
+ * order pyop2/sequential.py:55-72 adds them -- optionally with compensated
+ * (Kahan) summation.  out and lma are float64.  Replaces the LMA buffer +
+ * atomic scatter of pyop2/cuda.py:177-270 and the coloured INC of
+ * cuda_indirect_loop.jinja2:169-189 where the result must not depend on
+ * scheduling.
  * ---------------------------------------------------------------------- */
 /* Incidence of a scalar Mat assembly over CSR positions: for each position,
- * the local entries (e * ra * ca + r * ca + c) that add to it.  Fails with
+ * the local entries that add to it, in element order, each given as its
+ * index in the tiled contribution array (K = ra * ca).  Fails with
  * OP2B_ERR_MAP if an entry is not in the Sparsity. */
 int op2b_mat_incidence_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64_t cmap,
                              int32_t nelem, int32_t ra, int32_t ca, int32_t nnz,
                              uint64_t stream, uint64_t *incidence);
+/* flags: OP2B_LMA_KAHAN compensated sums; OP2B_LMA_FROM_ZERO start from 0
+ * instead of reading out[] (the caller knows the target is zero);
+ * OP2B_LMA_MAT_INDEX the incidence comes from op2b_mat_incidence_build
+ * (list entries are contribution-array indices; cdim 1, arity and kmask
+ * ignored).  Otherwise the incidence is a Map's (op2b_incidence_build: flat
+ * positions e * arity + k), positions whose k is not set in kmask are
+ * skipped, cdim is 1 to 4 and arity at most 64. */
+#define OP2B_LMA_KAHAN     1
+#define OP2B_LMA_FROM_ZERO 2
+#define OP2B_LMA_MAT_INDEX 4
 int op2b_lma_reduce(uint64_t out, int32_t cdim, uint64_t ptr, uint64_t list, int32_t ntargets,
-                    uint64_t lma, int64_t nelem, int32_t arity, uint64_t kmask, int32_t kahan,
+                    uint64_t lma, int64_t nelem, int32_t arity, uint64_t kmask, int32_t flags,
                     uint64_t stream);
 
 /* ------------------------------------------------------------------------

@@ -529,6 +529,9 @@ class Mat(DeviceDataMixin, base.Mat):
         base.Mat.__init__(self, sparsity, dtype, name)
         self._state = DEVICE_UNALLOCATED
         self._vals = None
+        # True while every value is known to be zero (fresh or zero()ed): the
+        # two-phase reduction then need not read the values
+        self._is_zero = True
 
     def _device_values(self):
         if self._vals is None:
@@ -560,11 +563,13 @@ class Mat(DeviceDataMixin, base.Mat):
 
     def zero(self):
         self._device_values().memset(0)
+        self._is_zero = True
 
     def zero_rows(self, rows, diag_val):
         """Zero the given rows except the diagonal, set to diag_val."""
         rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).ravel())
         vals = self._device_values()
+        self._is_zero = False
         call("op2b_mat_zero_rows", vals.ptr, self._sparsity._d_rowptr, self._sparsity._d_colidx,
              rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, float(diag_val),
              self.dtype.itemsize, 0)
@@ -1096,17 +1101,18 @@ class _BoundLoop(object):
             # incidences their reduction walks (phase 2, op2b_lma_reduce)
             self.lma = []
             self.kahan = bool(cfg.cfg['kahan'])
+            n32 = (n + 31) // 32 * 32     # contribution arrays come in tiles of 32
             for j, m in enumerate(mats):
                 s = next(a for a in specs if a.kind == "mat" and a.slot == j)
                 rmap, cmap = maps[s.mslot], maps[s.cmslot]
-                buf = DeviceBuffer(max(1, n * rmap.dim * cmap.dim) * 8)
+                buf = DeviceBuffer(max(1, n32 * rmap.dim * cmap.dim) * 8)
                 vals["lm%d" % j] = buf.ptr
                 inc = m.sparsity._mat_incidence(rmap, cmap)
                 self.lma.append((buf, inc, m, 1, m.sparsity._d_nz, rmap.dim * cmap.dim,
                                  (1 << (rmap.dim * cmap.dim)) - 1))
             for k, st in enumerate(stages):
                 d, mp = dats[st[0]], maps[st[1]]
-                buf = DeviceBuffer(max(1, n * mp.dim * st[3]) * 8)
+                buf = DeviceBuffer(max(1, n32 * mp.dim * st[3]) * 8)
                 vals["ld%d" % k] = buf.ptr
                 mask = 0
                 for ix in st[4]:
@@ -1205,11 +1211,19 @@ class _BoundLoop(object):
         else:
             call("op2b_launch", mod.fn, self.grid, self.block_size, 0, 0, params, self.layout.nbytes)
         if self.spec.mode == "lma":
-            kahan = int(self.kahan)
+            kahan = 1 if self.kahan else 0            # OP2B_LMA_KAHAN
             for buf, inc, target, cdim, ntargets, arity, mask in self.lma:
-                out = target._device_values().ptr if isinstance(target, Mat) else target._device.ptr
+                if isinstance(target, Mat):
+                    out = target._device_values().ptr
+                    # Mat incidences hold contribution indices (OP2B_LMA_MAT_INDEX);
+                    # a Mat known to be zero needs no read of its values
+                    # (OP2B_LMA_FROM_ZERO)
+                    flags = kahan | 4 | (2 if target._is_zero else 0)
+                    target._is_zero = False
+                else:
+                    out, flags = target._device.ptr, kahan
                 call("op2b_lma_reduce", out, cdim, inc.ptr, inc.list, ntargets, buf.ptr, n,
-                     arity, mask, kahan, 0)
+                     arity, mask, flags, 0)
         for d in self._written:
             d._state = DEVICE
             maybe_setflags(d._data, write=False)
@@ -1217,6 +1231,7 @@ class _BoundLoop(object):
             args[self._gbl[k][1]].data._state = DEVICE
         for m in self.mats:
             m._state = DEVICE
+            m._is_zero = False
 
 
 _ENV = {"gen": None, "key": None}

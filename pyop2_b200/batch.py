@@ -201,6 +201,7 @@ class LoopInstance(object):
             g._state = b200.DEVICE
         for m in self.mats:
             m._state = b200.DEVICE
+            m._is_zero = False
 
 
 class PatchedInstance(object):

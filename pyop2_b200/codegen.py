@@ -524,8 +524,10 @@ def _inc_sink(spec, a, n, k, src, val, ind):
     an atomic add, or in the two-phase form a store to the contribution array
     of the arg's (Dat, Map) pair."""
     if spec.mode == "lma":
-        return "%sop2b_store(p.ld%d + ((op2b_i64)%d * p.set_size + e) * %d, %s);" % (
-            ind, a.stage, k, a.cdim, val)
+        # tiles of 32 elements: for one position k a warp writes 32 adjacent
+        # rows, and one element's rows stay within its tile
+        return "%sop2b_store(p.ld%d + op2b_lma_index(e, %d, %d) * %d, %s);" % (
+            ind, a.stage, k, spec.maps[spec.stages[a.stage][1]], a.cdim, val)
     return "%sop2b_atomic_row(%s, %s);" % (ind, src, val)
 
 
@@ -975,8 +977,8 @@ def _mat_addto(spec, n, a, ind, atomic=False, lma=False):
     if lma:
         # two-phase form: the local entry goes to the contribution array at
         # k = r * ca + c; op2b_lma_reduce adds it to its CSR slot
-        L.append("%s  p.lm%d[((op2b_i64)(%s * %d + %s)) * p.set_size + e] = A%d[i0][i1];"
-                 % (ind, j, ri, a.carity, ci, n))
+        L.append("%s  p.lm%d[op2b_lma_index(e, %s * %d + %s, %d)] = A%d[i0][i1];"
+                 % (ind, j, ri, a.carity, ci, a.arity * a.carity, n))
         L.append("%s}" % ind)
         return L
     if a.rm * a.cm == 1:

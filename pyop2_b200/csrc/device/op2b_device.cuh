@@ -90,6 +90,12 @@ __device__ __forceinline__ void op2b_zero(T (&a)[N]) {
   for (int k = 0; k < N; ++k) a[k] = T(0);
 }
 
+// Row of the contribution of element e at position k (of K) in a two-phase
+// contribution array: tiles of 32 elements, position-major inside a tile.
+__device__ __forceinline__ op2b_i64 op2b_lma_index(op2b_i64 e, int k, int K) {
+  return (((e >> 5) * K + k) << 5) + (e & 31);
+}
+
 __device__ __forceinline__ int op2b_csr_find(const int *__restrict__ rowptr,
                                              const int *__restrict__ colidx, int row, int col) {
   int lo = rowptr[row], hi = rowptr[row + 1];
