@@ -250,6 +250,35 @@ int op2b_lma_reduce(uint64_t out, int32_t cdim, uint64_t ptr, uint64_t list, int
                     uint64_t stream);
 
 /* ------------------------------------------------------------------------
+ * Linear algebra on device CSR Mats (float64 values, int32 rowptr/colidx)
+ * and Dat vectors.  Replaces the PETSc KSP solve of pyop2/petsc_base.py:
+ * 160-220 (defaults 'cg' + 'jacobi', pyop2/base.py:1591-1601), the Cusp CG of
+ * pyop2/cuda.py:445-600, and the host-side Dat arithmetic and norm of
+ * pyop2/base.py:749-797, 836-839.  Reductions are deterministic (fixed
+ * combination order for a given launch shape).
+ * ---------------------------------------------------------------------- */
+/* y = alpha * A x + beta * y over nrows rows (beta == 0: y is not read). */
+int op2b_csr_spmv(uint64_t rowptr, uint64_t colidx, uint64_t vals, int32_t nrows, int64_t nnz,
+                  uint64_t x, uint64_t y, double alpha, double beta, uint64_t stream);
+/* out[i] = x[i] op y[i] (y != 0) or x[i] op yscalar (y == 0); op 0 add,
+ * 1 subtract, 2 multiply, 3 divide; dtype 0 float64, 1 float32, 2 int32;
+ * out may equal x. */
+int op2b_vec_binop(uint64_t out, uint64_t x, uint64_t y, double yscalar, int64_t n, int32_t op,
+                   int32_t dtype, uint64_t stream);
+/* *result = sum_i x[i] * y[i] (float64), returned to the host. */
+int op2b_vec_dot(uint64_t x, uint64_t y, int64_t n, double *result, uint64_t stream);
+/* Conjugate gradients on A x = b from x = 0, left-preconditioned by the
+ * inverse diagonal of A (jacobi != 0) or not.  Stops at the first iteration
+ * k whose preconditioned residual norm r_k = ||M^-1 (b - A x_k)|| satisfies
+ * r_k <= max(rtol * r_0, atol) (reason 1), r_k >= dtol * r_0 (reason 2), is
+ * not finite (reason 3), or at k = max_it (reason 4).  iterations = k;
+ * history (may be NULL) receives r_0 .. r_k (iterations + 1 values). */
+int op2b_cg_solve(uint64_t rowptr, uint64_t colidx, uint64_t vals, int32_t nrows, int64_t nnz,
+                  uint64_t x, uint64_t b, int32_t jacobi, double rtol, double atol, double dtol,
+                  int32_t max_it, int32_t *iterations, int32_t *reason, double *history,
+                  uint64_t stream);
+
+/* ------------------------------------------------------------------------
  * Mat operations on the device CSR values (dtype 4 = float32, 8 = float64).
  * Replaces cuda.Mat.zero_rows / zero (pyop2/cuda.py:289-301) and PETSc
  * MatZeroRowsLocal (pyop2/petsc_base.py:131-135).

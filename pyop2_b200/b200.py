@@ -278,9 +278,60 @@ class Dat(DeviceDataMixin, base.Dat):
         self._device.memset(0)
         self._state = DEVICE
 
+    # ------------------------------------------------ arithmetic on the device
+    # pyop2/base.py:749-797 computed these on the host copies; here float64 /
+    # float32 (and int32 except division) Dats stay on the device
+    _BINOP_DTYPES = {np.dtype(np.float64): 0, np.dtype(np.float32): 1, np.dtype(np.int32): 2}
+    _BINOP_CODES = {"add": 0, "sub": 1, "mul": 2, "truediv": 3}
+
+    def _device_binop(self, other, opname, out):
+        """out = self op other on the device; False if the operands need the
+        host path (other dtypes, integer division, mismatched shapes)."""
+        code = self._BINOP_DTYPES.get(self.dtype)
+        op = self._BINOP_CODES[opname]
+        if code is None or (code == 2 and op == 3):
+            return False
+        n = self.dataset.total_size * self.cdim
+        if np.isscalar(other):
+            yptr, ys = 0, float(base.as_type(other, self.dtype))
+        elif isinstance(other, Dat):
+            if other.dtype != self.dtype or other.dataset.total_size * other.cdim != n:
+                return False
+            other._to_device()
+            yptr, ys = other._device.ptr, 0.0
+        else:
+            return False
+        self._to_device()
+        if out is not self:
+            out._allocate_device()
+        call("op2b_vec_binop", out._device.ptr, self._device.ptr, yptr, ys, n, op, code, 0)
+        out._state = DEVICE
+        maybe_setflags(out._data, write=False)
+        return True
+
+    def _op(self, other, op):
+        name = op.__name__.strip("_")
+        out = Dat(self.dataset, None, self.dtype)
+        if self._device_binop(other, name, out):
+            return out
+        return base.Dat._op(self, other, op)
+
+    def _iop(self, other, op):
+        name = op.__name__.strip("_").lstrip("i")
+        if self._device_binop(other, name, self):
+            return self
+        return base.Dat._iop(self, other, op)
+
     @property
     def norm(self):
-        return np.linalg.norm(self.data_ro)
+        """L2 norm of the flattened values (on the device for float64)."""
+        if self.dtype != np.float64:
+            return np.linalg.norm(self.data_ro)
+        self._to_device()
+        r = C.c_double()
+        n = self.dataset.total_size * self.cdim
+        call("op2b_vec_dot", self._device.ptr, self._device.ptr, n, C.byref(r), 0)
+        return float(np.sqrt(r.value))
 
 
 class Const(DeviceDataMixin, base.Const):
@@ -578,9 +629,62 @@ class Mat(DeviceDataMixin, base.Mat):
         pass
 
 
+_CG_REASONS = {1: "converged (relative or absolute tolerance)", 2: "diverged (dtol)",
+               3: "breakdown (non-finite residual)", 4: "iteration limit"}
+
+
 class Solver(base.Solver):
+    """Conjugate gradients with Jacobi or no preconditioning on the device
+    (op2b_cg_solve), for the reference's defaults 'cg' + 'jacobi'
+    (pyop2/base.py:1591-1601, pyop2/petsc_base.py:160-220).  Like PETSc's
+    default, the solve starts from x = 0 and tests the preconditioned
+    residual norm against max(rtol * r0, atol) and dtol * r0.  After a solve,
+    ``iterations``, ``reason`` and ``residual_history`` describe it."""
+
     def solve(self, A, x, b):
-        raise NotImplementedError("The linear solve is not part of the B200 backend's hot path")
+        p = self.parameters
+        if p['linear_solver'] != 'cg':
+            raise NotImplementedError("linear_solver %r: the B200 backend solves with 'cg'"
+                                      % p['linear_solver'])
+        pc = p['preconditioner']
+        if pc not in ('jacobi', 'none', None):
+            raise NotImplementedError("preconditioner %r: the B200 backend offers 'jacobi' and "
+                                      "'none'" % pc)
+        check_errors()
+        sp = A.sparsity
+        sp._ensure()
+        nrows = sp._lsize
+        for d, nm in ((x, "x"), (b, "b")):
+            if d.dtype != np.float64 or d.dataset.total_size * d.cdim != nrows:
+                raise ValueError("%s must be a float64 Dat of %d values (the Mat's rows)" % (nm, nrows))
+        b._to_device()
+        if x._state is DEVICE_UNALLOCATED:
+            x._allocate_device()
+        vals = A._device_values()
+        max_it = int(p['maximum_iterations'])
+        hist = np.zeros(max_it + 1, dtype=np.float64)
+        its, reason = C.c_int32(), C.c_int32()
+        call("op2b_cg_solve", sp._d_rowptr, sp._d_colidx, vals.ptr, nrows, sp._d_nz,
+             x._device.ptr, b._device.ptr, 1 if pc == 'jacobi' else 0,
+             float(p['relative_tolerance']), float(p['absolute_tolerance']),
+             float(p['divergence_tolerance']), max_it, C.byref(its), C.byref(reason),
+             hist.ctypes.data_as(C.POINTER(C.c_double)), 0)
+        x._state = DEVICE
+        maybe_setflags(x._data, write=False)
+        x.needs_halo_update = True
+        self.iterations, self.reason = its.value, reason.value
+        self.residual_history = hist[:its.value + 1].copy()
+        if p.get('monitor_convergence'):
+            for k, r in enumerate(self.residual_history):
+                debug("%3d CG preconditioned residual norm %14.12e" % (k, r))
+        if self.reason != 1:
+            msg = ("CG failed to converge in %d iterations: %s (residual norm %e)"
+                   % (self.iterations, _CG_REASONS.get(self.reason, self.reason),
+                      self.residual_history[-1]))
+            if p.get('error_on_nonconvergence', True):
+                raise RuntimeError(msg)
+            import warnings
+            warnings.warn(msg)
 
 
 def solve(M, x, b):
