@@ -275,6 +275,11 @@ def run_gpu(args, ws, rank, local):
             print(json.dumps({"batching": bench_batching(op2, b200, args.batch_meshes or 4096)}))
         d.close()
         return 0
+    if args.solve_only:
+        if rank == 0:
+            print(json.dumps({"solve": bench_solve(op2, b200)}))
+        d.close()
+        return 0
     if args.serving_only:
         if rank == 0:
             print(json.dumps({"serving": bench_serving(op2, b200, args.serve_requests or 3000,
@@ -416,6 +421,9 @@ def run_gpu(args, ws, rank, local):
     serving = None
     if args.serve_requests > 0:
         serving = bench_serving(op2, b200, args.serve_requests, args.serve_rate)
+    solve = None
+    if not args.no_solve:
+        solve = bench_solve(op2, b200)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -449,6 +457,7 @@ def run_gpu(args, ws, rank, local):
         "mat_assembly": assembly,
         "batching": batching,
         "serving": serving,
+        "solve": solve,
         "inc_mode": op2_cfg_inc_mode(),
         "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
     }
@@ -660,6 +669,68 @@ def bench_serving(op2, b200, nreq, rate, seed=0, n_p1=16, n_quad=16):
             "resident_setup_s": round(resident_s, 1), "tune_s": round(tune_s, 1)}
 
 
+def bench_solve(op2, b200, n=1024, reps=20):
+    """Linear solve on an assembled Mat: the P2 mass matrix of the n x n
+    grid (48.25 M nonzeros at n = 1024), Jacobi-preconditioned CG from x = 0
+    to rtol 1e-8 (op2.solve), and the CSR SpMV alone.  SpMV algorithmic
+    bytes: values and column indices (12 B per nonzero), row pointers, x
+    read once, y written once.  CPU leg: the oracle's numpy SpMV on the same
+    matrix (a bounded sample of 3 products)."""
+    from oracle import linalg
+    from pyop2_b200._lib import call
+    from pyop2_b200.workloads import fem
+    P = fem.build_p2(op2, n, seed=0)
+    fem.assemble_p2(op2, P)
+    b200.synchronize()
+    sp = P.sparsity
+    rows, nnz = sp._lsize, int(sp.nz)
+    rng = np.random.default_rng(11)
+    rhs = rng.standard_normal(rows)
+    b = op2.Dat(P.dofs, rhs.copy(), np.float64, "b")   # a Dat reshapes the array it keeps
+    x = op2.Dat(P.dofs, np.zeros(rows), np.float64, "x")
+    solver = b200.Solver(relative_tolerance=1e-8)
+    solver.solve(P.M, x, b)                       # warm-up (device copies)
+    ts = []
+    for _ in range(3):
+        b200.l2_flush()
+        e0 = b200.Event().record()
+        solver.solve(P.M, x, b)
+        e1 = b200.Event().record()
+        e1.synchronize()
+        ts.append(e0.elapsed_ms(e1))
+    solve_ms = statistics.median(ts)
+    resid = float(np.abs(linalg.csr_matvec(sp.rowptr, sp.colidx, P.M.array, x.data_ro.ravel())
+                         - rhs).max() / np.abs(rhs).max())
+    vals = P.M._device_values().ptr
+    xd, yd = b._device.ptr, b200.DeviceBuffer(rows * 8)
+
+    by_group = {}
+    for group in (0, 1, 2, 4, 8, 16):   # 0: the library's choice from the mean row length
+        def spmv(group=group):
+            call("op2b_csr_spmv", sp._d_rowptr, sp._d_colidx, vals, rows, nnz, xd, yd.ptr, 1.0,
+                 0.0, group, 0)
+        by_group[group] = _timed(spmv, reps, b200)
+    spmv_ms = by_group[0]
+    spmv_bytes = nnz * 12 + (rows + 1) * 4 + rows * 16
+    mvals = P.M.array
+    t0 = time.time()
+    for _ in range(3):
+        linalg.csr_matvec(sp.rowptr, sp.colidx, mvals, rhs)
+    cpu_s = (time.time() - t0) / 3
+    peak, _ = _peaks()
+    return {"matrix": "P2 mass %dx%d" % (n, n), "rows": rows, "nnz": nnz,
+            "solver": "cg + jacobi, rtol 1e-8, x0 = 0", "iterations": solver.iterations,
+            "reason": solver.reason, "solve_ms": round(solve_ms, 3),
+            "ms_per_iteration": round(solve_ms / max(1, solver.iterations), 4),
+            "max_rel_residual": resid,
+            "spmv_ms": round(spmv_ms, 4), "spmv_GBps": round(spmv_bytes / (spmv_ms * 1e-3) / 1e9, 1),
+            "spmv_frac_of_measured_peak": round(spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak, 3),
+            "spmv_algorithmic_bytes": spmv_bytes,
+            "spmv_ms_by_lanes_per_row": {str(k): round(v, 4) for k, v in by_group.items()},
+            "cpu_spmv": {"GBps": round(spmv_bytes / cpu_s / 1e9, 2), "cores": 1,
+                         "kind": "port", "sample": "3 numpy CSR products (oracle)"}}
+
+
 def bench_assembly(op2, b200, reps=5):
     """Mat assembly legs: P1 256x256 mass + RHS and P2 1024x1024
     stiffness + mass in FP64 and in the precision form (FP32 element math and
@@ -779,6 +850,9 @@ def main(argv=None):
                    help="mean Poisson arrival rate of the serving leg (requests/s)")
     p.add_argument("--serving-only", action="store_true",
                    help="run only the serving leg and print its figures")
+    p.add_argument("--no-solve", action="store_true", help="skip the linear-solve leg")
+    p.add_argument("--solve-only", action="store_true",
+                   help="run only the linear-solve leg and print its figures")
     p.add_argument("--l2-fetch", type=int, default=-1,
                    help="L2 fetch granularity in bytes (32/64/128; 0 driver default; -1 backend default)")
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")

@@ -257,9 +257,11 @@ int op2b_lma_reduce(uint64_t out, int32_t cdim, uint64_t ptr, uint64_t list, int
  * pyop2/base.py:749-797, 836-839.  Reductions are deterministic (fixed
  * combination order for a given launch shape).
  * ---------------------------------------------------------------------- */
-/* y = alpha * A x + beta * y over nrows rows (beta == 0: y is not read). */
+/* y = alpha * A x + beta * y over nrows rows (beta == 0: y is not read).
+ * group: lanes per row (1, 2, 4, 8, 16 or 32; 0 picks by the mean row length). */
 int op2b_csr_spmv(uint64_t rowptr, uint64_t colidx, uint64_t vals, int32_t nrows, int64_t nnz,
-                  uint64_t x, uint64_t y, double alpha, double beta, uint64_t stream);
+                  uint64_t x, uint64_t y, double alpha, double beta, int32_t group,
+                  uint64_t stream);
 /* out[i] = x[i] op y[i] (y != 0) or x[i] op yscalar (y == 0); op 0 add,
  * 1 subtract, 2 multiply, 3 divide; dtype 0 float64, 1 float32, 2 int32;
  * out may equal x. */

@@ -120,7 +120,7 @@ def test_spmv_matches_oracle(op2):
     y0 = np.random.default_rng(6).standard_normal(n)
     yd.from_host(y0)
     call("op2b_csr_spmv", sp._d_rowptr, sp._d_colidx, P.K._device_values().ptr, n, sp._d_nz,
-         xd.ptr, yd.ptr, 2.0, -0.5, 0)
+         xd.ptr, yd.ptr, 2.0, -0.5, 0, 0)
     y = np.empty(n)
     yd.to_host(y)
     want = 2.0 * linalg.csr_matvec(sp.rowptr, sp.colidx, P.K.array, xv) - 0.5 * y0
