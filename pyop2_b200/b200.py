@@ -688,7 +688,8 @@ class Solver(base.Solver):
 
 
 def solve(M, x, b):
-    """op2.solve (pyop2/op2.py: solve): not provided by this backend."""
+    """op2.solve (pyop2/op2.py: solve): M x = b with the default Solver
+    parameters, on the device."""
     Solver().solve(M, x, b)
 
 
