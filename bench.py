@@ -263,6 +263,8 @@ def run_gpu(args, ws, rank, local):
         opts["min_blocks_per_sm"] = args.min_blocks
     if args.inc_mode:
         opts["inc_mode"] = args.inc_mode
+    if args.staged_block_size:
+        opts["staged_block_size"] = args.staged_block_size
     op2.init(backend="b200", device=local, **opts)
     if args.assembly_only:
         # the Mat assembly legs alone (profiling their kernels); not a bench line
@@ -836,6 +838,8 @@ def main(argv=None):
     p.add_argument("--ny", type=int, default=NY, help="cells along y (default 600)")
     p.add_argument("--part-size", type=int, default=0, help="plan partition size (0: backend default)")
     p.add_argument("--block-size", type=int, default=0, help="threads per CTA (0: backend default)")
+    p.add_argument("--staged-block-size", type=int, default=0,
+                   help="threads per CTA of staged loops (0: backend default)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     p.add_argument("--no-assembly", action="store_true", help="skip the Mat assembly legs")
     p.add_argument("--assembly-only", action="store_true",
@@ -858,7 +862,7 @@ def main(argv=None):
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")
     p.add_argument("--no-permute", action="store_true",
                    help="structured (unpermuted) cell/node numbering instead of the random one")
-    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic", "lma"],
+    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic", "lma", "staged"],
                    help="INC conflict resolution of indirect loops (default: backend default)")
     args = p.parse_args(argv)
     _set_mesh(args.nx, args.ny)

@@ -182,6 +182,42 @@ int op2b_plan_ncolblk_host(uint64_t plan, int32_t *out, int32_t n);
 int op2b_plan_free(uint64_t plan);
 
 /* ------------------------------------------------------------------------
+ * Locality partition for staged indirect loops.  The reference partitions
+ * into blocks of consecutive elements (pyop2/plan.pyx:107-110) and stages
+ * each block's indirect rows in shared memory (:112-212); on a permuted mesh
+ * numbering consecutive elements share no targets, so this builder first
+ * reorders the iteration set into compact regions: seeds hashed from
+ * element ids (about one per region_size elements), a multi-source
+ * breadth-first search over the element graph of grow_map (elements sharing
+ * a target are adjacent; ties to the smaller region id, so the result is
+ * deterministic), elements sorted by (region, level, id), each region cut
+ * into nearly equal blocks of at most part_size elements.  Then, per block
+ * and staged Map (all rows), the sorted distinct targets and, per position
+ * of the reordered set and Map row, the target's index among them; and per
+ * block the reference's greedy thread colouring (pyop2/plan.pyx:282-324)
+ * over the targets of the staged Maps with stage_inc[s] != 0, so elements of
+ * one colour never share such a target.  part_size * stage_arity must not
+ * exceed 16384; at most 64 staged Maps.
+ * ---------------------------------------------------------------------- */
+int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_size,
+                           uint64_t grow_map, int32_t grow_arity, int32_t grow_ntargets,
+                           int32_t nstage, const uint64_t *stage_map, const int32_t *stage_arity,
+                           const int32_t *stage_inc, uint64_t stream, uint64_t *plan);
+/* max_count: nstage entries, the largest distinct-target count of a block;
+ * max_nthrcol: the most thread colours of a block. */
+int op2b_region_plan_info(uint64_t plan, int32_t *nblocks, int32_t *nregions, int32_t *levels,
+                          int32_t *max_count, int64_t *tlist_len, int32_t *max_nthrcol);
+/* Device arrays (int32 unless noted): 0 order [set_size] (element at each
+ * position), 1 boff [nblocks+1] (first position of each block), 2 tlist
+ * (distinct targets, block-major then staged Map), 3 toff [nblocks*nstage+1]
+ * (offset of each (block, Map) list in tlist), 4 tcnt [nblocks*nstage],
+ * 5 loc (int16) [sum of arities][set_size]: row r of staged Map s for the
+ * element at position pos is tlist[toff[b*nstage+s] + loc[(row0(s)+r)*set_size+pos]],
+ * 6 thrcol [set_size] (thread colour per position), 7 nthrcol [nblocks]. */
+int op2b_region_plan_array(uint64_t plan, int32_t which, uint64_t *dptr, int64_t *count);
+int op2b_region_plan_free(uint64_t plan);
+
+/* ------------------------------------------------------------------------
  * Sparsity: CSR pattern built on the GPU.  Replaces core.build_sparsity
  * (pyop2/op_lib_core.pyx:544-596) and build_sparsity_pattern_seq
  * (pyop2/sparsity_utils.cxx:5-51): rows = rmult*rmap+r, cols = cmult*cmap+c,

@@ -766,6 +766,76 @@ class DevicePlan(object):
             _lib._lib.op2b_plan_free(h)
 
 
+_REGION_ARRAYS = ("order", "boff", "tlist", "toff", "tcnt", "loc", "thrcol", "nthrcol")
+_REGION_CACHE = {}
+
+
+class RegionPlan(object):
+    """Locality partition of an iteration set (op2b_region_plan_build):
+    regions grown through ``grow_map`` around hashed seeds (about one per
+    ``region_size`` elements), cut into blocks of at most ``part_size``
+    elements, with each block's distinct targets of every staged Map and
+    thread colours over the targets of the staged Maps flagged in
+    ``stage_inc``."""
+
+    def __init__(self, set_size, part_size, region_size, grow_map, stage_maps, stage_inc=None):
+        ns = len(stage_maps)
+        smap = (C.c_uint64 * max(ns, 1))(*[m._to_device().ptr for m in stage_maps])
+        sar = (C.c_int32 * max(ns, 1))(*[m.dim for m in stage_maps])
+        sinc = (C.c_int32 * max(ns, 1))(*[1 if (stage_inc is None or f) else 0
+                                          for f in (stage_inc or [1] * ns)])
+        h = C.c_uint64()
+        call("op2b_region_plan_build", set_size, part_size, region_size, grow_map._to_device().ptr,
+             grow_map.dim, grow_map.dataset.total_size, ns, smap, sar, sinc, 0, C.byref(h))
+        self._handle = h.value
+        nb, nr, lv, tl, mt = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32()
+        mc = (C.c_int32 * max(ns, 1))()
+        call("op2b_region_plan_info", self._handle, C.byref(nb), C.byref(nr), C.byref(lv), mc,
+             C.byref(tl), C.byref(mt))
+        self.nblocks, self.nregions, self.levels = nb.value, nr.value, lv.value
+        self.max_nthrcol = mt.value
+        self.max_count = list(mc)[:ns]
+        self.set_size, self.part_size, self.nstage = set_size, part_size, ns
+        self._keep = [grow_map] + list(stage_maps)
+        self.dptr, self.counts = {}, {}
+        for k, name in enumerate(_REGION_ARRAYS):
+            p, n = C.c_uint64(), C.c_int64()
+            call("op2b_region_plan_array", self._handle, k, C.byref(p), C.byref(n))
+            self.dptr[name], self.counts[name] = p.value, n.value
+
+    def host_array(self, name):
+        out = np.zeros(self.counts[name], dtype=np.int16 if name == "loc" else np.int32)
+        if out.size:
+            call("op2b_memcpy_d2h", out.ctypes.data, self.dptr[name], out.nbytes, 0)
+        return out
+
+    def __getattr__(self, name):
+        if name in _REGION_ARRAYS:
+            return self.host_array(name)
+        raise AttributeError(name)
+
+    def __del__(self):
+        h = getattr(self, "_handle", 0)
+        if h and _state['init'] and _lib._lib is not None:
+            _lib._lib.op2b_region_plan_free(h)
+
+
+def region_plan(iterset, maps, region):
+    """The cached locality partition of a staged loop."""
+    ps = int(cfg.cfg['partition_size']) or 384
+    amax = max(region["stage_arity"])
+    ps = max(1, min(ps, 16384 // amax))
+    rs = int(cfg.cfg['region_size']) or max(1, ps // 2)
+    reps = [maps[k] for k in region["stage_maps"]]
+    grow = reps[region["grow"]]
+    inc = [st in region["inc_stages"] for st in range(len(reps))]
+    key = (iterset.size, ps, rs, id(grow), tuple(id(m) for m in reps), tuple(inc))
+    plan = _REGION_CACHE.get(key)
+    if plan is None:
+        plan = _REGION_CACHE[key] = RegionPlan(iterset.size, ps, rs, grow, reps, inc)
+    return plan
+
+
 def Plan(kernel, iset, *args, **kwargs):
     """Reference-compatible plan constructor (pyop2/device.py:305-322,
     plan.pyx:93-105): ``args`` are unwound Args, ``partition_size``,
@@ -1095,10 +1165,18 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
         spec.owner = owner
         spec.mode = "owner"
         indirect = False
+    elif (indirect and (inc_mode or cfg.cfg['inc_mode']) == 'staged' and codegen.staged_capable(spec)
+          and iterset.size >= int(cfg.cfg['staged_min_size'])):
+        spec.mode = "staged"
+        spec.region = _region_layout(specs, maps)
+        if block_size is None:
+            spec.block_size = bs = int(cfg.cfg['staged_block_size'])
+        indirect = False   # one launch over the locality partition's blocks
     elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'lma' and codegen.lma_capable(spec):
         spec.mode = "lma"
         indirect = False   # launched like a direct loop, then reduced per target
-    elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'atomic' and codegen.atomic_capable(spec):
+    elif (indirect and (inc_mode or cfg.cfg['inc_mode']) in ('atomic', 'staged')
+          and codegen.atomic_capable(spec)):
         spec.mode = "atomic"
         indirect = False   # launched like a direct loop: no plan
         spec.mat_slots = bool(cfg.cfg['mat_slots']) and _slots_usable(specs)
@@ -1106,6 +1184,52 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
                 iterset=iterset, block_size=bs)
+
+
+def _same_values(m1, m2):
+    """Maps with the same target Set size, arity and values (e.g. one
+    connectivity declared once per target DataSet) stage one target list."""
+    if m1 is m2:
+        return True
+    if m1.dim != m2.dim or m1.dataset.size != m2.dataset.size or m1.iterset is not m2.iterset:
+        return False
+    return np.array_equal(m1.values, m2.values)
+
+
+def _region_layout(specs, maps):
+    """Staged Maps of a staged loop: Map slots with the same values share
+    one; loc rows numbered over the staged Maps in order; INC (Dat, staged
+    Map) accumulators in order of first use; the growth Map is the INC
+    Map with the most rows."""
+    used = sorted({s.mslot for s in specs if s.kind in ("ind", "vec", "its")})
+    reps, map_stage = [], {}
+    for k in used:
+        for st, r in enumerate(reps):
+            if _same_values(maps[k], maps[r]):
+                map_stage[k] = st
+                break
+        else:
+            map_stage[k] = len(reps)
+            reps.append(k)
+    arity = [maps[r].dim for r in reps]
+    row_base = [sum(arity[:st]) for st in range(len(reps))]
+    pairs, reads = [], []
+    grow = None
+    for s in specs:
+        if s.kind not in ("ind", "vec", "its"):
+            continue
+        st = map_stage[s.mslot]
+        pr = (s.slot, st, s.ctype, s.cdim)
+        if s.access == "INC":
+            if pr not in pairs:
+                pairs.append(pr)
+            if grow is None or arity[st] > arity[grow]:
+                grow = st
+        elif s.access == "READ" and pr not in reads:
+            reads.append(pr)
+    inc_stages = sorted({st for (_, st, _, _) in pairs})
+    return dict(map_stage=map_stage, stage_arity=arity, row_base=row_base, inc_pairs=pairs,
+                read_pairs=reads, inc_stages=inc_stages, stage_maps=reps, grow=grow)
 
 
 def _sync_consts(mod, consts):
@@ -1198,9 +1322,22 @@ class _BoundLoop(object):
         self.vals = vals
         n = iterset.size
         self.range_end = n
+        self.launch_smem = 0
         if indirect:
             self.grid = 0
             self.max_grid = self.plan.max_blocks_per_color
+        elif spec.mode == "staged":
+            rp = region_plan(iterset, maps, spec.region)
+            self.region_plan = rp
+            for name in _REGION_ARRAYS:
+                vals["rg_" + name] = rp.dptr[name]
+            self.launch_smem = codegen.staged_smem(spec, rp.max_count)
+            if self.launch_smem > _state['smem_optin']:
+                raise DeviceError("par_loop %s needs %d bytes of shared memory per block; "
+                                  "lower partition_size" % (loop.kernel.name, self.launch_smem))
+            self.module.ensure_smem(self.launch_smem)
+            self.grid = rp.nblocks
+            self.max_grid = max(1, rp.nblocks)
         elif spec.mode == "lma":
             # two-phase INC: contribution arrays (phase 1, the stub) and the
             # incidences their reduction walks (phase 2, op2b_lma_reduce)
@@ -1314,7 +1451,8 @@ class _BoundLoop(object):
             call("op2b_launch_colored", mod.fn, plan.ncolors, plan.ncolblk_host, self.block_size,
                  self.smem, 0, params, self.layout.nbytes, codegen.ParamLayout.COL_OFFSET)
         else:
-            call("op2b_launch", mod.fn, self.grid, self.block_size, 0, 0, params, self.layout.nbytes)
+            call("op2b_launch", mod.fn, self.grid, self.block_size, self.launch_smem, 0, params,
+                 self.layout.nbytes)
         if self.spec.mode == "lma":
             kahan = 1 if self.kahan else 0            # OP2B_LMA_KAHAN
             for buf, inc, target, cdim, ntargets, arity, mask in self.lma:
@@ -1350,7 +1488,8 @@ def _env_key():
         _ENV["key"] = (tuple((c.name, c.dtype.str, c.cdim) for c in base.Const._definitions()),
                        (cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
                         cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode'], cfg.cfg['owner_mode'],
-                        cfg.cfg['kahan'], cfg.cfg['mat_slots']))
+                        cfg.cfg['kahan'], cfg.cfg['mat_slots'], cfg.cfg['region_size'],
+                        cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

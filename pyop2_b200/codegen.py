@@ -79,6 +79,11 @@ class LoopSpec(object):
         # scalar Mats found through scatter-slot tables (op2b_mat_slots_build)
         # instead of a row search per entry (atomic and batched forms)
         self.mat_slots = False
+        # staged form over a locality partition (mode 'staged'): map_stage
+        # {map slot: staged Map}, stage_arity, row_base (first loc row of each
+        # staged Map), read_pairs / inc_pairs [(Dat slot, staged Map, ctype,
+        # cdim)] staged / accumulated in shared memory
+        self.region = None
         self.kernel_name = kernel_name
         self.kernel_code = kernel_code
         self.extents = tuple(extents)
@@ -100,12 +105,20 @@ class LoopSpec(object):
                 tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
                 self.block_size, self.fmad, self.min_blocks, self.mode,
                 tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
-                self.mat_slots)
+                self.mat_slots, _freeze(self.region))
 
     @property
     def needs_coloring(self):
         return any(a.kind == "mat" or (a.kind in ("ind", "vec", "its") and a.access == "INC")
                    for a in self.args)
+
+
+def _freeze(v):
+    if isinstance(v, dict):
+        return tuple(sorted((k, _freeze(x)) for k, x in v.items()))
+    if isinstance(v, (list, tuple)):
+        return tuple(_freeze(x) for x in v)
+    return v
 
 
 class ParamLayout(object):
@@ -122,6 +135,9 @@ class ParamLayout(object):
         if spec.mode == "plan":
             f += ["blkmap", "offset", "nelems", "nthrcol", "thrcol", "ind_map", "ind_sizes",
                   "ind_offs", "loc_map"]
+        if spec.mode == "staged":
+            f += ["rg_order", "rg_boff", "rg_tlist", "rg_toff", "rg_tcnt", "rg_loc", "rg_thrcol",
+                  "rg_nthrcol"]
         for j in range(len(spec.dats)):
             f.append("d%d" % j)
             if spec.dats[j][1]:
@@ -161,7 +177,10 @@ def _struct_decl(spec, layout):
     types = {"blkmap": "const int *", "offset": "const int *", "nelems": "const int *",
              "nthrcol": "const int *", "thrcol": "const int *", "ind_map": "const int *",
              "ind_sizes": "const int *", "ind_offs": "const int *", "loc_map": "const short *",
-             "err": "int *", "inc_ptr": "const int *", "inc_list": "const int *"}
+             "err": "int *", "inc_ptr": "const int *", "inc_list": "const int *",
+             "rg_order": "const int *", "rg_boff": "const int *", "rg_tlist": "const int *",
+             "rg_toff": "const int *", "rg_tcnt": "const int *", "rg_loc": "const short *",
+             "rg_thrcol": "const int *", "rg_nthrcol": "const int *"}
     for n in layout.fields:
         if n in types:
             t = types[n]
@@ -244,7 +263,7 @@ def generate(spec):
         w(_batch_body(spec))
         return "\n".join(out), layout, batch_stub_names(spec)[0]
     body = {"plan": _indirect_body, "atomic": _atomic_body, "lma": _atomic_body,
-            "direct": _direct_body, "owner": _owner_body}[spec.mode](spec)
+            "direct": _direct_body, "owner": _owner_body, "staged": _staged_body}[spec.mode](spec)
     w(body)
     return "\n".join(out), layout, stub_name(spec)
 
@@ -514,6 +533,197 @@ def _atomic_body(spec):
              " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
     L += _atomic_element(spec, "    ")
     L.append("  }")
+    _gbl_epilogue(spec, L)
+    L.append("}")
+    return "\n".join(L)
+
+
+def staged_capable(spec):
+    """Loops the staged form runs: indirect Dat args only (no Mats), at
+    least one indirect INC."""
+    inc = False
+    for a in spec.args:
+        if a.kind == "mat":
+            return False
+        if a.kind in ("ind", "vec", "its") and a.access == "INC":
+            inc = True
+    return inc
+
+
+_CSIZE = {"double": 8, "float": 4, "int": 4, "unsigned int": 4, "long": 8, "long long": 8,
+          "unsigned long": 8, "unsigned long long": 8, "short": 2, "unsigned short": 2,
+          "char": 1, "unsigned char": 1, "signed char": 1}
+
+
+def staged_smem(spec, max_count):
+    """Dynamic shared memory of a staged launch: the staged READ rows and
+    the INC accumulators, each 16-byte aligned, at the largest per-block
+    target counts."""
+    R = spec.region
+    nb = 0
+    for (slot, st, ctype, cdim) in R["read_pairs"] + R["inc_pairs"]:
+        nb += (max_count[st] * cdim * _CSIZE[ctype] + 15) // 16 * 16
+    return nb
+
+
+def staged_used(spec):
+    R = spec.region
+    used_maps = {a.mslot for a in spec.args if a.kind in ("ind", "vec", "its")}
+    return sorted({R["map_stage"][k] for k in used_maps})
+
+
+def _staged_body(spec):
+    """Indirect loop over a locality partition (op2b_region_plan_build), one
+    CTA per block of the reordered set.  The block's distinct target rows
+    of every READ (Dat, staged Map) pair are copied to shared memory once;
+    INC rows are added into shared accumulators colour by colour (the
+    plan's thread colours: no two elements of a colour share a target, so
+    the adds need no atomics) and added to the Dats once per distinct
+    target at the end, with global atomics since neighbouring blocks share
+    targets.  WRITE/RW indirect rows are global pointers (OP2 leaves their
+    conflicts to the user)."""
+    bs = spec.block_size
+    R = spec.region
+    ns = len(R["stage_arity"])
+    used = staged_used(spec)
+    read_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["read_pairs"])}
+    inc_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["inc_pairs"])}
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
+    L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
+    L.append("  const int blk = blockIdx.x;")
+    L.append("  const int start = p.rg_boff[blk];")
+    L.append("  const int nelem = p.rg_boff[blk + 1] - start;")
+    L.append("  const op2b_i64 set_size = p.set_size;")
+    L.append("  int smem_off = 0;")
+    for st in used:
+        L.append("  const int n_s%d = p.rg_tcnt[blk * %d + %d];" % (st, ns, st))
+        L.append("  const int *tl_s%d = p.rg_tlist + p.rg_toff[blk * %d + %d];" % (st, ns, st))
+    for q, (slot, st, t, c) in enumerate(R["read_pairs"]):
+        L.append("  %s *rd%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
+        L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
+    # staged READ rows: one target id per row, the rows of every READ pair of
+    # the staged Map copied asynchronously (cp.async) where their size allows
+    for st in used:
+        pairs = [(q, slot, t, c) for q, (slot, s_, t, c) in enumerate(R["read_pairs"]) if s_ == st]
+        if not pairs:
+            continue
+        L.append("  for (int r = threadIdx.x; r < n_s%d; r += %d) {" % (st, bs))
+        L.append("    const op2b_i64 g = tl_s%d[r];" % st)
+        for q, slot, t, c in pairs:
+            nb = c * _CSIZE[t]
+            if nb % 4 == 0:
+                L.append("    op2b_cp_async_row<%d>(rd%d + r * %d, p.d%d + g * %d);" % (nb, q, c, slot, c))
+            else:
+                L.append("    for (int k = 0; k < %d; ++k) rd%d[r * %d + k] = p.d%d[g * %d + k];"
+                         % (c, q, c, slot, c))
+        L.append("  }")
+    for q, (slot, st, t, c) in enumerate(R["inc_pairs"]):
+        L.append("  %s *acc%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
+        L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
+        L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) acc%d[t] = (%s)0;"
+                 % (st, c, bs, q, t))
+    if R["read_pairs"]:
+        L.append("  op2b_cp_async_wait();")
+    L.append("  __syncthreads();")
+    _gbl_prologue(spec, L)
+    L.append("  const int ncol = p.rg_nthrcol[blk];")
+    L.append("  for (int base = 0; base < nelem; base += %d) {" % bs)
+    L.append("    const int idx = base + threadIdx.x;")
+    L.append("    const bool active = idx < nelem;")
+    L.append("    const op2b_i64 pos = start + (active ? idx : 0);")
+    ind = "    "
+    if any(a.kind == "direct" for a in spec.args):
+        L.append("%sconst op2b_i64 e = p.rg_order[pos];" % ind)
+    for st in used:
+        ar = R["stage_arity"][st]
+        L.append("%sint sl%d[%d];" % (ind, st, ar))
+        L.append("%s#pragma unroll" % ind)
+        L.append("%sfor (int r = 0; r < %d; ++r) sl%d[r] = active ? (int)p.rg_loc[(op2b_i64)(%d + r) * "
+                 "set_size + pos] : 0;" % (ind, ar, st, R["row_base"][st]))
+    decl, pre, post, exprs, adds = [], [], [], [], []
+    for n, a in enumerate(spec.args):
+        t, c = a.ctype, a.cdim
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
+            continue
+        if a.kind == "direct":
+            exprs.append(_direct_row(a, n, "e", pre, post, ind + "  "))
+            continue
+        st = R["map_stage"][a.mslot]
+        cnt = a.arity if a.kind == "vec" else a.ext
+
+        def row_ptr(rowexpr):
+            if a.access == "READ":
+                return "rd%d + %s * %d" % (read_of[(a.slot, st)], "sl%d[%s]" % (st, rowexpr), c)
+            return "p.d%d + (op2b_i64)tl_s%d[sl%d[%s]] * %d" % (a.slot, st, st, rowexpr, c)
+        if a.access == "READ":
+            # staged rows into registers with vector shared-memory loads
+            if a.kind == "ind":
+                pre.append("%s  __align__(16) %s a%d[%d];" % (ind, t, n, c))
+                pre.append("%s  op2b_load<%s, %d, false>(a%d, %s);" % (ind, t, c, n, row_ptr(str(a.idx))))
+                exprs.append("a%d" % n)
+            else:
+                pre.append("%s  __align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
+                for r in range(cnt):
+                    pre.append("%s  op2b_load<%s, %d, false>(a%d[%d], %s);" % (ind, t, c, n, r, row_ptr(str(r))))
+                if a.kind == "vec":
+                    pre.append("%s  %s *a%d_v[%d] = {%s};" %
+                               (ind, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
+                    exprs.append("a%d_v" % n)
+                else:
+                    exprs.append("a%d[i%d]" % (n, a.idx))
+            continue
+        if a.access == "INC":
+            q = inc_of[(a.slot, st)]
+            if a.kind == "ind":
+                decl.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind, t, n, c, n))
+                exprs.append("a%d" % n)
+                adds.append(("a%d" % n, "sl%d[%d]" % (st, a.idx), q, c))
+            else:
+                decl.append("%s__align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
+                decl.append("%sfor (int q = 0; q < %d; ++q) op2b_zero(a%d[q]);" % (ind, cnt, n))
+                for r in range(cnt):
+                    adds.append(("a%d[%d]" % (n, r), "sl%d[%d]" % (st, r), q, c))
+                if a.kind == "vec":
+                    pre.append("%s  %s *a%d_v[%d] = {%s};" %
+                               (ind, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
+                    exprs.append("a%d_v" % n)
+                else:
+                    exprs.append("a%d[i%d]" % (n, a.idx))
+        else:
+            if a.kind == "ind":
+                exprs.append(row_ptr(str(a.idx)))
+            elif a.kind == "vec":
+                pre.append("%s  %s *a%d_v[%d] = {%s};" %
+                           (ind, t, n, cnt, ", ".join(row_ptr(str(r)) for r in range(cnt))))
+                exprs.append("a%d_v" % n)
+            else:
+                exprs.append(row_ptr("i%d" % a.idx))
+    L += decl
+    L.append("%sint col = -1;" % ind)
+    L.append("%sif (active) {" % ind)
+    L += pre
+    L += _itspace_open(spec, ind + "  ")
+    L.append(_kernel_call(spec, exprs, ind + "  " + "  " * len(spec.extents)))
+    L += _itspace_close(spec, ind + "  ")
+    L += post
+    L.append("%s  col = p.rg_thrcol[pos];" % ind)
+    L.append("%s}" % ind)
+    L.append("%sfor (int c = 0; c < ncol; ++c) {" % ind)
+    L.append("%s  if (col == c) {" % ind)
+    for var, lrow, q, c in adds:
+        L.append("%s    { %s *dst = acc%d + %s * %d;" % (ind, R["inc_pairs"][q][2], q, lrow, c))
+        L.append("%s      for (int k = 0; k < %d; ++k) dst[k] += %s[k]; }" % (ind, c, var))
+    L.append("%s  }" % ind)
+    L.append("%s  __syncthreads();" % ind)
+    L.append("%s}" % ind)
+    L.append("  }")
+    for q, (slot, st, ctype, cdim) in enumerate(R["inc_pairs"]):
+        L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (st, cdim, bs))
+        L.append("    const int r = t / %d, k = t - r * %d;" % (cdim, cdim))
+        L.append("    op2b_atomic_add(p.d%d + (op2b_i64)tl_s%d[r] * %d + k, acc%d[t]);"
+                 % (slot, st, cdim, q))
+        L.append("  }")
     _gbl_epilogue(spec, L)
     L.append("}")
     return "\n".join(L)

@@ -23,7 +23,20 @@ keys of the B200 backend:
   every contribution, then each target adds its contributions in element
   order -- the sequential backend's order -- optionally Kahan-compensated;
   deterministic and independent of the launch configuration; loops it cannot
-  run fall back to ``'color'``);
+  run fall back to ``'color'``) or ``'staged'`` (one launch over a locality
+  partition: the set is reordered into compact regions grown on the GPU,
+  each block's distinct targets are staged in shared memory and INC rows
+  accumulated there, then added once per target with atomics; summation
+  order varies between runs within rounding; loops without indirect INC or
+  with Mats run as ``'atomic'``);
+* ``region_size``: elements per region (one hashed seed per about this many
+  elements) of the staged form's locality partition (0: half the partition
+  size, whose default in the staged form is 384);
+* ``staged_block_size``: threads per CTA of the staged form's stubs (one
+  CTA per block of the partition);
+* ``staged_min_size``: iteration sets smaller than this run the atomic form
+  even when ``inc_mode`` is ``'staged'`` (a partition of them has too few
+  blocks to fill the GPU);
 * ``owner_mode``: owner-computes for loops whose only write is INC into one
   Dat through one Map or into one scalar Mat: one warp per target adds the
   target's contributions in the sequential backend's order and writes it once
@@ -60,6 +73,9 @@ _defaults = {
     'l2_fetch_granularity': 32,
     'min_blocks_per_sm': 0,
     'inc_mode': 'atomic',
+    'region_size': 0,
+    'staged_min_size': 65536,
+    'staged_block_size': 128,
     'owner_mode': 'never',
     'kahan': False,
     'mat_slots': True,

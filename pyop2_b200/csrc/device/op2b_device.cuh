@@ -20,6 +20,37 @@ typedef unsigned long long op2b_u64;
 
 #define OP2B_FULL_MASK 0xffffffffu
 
+// Asynchronous copy (cp.async) of one row of B bytes, B a multiple of 4,
+// from global to shared memory in 16-, 8- or 4-byte pieces as the size
+// allows; both addresses must be aligned to the piece size.
+// op2b_cp_async_wait() waits for every copy the thread has issued.
+template <int B>
+__device__ __forceinline__ void op2b_cp_async_row(void *dst, const void *src) {
+  unsigned long long s;
+  asm("cvta.to.shared.u64 %0, %1;" : "=l"(s) : "l"(dst));
+  const unsigned sa = (unsigned)s;
+  const char *g = reinterpret_cast<const char *>(src);
+  if constexpr (B % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < B / 16; ++i)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa + 16 * i), "l"(g + 16 * i)
+                   : "memory");
+  } else if constexpr (B % 8 == 0) {
+#pragma unroll
+    for (int i = 0; i < B / 8; ++i)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa + 8 * i), "l"(g + 8 * i)
+                   : "memory");
+  } else {
+    static_assert(B % 4 == 0, "cp.async rows are multiples of 4 bytes");
+#pragma unroll
+    for (int i = 0; i < B / 4; ++i)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa + 4 * i), "l"(g + 4 * i)
+                   : "memory");
+  }
+}
+
+__device__ __forceinline__ void op2b_cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename T, int N, bool RO>
 __device__ __forceinline__ void op2b_load(T (&dst)[N], const T *__restrict__ src) {
   constexpr int B = N * (int)sizeof(T);

@@ -1,0 +1,543 @@
+// Locality partition of an iteration set for staged indirect loops.
+//
+// The reference partitions an iteration set into blocks of consecutive
+// elements (pyop2/plan.pyx:107-110) and stages each block's indirectly
+// accessed rows in shared memory (:112-212).  Consecutive elements share
+// targets only if the mesh numbering is local; on a permuted numbering a
+// block of 1024 edges touches ~1300 distinct cells and staging saves nothing.
+// This builder reorders the set instead:
+//  * regions: seeds are picked by hashing element ids (about one per
+//    region_size elements); a multi-source breadth-first search over the
+//    element graph (two elements adjacent when they share a target of the
+//    growth Map) gives every element the key (level, region) of the nearest
+//    seed, ties to the smaller region id, so the result does not depend on
+//    scheduling;
+//  * order: elements sorted by (region, level, element id);
+//  * blocks: each region cut into nearly equal runs of at most part_size
+//    elements;
+//  * staging: per block and staged Map the sorted distinct targets over all
+//    Map rows (tlist / toff / tcnt) and, per position of the reordered set
+//    and Map row, the target's index in that list (loc, int16);
+//  * thread colouring: per block, the reference's greedy colouring
+//    (pyop2/plan.pyx:282-324: elements in order, 32-colour masks per round)
+//    over the targets of the staged Maps marked as INC targets, so elements
+//    of one colour never add to the same staged row (thrcol per position,
+//    nthrcol per block).
+// A staged stub (see codegen) walks block b over positions
+// boff[b] .. boff[b+1], element order[pos], and finds row r of staged Map s
+// at tlist[toff[b][s] + loc[row_base(s) + r][pos]].
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "op2b_block_sort.cuh"
+#include "op2b_internal.h"
+#include "op2b_scan.cuh"
+
+extern "C" int op2b_incidence_build(uint64_t map, int32_t nelem, int32_t arity, int32_t ntargets,
+                                    uint64_t stream, uint64_t *incidence);
+extern "C" int op2b_incidence_arrays(uint64_t incidence, uint64_t *ptr, uint64_t *list,
+                                     int32_t *max_degree);
+extern "C" int op2b_incidence_free(uint64_t incidence);
+
+namespace op2b {
+
+struct RegionPlan {
+  int32_t set_size = 0, part_size = 0, nblocks = 0, nstage = 0, nregions = 0, levels = 0;
+  int32_t loc_rows = 0;
+  int64_t tlist_len = 0;
+  int32_t *order = nullptr, *boff = nullptr, *tlist = nullptr, *toff = nullptr, *tcnt = nullptr;
+  int32_t *thrcol = nullptr, *nthrcol = nullptr;
+  int16_t *loc = nullptr;
+  int32_t max_nthrcol = 0;
+  std::vector<int32_t> max_count;   // per staged Map: largest tcnt over blocks
+};
+
+constexpr int kRgThreads = 256;
+constexpr int kRgMaxKeys = 16384;          // part_size * arity per staged Map
+constexpr uint64_t kUnset = ~0ull;
+constexpr int kRgLevelChunk = 8;           // BFS levels between two looks at progress
+constexpr int kRgMaxLevels = 1 << 16;
+
+__device__ __forceinline__ uint32_t rg_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+
+__global__ void rg_seed_kernel(int n, int region_size, int32_t *__restrict__ flag) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    flag[e] = (e == 0 || rg_hash((uint32_t)e) % (uint32_t)region_size == 0) ? 1 : 0;
+}
+
+// key = level << 32 | region; seeds start at level 0 with their rank as region.
+__global__ void rg_init_kernel(int n, const int32_t *__restrict__ flag, const int32_t *__restrict__ rank,
+                               uint64_t *__restrict__ ekey) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    ekey[e] = flag[e] ? (uint64_t)(uint32_t)rank[e] : kUnset;
+}
+
+// Elements of level L hand their key to their targets (the smallest wins).
+__global__ void rg_push_kernel(int n, const int32_t *__restrict__ map, int arity, int ntargets,
+                               uint32_t level,
+                               const uint64_t *__restrict__ ekey,
+                               unsigned long long *__restrict__ tkey) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const uint64_t k = ekey[e];
+    if (k == kUnset || (uint32_t)(k >> 32) != level) continue;
+    for (int r = 0; r < arity; ++r) {
+      const int t = map[(int64_t)e * arity + r];
+      if (t >= 0 && t < ntargets) atomicMin(&tkey[t], (unsigned long long)k);
+    }
+  }
+}
+
+// Unlabelled elements take the smallest key among their targets, one level
+// further.  Every labelled target of an unlabelled element carries the
+// current level (an earlier one would have labelled the element earlier).
+__global__ void rg_pull_kernel(int n, const int32_t *__restrict__ map, int arity, int ntargets,
+                               uint64_t *__restrict__ ekey, const unsigned long long *__restrict__ tkey,
+                               int32_t *__restrict__ changed) {
+  int any = 0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    if (ekey[e] != kUnset) continue;
+    uint64_t best = kUnset;
+    for (int r = 0; r < arity; ++r) {
+      const int t = map[(int64_t)e * arity + r];
+      if (t >= 0 && t < ntargets) best = min(best, (uint64_t)tkey[t]);
+    }
+    if (best != kUnset) {
+      ekey[e] = ((best >> 32) + 1) << 32 | (best & 0xffffffffull);
+      any = 1;
+    }
+  }
+  if (__syncthreads_or(any) && threadIdx.x == 0) *changed = 1;
+}
+
+// Bucket of each element: region * nlevels + level; elements the search did
+// not reach (components without a seed) form regions of consecutive ids.
+__global__ void rg_bucket_kernel(int n, const uint64_t *__restrict__ ekey, int nseeds, int part_size,
+                                 int nlevels, int32_t *__restrict__ bucket) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const uint64_t k = ekey[e];
+    int64_t region, level;
+    if (k == kUnset) {
+      region = nseeds + e / part_size;
+      level = 0;
+    } else {
+      region = (int64_t)(k & 0xffffffffull);
+      level = (int64_t)(k >> 32);
+    }
+    bucket[e] = (int32_t)(region * nlevels + (nlevels > 1 ? level : 0));
+  }
+}
+
+// First position of every region in the sorted order.
+__global__ void rg_region_start_kernel(const int32_t *__restrict__ bptr, int nregions, int nlevels,
+                                       int32_t *__restrict__ rstart) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= nregions; r += gridDim.x * blockDim.x)
+    rstart[r] = bptr[(int64_t)r * nlevels];
+}
+
+struct RgStage {
+  const int32_t *map;
+  int32_t arity, loc_row;
+  int64_t cap;       // part_size * arity
+  int32_t *tmp;      // [nblocks][cap] distinct targets
+};
+
+// grid (nblocks, nstage): the distinct targets of the block's elements over
+// all rows of one staged Map, numbered in order of first use (keys taken
+// position by position, rows in order), and each (position, row)'s number.
+// Neighbouring elements of a block (one ring of the breadth-first search)
+// touch neighbouring targets, so first-use numbers put the rows a warp reads
+// close together in shared memory.
+__global__ void rg_stage_kernel(const RgStage *__restrict__ stages, int nstage, int set_size,
+                                const int32_t *__restrict__ order, const int32_t *__restrict__ boff,
+                                int npow2, int32_t *__restrict__ tcnt, int16_t *__restrict__ loc) {
+  extern __shared__ int rg_smem[];
+  const int blk = blockIdx.x, s = blockIdx.y;
+  const RgStage st = stages[s];
+  const int start = boff[blk], nelem = boff[blk + 1] - start;
+  const int nkeys = nelem * st.arity;
+  int *a = rg_smem;             // keys, then (first use << 14 | sorted rank) pairs
+  int *u = rg_smem + npow2;     // sorted distinct targets
+  const int n = next_pow2_dev(nkeys);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int v = INT_MAX;
+    if (i < nkeys) {
+      const int q = i / st.arity, r = i - q * st.arity;
+      v = st.map[(int64_t)order[start + q] * st.arity + r];
+    }
+    a[i] = v;
+  }
+  __syncthreads();
+  block_bitonic_sort(a, n);
+  const int nu = block_unique(a, nkeys, n, u);
+  // first use of every distinct target (keys < 16384, so 14 bits each)
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = INT_MAX;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nkeys; i += blockDim.x) {
+    const int q = i / st.arity, r = i - q * st.arity;
+    const int j = lower_bound(u, nu, st.map[(int64_t)order[start + q] * st.arity + r]);
+    atomicMin(&a[j], (i << 14) | j);
+  }
+  __syncthreads();
+  block_bitonic_sort(a, next_pow2_dev(nu));
+  // a[k] & 0x3fff: sorted rank of the k-th target by first use; invert it
+  int *num = u + npow2;         // [nu] first-use number of each sorted rank
+  for (int k = threadIdx.x; k < nu; k += blockDim.x) {
+    const int j = a[k] & 0x3fff;
+    st.tmp[(int64_t)blk * st.cap + k] = u[j];
+    num[j] = k;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nkeys; i += blockDim.x) {
+    const int q = i / st.arity, r = i - q * st.arity;
+    const int v = st.map[(int64_t)order[start + q] * st.arity + r];
+    loc[(int64_t)(st.loc_row + r) * set_size + start + q] = (int16_t)num[lower_bound(u, nu, v)];
+  }
+  if (threadIdx.x == 0) tcnt[blk * nstage + s] = nu;
+}
+
+// One CTA per block: greedy thread colouring in position order over the
+// block-local targets of the INC staged Maps (masks of 32 colours per round,
+// as pyop2/plan.pyx:282-324); run by one thread, the masks in shared memory.
+__global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_t *__restrict__ inc,
+                                int nstage, int set_size, const int32_t *__restrict__ boff,
+                                const int32_t *__restrict__ tcnt, const int16_t *__restrict__ loc,
+                                int32_t *__restrict__ thrcol, int32_t *__restrict__ nthrcol) {
+  extern __shared__ uint32_t rg_masks[];
+  const int blk = blockIdx.x;
+  const int start = boff[blk], nelem = boff[blk + 1] - start;
+  // local target numbering: the INC staged Maps' lists one after the other
+  __shared__ int s_base[64];
+  __shared__ int s_total;
+  if (threadIdx.x == 0) {
+    int b = 0;
+    for (int q = 0; q < nstage; ++q) {
+      s_base[q] = b;
+      if (inc[q]) b += tcnt[blk * nstage + q];
+    }
+    s_total = b;
+  }
+  __syncthreads();
+  const int total = s_total;
+  for (int i = threadIdx.x; i < nelem; i += blockDim.x) thrcol[start + i] = -1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int base = 0, remaining = nelem, ncol = 0;
+    while (remaining > 0) {
+      for (int i = 0; i < total; ++i) rg_masks[i] = 0u;
+      remaining = 0;
+      for (int i = 0; i < nelem; ++i) {
+        if (thrcol[start + i] >= 0) continue;
+        uint32_t m = 0u;
+        for (int q = 0; q < nstage; ++q) {
+          if (!inc[q]) continue;
+          for (int r = 0; r < stages[q].arity; ++r)
+            m |= rg_masks[s_base[q] + loc[(int64_t)(stages[q].loc_row + r) * set_size + start + i]];
+        }
+        if (m == 0xffffffffu) {
+          ++remaining;
+          continue;
+        }
+        const int c = __ffs(~m) - 1;
+        thrcol[start + i] = base + c;
+        ncol = max(ncol, base + c + 1);
+        for (int q = 0; q < nstage; ++q) {
+          if (!inc[q]) continue;
+          for (int r = 0; r < stages[q].arity; ++r)
+            rg_masks[s_base[q] + loc[(int64_t)(stages[q].loc_row + r) * set_size + start + i]] |= 1u << c;
+        }
+      }
+      base += 32;
+    }
+    nthrcol[blk] = ncol;
+  }
+}
+
+__global__ void rg_compact_kernel(const RgStage *__restrict__ stages, int nstage,
+                                  const int32_t *__restrict__ tcnt, const int32_t *__restrict__ toff,
+                                  int32_t *__restrict__ tlist) {
+  const int blk = blockIdx.x, s = blockIdx.y;
+  const RgStage st = stages[s];
+  const int nu = tcnt[blk * nstage + s];
+  const int64_t dst = toff[blk * nstage + s];
+  for (int i = threadIdx.x; i < nu; i += blockDim.x) tlist[dst + i] = st.tmp[(int64_t)blk * st.cap + i];
+}
+
+static int rg_grid(int64_t n) {
+  return std::max(1, std::min(op2b_div_up(std::max<int64_t>(n, 1), kRgThreads), sm_count() * 8));
+}
+
+}  // namespace op2b
+
+using namespace op2b;
+
+static void region_release(RegionPlan *p, cudaStream_t s) {
+  if (!p) return;
+  int32_t *arrs[] = {p->order, p->boff, p->tlist, p->toff, p->tcnt, p->thrcol, p->nthrcol};
+  for (int32_t *a : arrs) dev_free(a, s);
+  dev_free(p->loc, s);
+  delete p;
+}
+
+extern "C" {
+
+int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_size,
+                           uint64_t grow_map, int32_t grow_arity, int32_t grow_ntargets,
+                           int32_t nstage, const uint64_t *stage_map, const int32_t *stage_arity,
+                           const int32_t *stage_inc, uint64_t stream, uint64_t *plan_out) {
+  OP2B_REQUIRE_INIT();
+  if (set_size < 0 || part_size <= 0 || region_size <= 0 || grow_arity <= 0 || grow_ntargets < 0 ||
+      nstage < 0 || nstage > 64 || !plan_out ||
+      (nstage > 0 && (!stage_map || !stage_arity || !stage_inc)))
+    return set_error(OP2B_ERR_ARG, "region plan: set_size %d part_size %d region_size %d",
+                     set_size, part_size, region_size);
+  int max_arity = 1, loc_rows = 0;
+  for (int q = 0; q < nstage; ++q) {
+    if (stage_arity[q] <= 0) return set_error(OP2B_ERR_ARG, "region plan: arity %d", stage_arity[q]);
+    max_arity = std::max(max_arity, (int)stage_arity[q]);
+    loc_rows += stage_arity[q];
+  }
+  if ((int64_t)part_size * max_arity > kRgMaxKeys)
+    return set_error(OP2B_ERR_ARG,
+                     "region plan: part_size %d x arity %d exceeds %d staged keys per block",
+                     part_size, max_arity, kRgMaxKeys);
+  cudaStream_t s = stream_of(stream);
+  RegionPlan *P = new RegionPlan();
+  P->set_size = set_size;
+  P->part_size = part_size;
+  P->nstage = nstage;
+  P->loc_rows = loc_rows;
+  P->max_count.assign(nstage, 0);
+  std::vector<void *> temps;
+  uint64_t inc = 0;
+  auto fail = [&](int rc) {
+    for (void *t : temps) dev_free(t, s);
+    if (inc) op2b_incidence_free(inc);
+    region_release(P, s);
+    return rc;
+  };
+#define RG_TRY(call)              \
+  do {                            \
+    int _rc = (call);             \
+    if (_rc) return fail(_rc);    \
+  } while (0)
+#define RG_CUDA(call) RG_TRY(check_cuda((call), #call))
+  auto alloc = [&](void **p, size_t bytes, bool temp) {
+    int rc = dev_alloc(p, std::max<size_t>(bytes, 16), s);
+    if (!rc && temp) temps.push_back(*p);
+    return rc;
+  };
+  const int n = set_size;
+  const int grid = rg_grid(n);
+  const int32_t *gmap = reinterpret_cast<const int32_t *>(grow_map);
+
+  // ---- regions: seeds, then a multi-source breadth-first search
+  int32_t *flag = nullptr, *rank = nullptr, *scal = nullptr;
+  uint64_t *ekey = nullptr;
+  unsigned long long *tkey = nullptr;
+  RG_TRY(alloc((void **)&flag, sizeof(int32_t) * n, true));
+  RG_TRY(alloc((void **)&rank, sizeof(int32_t) * n, true));
+  RG_TRY(alloc((void **)&scal, sizeof(int32_t) * (kRgLevelChunk + 2), true));
+  RG_TRY(alloc((void **)&ekey, sizeof(uint64_t) * n, true));
+  RG_TRY(alloc((void **)&tkey, sizeof(uint64_t) * (size_t)grow_ntargets, true));
+  int nseeds = 0, levels = 0;
+  if (n > 0) {
+    rg_seed_kernel<<<grid, kRgThreads, 0, s>>>(n, region_size, flag);
+    RG_TRY(device_excl_scan(flag, rank, n, scal, s));
+    RG_CUDA(cudaMemcpyAsync(&nseeds, scal, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    rg_init_kernel<<<grid, kRgThreads, 0, s>>>(n, flag, rank, ekey);
+    RG_CUDA(cudaMemsetAsync(tkey, 0xff, sizeof(uint64_t) * (size_t)grow_ntargets, s));
+    // levels in chunks; changed[j] records whether level base+j labelled anything
+    for (int base = 0; base < kRgMaxLevels; base += kRgLevelChunk) {
+      RG_CUDA(cudaMemsetAsync(scal, 0, sizeof(int32_t) * kRgLevelChunk, s));
+      for (int j = 0; j < kRgLevelChunk; ++j) {
+        rg_push_kernel<<<grid, kRgThreads, 0, s>>>(n, gmap, grow_arity, grow_ntargets,
+                                                   (uint32_t)(base + j), ekey, tkey);
+        rg_pull_kernel<<<grid, kRgThreads, 0, s>>>(n, gmap, grow_arity, grow_ntargets, ekey, tkey,
+                                                   scal + j);
+      }
+      int32_t changed[kRgLevelChunk];
+      RG_CUDA(cudaGetLastError());
+      RG_CUDA(cudaMemcpyAsync(changed, scal, sizeof changed, cudaMemcpyDeviceToHost, s));
+      RG_CUDA(cudaStreamSynchronize(s));
+      int last = -1;
+      for (int j = 0; j < kRgLevelChunk; ++j)
+        if (changed[j]) last = j;
+      if (last >= 0) levels = base + last + 1;
+      if (last < kRgLevelChunk - 1) break;
+    }
+  }
+  const int nlevels_all = levels + 1;   // levels 0 .. levels
+  const int nregions = nseeds + op2b_div_up(std::max(n, 1), part_size);
+  // sort key: (region, level) when the bucket count stays moderate, else region
+  int nlevels = nlevels_all;
+  if ((int64_t)nregions * nlevels > std::max<int64_t>(4LL * n, 1 << 20) ||
+      (int64_t)nregions * nlevels >= INT_MAX)
+    nlevels = 1;
+  P->nregions = nregions;
+  P->levels = nlevels_all;
+
+  // ---- order: counting sort by bucket, element ids ascending inside one
+  int32_t *bucket = rank;   // reuse
+  std::vector<int32_t> h_rstart(nregions + 1, 0);
+  RG_TRY(alloc((void **)&P->order, sizeof(int32_t) * n, false));
+  if (n > 0) {
+    rg_bucket_kernel<<<grid, kRgThreads, 0, s>>>(n, ekey, nseeds, part_size, nlevels, bucket);
+    RG_CUDA(cudaGetLastError());
+    const int nbuckets = nregions * nlevels;
+    RG_TRY(op2b_incidence_build(reinterpret_cast<uint64_t>(bucket), n, 1, nbuckets, stream, &inc));
+    uint64_t bptr = 0, blist = 0;
+    int32_t maxdeg = 0;
+    RG_TRY(op2b_incidence_arrays(inc, &bptr, &blist, &maxdeg));
+    RG_CUDA(cudaMemcpyAsync(P->order, reinterpret_cast<void *>(blist), sizeof(int32_t) * n,
+                            cudaMemcpyDeviceToDevice, s));
+    int32_t *rstart = nullptr;
+    RG_TRY(alloc((void **)&rstart, sizeof(int32_t) * (nregions + 1), true));
+    rg_region_start_kernel<<<rg_grid(nregions + 1), kRgThreads, 0, s>>>(
+        reinterpret_cast<const int32_t *>(bptr), nregions, nlevels, rstart);
+    RG_CUDA(cudaGetLastError());
+    RG_CUDA(cudaMemcpyAsync(h_rstart.data(), rstart, sizeof(int32_t) * (nregions + 1),
+                            cudaMemcpyDeviceToHost, s));
+    RG_CUDA(cudaStreamSynchronize(s));
+    RG_TRY(op2b_incidence_free(inc));
+    inc = 0;
+  }
+
+  // ---- blocks: every region cut into nearly equal runs of <= part_size
+  std::vector<int32_t> h_boff;
+  h_boff.push_back(0);
+  for (int r = 0; r < nregions; ++r) {
+    const int a = h_rstart[r], cnt = h_rstart[r + 1] - a;
+    if (cnt <= 0) continue;
+    const int pieces = op2b_div_up(cnt, part_size);
+    for (int q = 1; q <= pieces; ++q) h_boff.push_back(a + (int)((int64_t)cnt * q / pieces));
+  }
+  const int nblocks = (int)h_boff.size() - 1;
+  P->nblocks = nblocks;
+  RG_TRY(alloc((void **)&P->boff, sizeof(int32_t) * (nblocks + 1), false));
+  RG_CUDA(cudaMemcpyAsync(P->boff, h_boff.data(), sizeof(int32_t) * (nblocks + 1),
+                          cudaMemcpyHostToDevice, s));
+
+  // ---- staging lists of every staged Map
+  RG_TRY(alloc((void **)&P->tcnt, sizeof(int32_t) * (size_t)nblocks * nstage, false));
+  RG_TRY(alloc((void **)&P->toff, sizeof(int32_t) * ((size_t)nblocks * nstage + 1), false));
+  RG_TRY(alloc((void **)&P->loc, sizeof(int16_t) * (size_t)loc_rows * n, false));
+  RG_TRY(alloc((void **)&P->thrcol, sizeof(int32_t) * n, false));
+  RG_TRY(alloc((void **)&P->nthrcol, sizeof(int32_t) * nblocks, false));
+  if (nblocks > 0 && nstage > 0) {
+    std::vector<RgStage> h_st(nstage);
+    int row = 0;
+    for (int q = 0; q < nstage; ++q) {
+      h_st[q].map = reinterpret_cast<const int32_t *>(stage_map[q]);
+      h_st[q].arity = stage_arity[q];
+      h_st[q].loc_row = row;
+      h_st[q].cap = (int64_t)part_size * stage_arity[q];
+      row += stage_arity[q];
+      RG_TRY(alloc((void **)&h_st[q].tmp, sizeof(int32_t) * (size_t)nblocks * h_st[q].cap, true));
+    }
+    RgStage *d_st = nullptr;
+    RG_TRY(alloc((void **)&d_st, sizeof(RgStage) * nstage, true));
+    RG_CUDA(cudaMemcpyAsync(d_st, h_st.data(), sizeof(RgStage) * nstage, cudaMemcpyHostToDevice, s));
+    int npow2 = 1;
+    while (npow2 < part_size * max_arity) npow2 <<= 1;
+    const int smem = 3 * npow2 * (int)sizeof(int);
+    RG_CUDA(cudaFuncSetAttribute(rg_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    rg_stage_kernel<<<dim3(nblocks, nstage), kRgThreads, smem, s>>>(d_st, nstage, n, P->order,
+                                                                      P->boff, npow2, P->tcnt, P->loc);
+    RG_CUDA(cudaGetLastError());
+    std::vector<int32_t> h_cnt((size_t)nblocks * nstage);
+    RG_CUDA(cudaMemcpyAsync(h_cnt.data(), P->tcnt, sizeof(int32_t) * h_cnt.size(),
+                            cudaMemcpyDeviceToHost, s));
+    RG_CUDA(cudaStreamSynchronize(s));
+    std::vector<int32_t> h_off(h_cnt.size() + 1);
+    int64_t tot = 0;
+    for (size_t i = 0; i < h_cnt.size(); ++i) {
+      h_off[i] = (int32_t)tot;
+      tot += h_cnt[i];
+      int q = (int)(i % nstage);
+      P->max_count[q] = std::max(P->max_count[q], h_cnt[i]);
+    }
+    if (tot > INT_MAX) return fail(set_error(OP2B_ERR_ARG, "region plan: %lld staged targets", (long long)tot));
+    h_off[h_cnt.size()] = (int32_t)tot;
+    P->tlist_len = tot;
+    RG_CUDA(cudaMemcpyAsync(P->toff, h_off.data(), sizeof(int32_t) * h_off.size(),
+                            cudaMemcpyHostToDevice, s));
+    RG_TRY(alloc((void **)&P->tlist, sizeof(int32_t) * (size_t)tot, false));
+    rg_compact_kernel<<<dim3(nblocks, nstage), kRgThreads, 0, s>>>(d_st, nstage, P->tcnt, P->toff,
+                                                                   P->tlist);
+    RG_CUDA(cudaGetLastError());
+    // thread colours over the INC staged Maps' block-local targets
+    int32_t *d_inc = nullptr;
+    RG_TRY(alloc((void **)&d_inc, sizeof(int32_t) * nstage, true));
+    RG_CUDA(cudaMemcpyAsync(d_inc, stage_inc, sizeof(int32_t) * nstage, cudaMemcpyHostToDevice, s));
+    int64_t mask_words = 0;
+    for (int q = 0; q < nstage; ++q)
+      if (stage_inc[q]) mask_words += P->max_count[q];
+    const int csmem = (int)sizeof(uint32_t) * (int)std::max<int64_t>(mask_words, 1);
+    RG_CUDA(cudaFuncSetAttribute(rg_color_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem));
+    rg_color_kernel<<<nblocks, 32, csmem, s>>>(d_st, d_inc, nstage, n, P->boff, P->tcnt, P->loc,
+                                               P->thrcol, P->nthrcol);
+    RG_CUDA(cudaGetLastError());
+    std::vector<int32_t> h_nc(nblocks);
+    RG_CUDA(cudaMemcpyAsync(h_nc.data(), P->nthrcol, sizeof(int32_t) * nblocks, cudaMemcpyDeviceToHost, s));
+    RG_CUDA(cudaStreamSynchronize(s));
+    for (int b = 0; b < nblocks; ++b) P->max_nthrcol = std::max(P->max_nthrcol, h_nc[b]);
+  } else {
+    RG_TRY(alloc((void **)&P->tlist, 16, false));
+    RG_CUDA(cudaMemsetAsync(P->toff, 0, sizeof(int32_t) * ((size_t)nblocks * nstage + 1), s));
+    RG_CUDA(cudaMemsetAsync(P->thrcol, 0, sizeof(int32_t) * std::max(n, 1), s));
+    RG_CUDA(cudaMemsetAsync(P->nthrcol, 0, sizeof(int32_t) * std::max(nblocks, 1), s));
+    if (nblocks > 0) P->max_nthrcol = 1;
+  }
+  RG_CUDA(cudaStreamSynchronize(s));
+  for (void *t : temps) dev_free(t, s);
+  temps.clear();
+#undef RG_TRY
+#undef RG_CUDA
+  *plan_out = reinterpret_cast<uint64_t>(P);
+  return OP2B_OK;
+}
+
+int op2b_region_plan_info(uint64_t plan, int32_t *nblocks, int32_t *nregions, int32_t *levels,
+                          int32_t *max_count, int64_t *tlist_len, int32_t *max_nthrcol) {
+  RegionPlan *P = reinterpret_cast<RegionPlan *>(plan);
+  if (!P) return set_error(OP2B_ERR_ARG, "null region plan");
+  if (max_nthrcol) *max_nthrcol = P->max_nthrcol;
+  if (nblocks) *nblocks = P->nblocks;
+  if (nregions) *nregions = P->nregions;
+  if (levels) *levels = P->levels;
+  if (max_count)
+    for (int q = 0; q < P->nstage; ++q) max_count[q] = P->max_count[q];
+  if (tlist_len) *tlist_len = P->tlist_len;
+  return OP2B_OK;
+}
+
+int op2b_region_plan_array(uint64_t plan, int32_t which, uint64_t *dptr, int64_t *count) {
+  RegionPlan *P = reinterpret_cast<RegionPlan *>(plan);
+  if (!P || !dptr) return set_error(OP2B_ERR_ARG, "null region plan");
+  const int64_t nbs = (int64_t)P->nblocks * P->nstage;
+  void *ptrs[] = {P->order, P->boff, P->tlist, P->toff, P->tcnt, P->loc, P->thrcol, P->nthrcol};
+  const int64_t counts[] = {P->set_size, P->nblocks + 1, P->tlist_len, nbs + 1, nbs,
+                            (int64_t)P->loc_rows * P->set_size, P->set_size, P->nblocks};
+  if (which < 0 || which > 7) return set_error(OP2B_ERR_ARG, "region plan array %d", which);
+  *dptr = reinterpret_cast<uint64_t>(ptrs[which]);
+  if (count) *count = counts[which];
+  return OP2B_OK;
+}
+
+int op2b_region_plan_free(uint64_t plan) {
+  OP2B_REQUIRE_INIT();
+  region_release(reinterpret_cast<RegionPlan *>(plan), stream_of(0));
+  return OP2B_OK;
+}
+
+}  // extern "C"

@@ -165,6 +165,74 @@ def test_atomic_mode_stubs(host_op2, golden_matrices):
         cfg.configure(inc_mode="atomic", owner_mode="auto")
 
 
+def test_staged_mode_stubs(host_op2, golden_matrices):
+    """The staged form (locality partition, shared-memory INC accumulation)
+    compiles for Dat INC through indexed, vec-map and iteration-space args;
+    Maps with equal values share one staged target list; loops without an
+    indirect INC or with Mats run in the atomic form instead."""
+    op2 = host_op2
+    from pyop2_b200 import b200, base
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import airfoil
+    el, nd, vnd = op2.Set(2), op2.Set(4), op2.Set(4, 2)
+    emap = np.asarray(golden_matrices["elem_node_map"], np.int32)
+    en = op2.Map(el, nd, 3, emap, "en_s")
+    evn = op2.Map(el, vnd, 3, emap, "evn_s")
+    coords, f = op2.Dat(vnd, np.zeros(8)), op2.Dat(nd, np.zeros(4))
+    b, bv = op2.Dat(nd, np.zeros(4)), op2.Dat(vnd, np.zeros(8))
+    mat = op2.Mat(op2.Sparsity((en, en)), np.float64)
+    K = {k: op2.Kernel(v["code"], v["name"]) for k, v in golden_matrices["kernels"].items()}
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    A = airfoil.build(op2, 6, 3, 0)
+    cfg.configure(inc_mode="staged", owner_mode="never", staged_min_size=0)
+    try:
+        cases = [(K["rhs"], el, b(en, op2.INC), coords(evn, op2.READ), f(en, op2.READ)),
+                 (K["rhs_ffc_itspace"], el(3), b(en[op2.i[0]], op2.INC), coords(evn, op2.READ),
+                  f(en, op2.READ)),
+                 (K["rhs_ffc_vector_itspace"], el(3), bv(evn[op2.i[0]], op2.INC), coords(evn, op2.READ),
+                  bv(evn, op2.READ)),
+                 (A.k_res, A.edges, A.p_x(A.pedge[0], op2.READ), A.p_x(A.pedge[1], op2.READ),
+                  A.p_q(A.pevcell[0], op2.READ), A.p_q(A.pevcell[1], op2.READ),
+                  A.p_adt(A.pecell[0], op2.READ), A.p_adt(A.pecell[1], op2.READ),
+                  A.p_res(A.pevcell[0], op2.INC), A.p_res(A.pevcell[1], op2.INC)),
+                 (A.k_bres, A.bedges, A.p_x(A.pbedge[0], op2.READ), A.p_x(A.pbedge[1], op2.READ),
+                  A.p_q(A.pbevcell[0], op2.READ), A.p_adt(A.pbecell[0], op2.READ),
+                  A.p_res(A.pbevcell[0], op2.INC), A.p_bound(op2.IdentityMap, op2.READ))]
+        for k, it, *args in cases:
+            spec = b200.loop_spec(b200.ParLoop(k, it, *args))["spec"]
+            assert spec.mode == "staged", k.name
+            src, layout, _ = nvrtc_compile(spec)
+            assert "rg_thrcol" in layout.fields and "op2b_atomic_add(p.d" in src
+            R = spec.region
+            # en and evn (one connectivity, two target DataSets) stage one list
+            assert len(R["stage_arity"]) == (2 if k is A.k_res or k is A.k_bres else 1), k.name
+        res = b200.loop_spec(b200.ParLoop(*cases[3]))["spec"]
+        cells = res.region["map_stage"][res.args[6].mslot]
+        nodes = res.region["map_stage"][res.args[0].mslot]
+        assert res.region["inc_pairs"] == [(res.args[6].slot, cells, "double", 4)]
+        assert res.region["inc_stages"] == [cells]
+        # x through pedge, q through pevcell, adt through pecell: staged READ rows
+        assert sorted(res.region["read_pairs"]) == sorted([(res.args[0].slot, nodes, "double", 2),
+                                                           (res.args[2].slot, cells, "double", 4),
+                                                           (res.args[4].slot, cells, "double", 1)])
+        # below staged_min_size: the atomic form
+        cfg.configure(staged_min_size=1 << 30)
+        assert b200.loop_spec(b200.ParLoop(*cases[3]))["spec"].mode == "atomic"
+        cfg.configure(staged_min_size=0)
+        # no indirect INC / a Mat: the atomic form
+        adt = b200.loop_spec(b200.ParLoop(A.k_adt, A.cells, *([A.p_x(A.pcell[k], op2.READ) for k in range(4)] +
+                             [A.p_q(op2.IdentityMap, op2.READ), A.p_adt(op2.IdentityMap, op2.WRITE)])))
+        assert adt["spec"].mode == "atomic"
+        m = b200.loop_spec(b200.ParLoop(K["mass"], el(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.INC),
+                                        coords(evn, op2.READ)))
+        assert m["spec"].mode == "atomic"
+    finally:
+        cfg.configure(inc_mode="atomic", owner_mode="never", staged_min_size=65536)
+        for c in A.consts:
+            c.remove_from_namespace()
+
+
 def test_owner_mode_stubs(host_op2, golden_matrices):
     """Owner-computes stubs: scalar Mat INC/WRITE, 1-d iteration-space Dat
     INC, indexed / vec-map Dat INC (owner_mode='always'), with and without

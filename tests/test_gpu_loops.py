@@ -20,6 +20,17 @@ def op2(backend):
     return _op2
 
 
+@pytest.fixture(params=["atomic", "color", "staged"])
+def indirect_mode(request):
+    """Indirect loops under each INC strategy: atomic adds, the coloured
+    plan, and the staged locality partition."""
+    from pyop2_b200 import configuration as cfg
+    old = (cfg.cfg['inc_mode'], cfg.cfg['staged_min_size'])
+    cfg.configure(inc_mode=request.param, staged_min_size=0)
+    yield request.param
+    cfg.configure(inc_mode=old[0], staged_min_size=old[1])
+
+
 # ----------------------------------------------------------- direct loops
 class TestDirectLoop:
     """test_direct_loop.py:79-213"""
@@ -171,6 +182,10 @@ class TestDirectLoop:
 # --------------------------------------------------------- indirect loops
 class TestIndirectLoop:
     """test_indirect_loop.py:70-145"""
+
+    @pytest.fixture(autouse=True)
+    def _mode(self, indirect_mode):
+        return indirect_mode
 
     @pytest.fixture
     def iterset(self, op2):
@@ -437,6 +452,10 @@ def vm(op2):
 class TestVectorMap:
     """test_vector_map.py:95-211"""
 
+    @pytest.fixture(autouse=True)
+    def _mode(self, indirect_mode):
+        return indirect_mode
+
     def test_sum_nodes_to_edges(self, op2):
         nedges = NNODES - 1
         nodes = op2.Set(NNODES, 1, "nodes")
@@ -505,6 +524,10 @@ class TestVectorMap:
 
 class TestIterationSpaceDats:
     """test_iteration_space_dats.py:95-211"""
+
+    @pytest.fixture(autouse=True)
+    def _mode(self, indirect_mode):
+        return indirect_mode
 
     def test_sum_nodes_to_edges(self, op2):
         nedges = NNODES - 1

@@ -32,14 +32,14 @@ def _clear_consts(op2mod):
     seq._CONSTS.clear()
 
 
-@pytest.fixture(params=["atomic", "color", "lma"])
+@pytest.fixture(params=["atomic", "color", "lma", "staged"])
 def inc_mode(request):
     """Run a test under both INC conflict strategies of indirect loops."""
     from pyop2_b200 import configuration as cfg
-    old = cfg.cfg['inc_mode']
-    cfg.configure(inc_mode=request.param)
+    old = (cfg.cfg['inc_mode'], cfg.cfg['staged_min_size'])
+    cfg.configure(inc_mode=request.param, staged_min_size=0)
     yield request.param
-    cfg.configure(inc_mode=old)
+    cfg.configure(inc_mode=old[0], staged_min_size=old[1])
 
 
 @pytest.mark.parametrize("nx,ny,seed", [(24, 12, 0), (60, 30, 1)])

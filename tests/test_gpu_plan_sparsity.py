@@ -211,3 +211,67 @@ def test_sparsity_empty_rows(op2):
     v = np.array([[0, 2], [2, 4]], np.int32)
     sp = _compare_sparsity(op2, 1, 1, [(v, v, 2, 2, 2)], 6, 6)
     assert list(sp._d_nnz) == [2, 0, 3, 0, 2, 0]
+
+
+# ------------------------------------------------- locality partition
+def _region_check(op2, n, grow, stages, part, rs, inc=None):
+    """Device locality partition (op2b_region_plan_build) equals the numpy
+    restatement (oracle/region.py) array for array; grow / stages are
+    (values [n][arity], target size); inc flags the staged Maps the thread
+    colours separate."""
+    from oracle import region
+    from pyop2_b200 import b200
+    it = op2.Set(n)
+    mk = {}
+
+    def dmap(vals, ntg):
+        key = id(vals)
+        if key not in mk:
+            mk[key] = op2.Map(it, op2.Set(ntg), vals.shape[1], vals)
+        return mk[key]
+    rp = b200.RegionPlan(n, part, rs, dmap(*grow), [dmap(v, t) for v, t in stages], inc)
+    want = region.region_plan(grow[0], grow[1], [v for v, _ in stages], part, rs, inc)
+    for name in ("order", "boff", "tlist", "toff", "tcnt", "thrcol", "nthrcol"):
+        np.testing.assert_array_equal(rp.host_array(name), want[name], err_msg=name)
+    np.testing.assert_array_equal(rp.host_array("loc"), want["loc"].ravel())
+    assert (rp.nregions, rp.levels) == (want["nregions"], want["levels"])
+    ns = len(stages)
+    nb = len(want["boff"]) - 1
+    assert rp.nblocks == nb
+    assert rp.max_count == [int(want["tcnt"][s::ns].max()) if nb else 0 for s in range(ns)]
+    # blocks respect part_size and cover the set once
+    assert (np.diff(want["boff"]) <= part).all()
+    np.testing.assert_array_equal(np.sort(want["order"]), np.arange(n))
+    return rp, want
+
+
+@pytest.mark.parametrize("nx,ny,seed,part,rs", [(60, 30, 0, 1024, 512), (40, 17, 3, 256, 64),
+                                                (7, 5, 1, 32, 1000)])
+def test_region_plan_airfoil_matches_oracle(op2, nx, ny, seed, part, rs):
+    from pyop2_b200.workloads import meshes
+    g = meshes.airfoil_grid(nx, ny, seed)
+    pecell = np.asarray(g.pecell, np.int32).reshape(-1, 2)
+    pedge = np.asarray(g.pedge, np.int32).reshape(-1, 2)
+    rp, want = _region_check(op2, g.nedges, (pecell, g.ncells),
+                             [(pecell, g.ncells), (pedge, g.nnodes)], part, rs, [True, False])
+    assert rp.max_nthrcol == want["nthrcol"].max()
+    if nx == 60:
+        # compact regions: far fewer distinct cells per block than elements
+        assert want["tcnt"][0::2].sum() < 0.7 * g.nedges
+
+
+def test_region_plan_p2_and_disconnected(op2):
+    from pyop2_b200.workloads import meshes
+    coords, elem = meshes.square_p2(12, seed=4)
+    elem = np.asarray(elem, np.int32)
+    _region_check(op2, elem.shape[0], (elem, coords.shape[0]), [(elem, coords.shape[0])], 2048, 100)
+    # arity 1 onto distinct targets: no element is adjacent to another, so
+    # all but the seeds fall into the consecutive leftover regions
+    n = 5000
+    perm = np.random.default_rng(0).permutation(n).astype(np.int32).reshape(n, 1)
+    _, want = _region_check(op2, n, (perm, n), [(perm, n)], 128, 64)
+    assert want["levels"] == 1
+    # empty set
+    e = np.zeros((0, 2), np.int32)
+    rp, _ = _region_check(op2, 0, (e, 4), [(e, 4)], 64, 64)
+    assert rp.nblocks == 0
