@@ -822,9 +822,7 @@ class RegionPlan(object):
 
 def region_plan(iterset, maps, region):
     """The cached locality partition of a staged loop."""
-    ps = int(cfg.cfg['partition_size']) or 384
-    amax = max(region["stage_arity"])
-    ps = max(1, min(ps, 16384 // amax))
+    ps = region["part_size"]
     rs = int(cfg.cfg['region_size']) or max(1, ps // 2)
     reps = [maps[k] for k in region["stage_maps"]]
     grow = reps[region["grow"]]
@@ -1168,9 +1166,13 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
     elif (indirect and (inc_mode or cfg.cfg['inc_mode']) == 'staged' and codegen.staged_capable(spec)
           and iterset.size >= int(cfg.cfg['staged_min_size'])):
         spec.mode = "staged"
-        spec.region = _region_layout(specs, maps)
+        spec.region = R = _region_layout(specs, maps)
         if block_size is None:
             spec.block_size = bs = int(cfg.cfg['staged_block_size'])
+        # blocks of at most part_size elements; the stub runs ept passes of bs
+        ps = int(cfg.cfg['partition_size']) or 384
+        R["part_size"] = ps = max(1, min(ps, 16384 // max(R["stage_arity"])))
+        R["ept"] = (ps + bs - 1) // bs
         indirect = False   # one launch over the locality partition's blocks
     elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'lma' and codegen.lma_capable(spec):
         spec.mode = "lma"

@@ -598,6 +598,22 @@ def _staged_body(spec):
     for st in used:
         L.append("  const int n_s%d = p.rg_tcnt[blk * %d + %d];" % (st, ns, st))
         L.append("  const int *tl_s%d = p.rg_tlist + p.rg_toff[blk * %d + %d];" % (st, ns, st))
+    # every element of this thread (ept passes of bs): its loc rows, colour
+    # and element id are loaded now, while the staged rows are in flight
+    ept = R["ept"]
+    for j in range(ept):
+        L.append("  const int idx_%d = %d + threadIdx.x;" % (j, j * bs))
+        L.append("  const bool active_%d = idx_%d < nelem;" % (j, j))
+        L.append("  const op2b_i64 pos_%d = start + (active_%d ? idx_%d : 0);" % (j, j, j))
+        for st in used:
+            ar = R["stage_arity"][st]
+            L.append("  int sl%d_%d[%d];" % (st, j, ar))
+            L.append("  #pragma unroll")
+            L.append("  for (int r = 0; r < %d; ++r) sl%d_%d[r] = active_%d ? (int)p.rg_loc[(op2b_i64)(%d + r) * "
+                     "set_size + pos_%d] : 0;" % (ar, st, j, j, R["row_base"][st], j))
+        L.append("  const int col_%d = active_%d ? p.rg_thrcol[pos_%d] : -1;" % (j, j, j))
+        if any(a.kind == "direct" for a in spec.args):
+            L.append("  const op2b_i64 e_%d = active_%d ? p.rg_order[pos_%d] : 0;" % (j, j, j))
     for q, (slot, st, t, c) in enumerate(R["read_pairs"]):
         L.append("  %s *rd%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
         L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
@@ -627,19 +643,8 @@ def _staged_body(spec):
     L.append("  __syncthreads();")
     _gbl_prologue(spec, L)
     L.append("  const int ncol = p.rg_nthrcol[blk];")
-    L.append("  for (int base = 0; base < nelem; base += %d) {" % bs)
-    L.append("    const int idx = base + threadIdx.x;")
-    L.append("    const bool active = idx < nelem;")
-    L.append("    const op2b_i64 pos = start + (active ? idx : 0);")
     ind = "    "
-    if any(a.kind == "direct" for a in spec.args):
-        L.append("%sconst op2b_i64 e = p.rg_order[pos];" % ind)
-    for st in used:
-        ar = R["stage_arity"][st]
-        L.append("%sint sl%d[%d];" % (ind, st, ar))
-        L.append("%s#pragma unroll" % ind)
-        L.append("%sfor (int r = 0; r < %d; ++r) sl%d[r] = active ? (int)p.rg_loc[(op2b_i64)(%d + r) * "
-                 "set_size + pos] : 0;" % (ind, ar, st, R["row_base"][st]))
+    has_direct = any(a.kind == "direct" for a in spec.args)
     decl, pre, post, exprs, adds = [], [], [], [], []
     for n, a in enumerate(spec.args):
         t, c = a.ctype, a.cdim
@@ -699,25 +704,32 @@ def _staged_body(spec):
                 exprs.append("a%d_v" % n)
             else:
                 exprs.append(row_ptr("i%d" % a.idx))
-    L += decl
-    L.append("%sint col = -1;" % ind)
-    L.append("%sif (active) {" % ind)
-    L += pre
-    L += _itspace_open(spec, ind + "  ")
-    L.append(_kernel_call(spec, exprs, ind + "  " + "  " * len(spec.extents)))
-    L += _itspace_close(spec, ind + "  ")
-    L += post
-    L.append("%s  col = p.rg_thrcol[pos];" % ind)
-    L.append("%s}" % ind)
-    L.append("%sfor (int c = 0; c < ncol; ++c) {" % ind)
-    L.append("%s  if (col == c) {" % ind)
-    for var, lrow, q, c in adds:
-        L.append("%s    { %s *dst = acc%d + %s * %d;" % (ind, R["inc_pairs"][q][2], q, lrow, c))
-        L.append("%s      for (int k = 0; k < %d; ++k) dst[k] += %s[k]; }" % (ind, c, var))
-    L.append("%s  }" % ind)
-    L.append("%s  __syncthreads();" % ind)
-    L.append("%s}" % ind)
-    L.append("  }")
+    for j in range(ept):
+        L.append("  if (%d < nelem) {" % (j * bs))
+        L.append("%sconst bool active = active_%d;" % (ind, j))
+        if has_direct:
+            L.append("%sconst op2b_i64 e = e_%d;" % (ind, j))
+        for st in used:
+            ar = R["stage_arity"][st]
+            L.append("%sconst int sl%d[%d] = {%s};" % (ind, st, ar, ", ".join(
+                "sl%d_%d[%d]" % (st, j, r) for r in range(ar))))
+        L += decl
+        L.append("%sif (active) {" % ind)
+        L += pre
+        L += _itspace_open(spec, ind + "  ")
+        L.append(_kernel_call(spec, exprs, ind + "  " + "  " * len(spec.extents)))
+        L += _itspace_close(spec, ind + "  ")
+        L += post
+        L.append("%s}" % ind)
+        L.append("%sfor (int c = 0; c < ncol; ++c) {" % ind)
+        L.append("%s  if (col_%d == c) {" % (ind, j))
+        for var, lrow, q, c in adds:
+            L.append("%s    { %s *dst = acc%d + %s * %d;" % (ind, R["inc_pairs"][q][2], q, lrow, c))
+            L.append("%s      for (int k = 0; k < %d; ++k) dst[k] += %s[k]; }" % (ind, c, var))
+        L.append("%s  }" % ind)
+        L.append("%s  __syncthreads();" % ind)
+        L.append("%s}" % ind)
+        L.append("  }")
     for q, (slot, st, ctype, cdim) in enumerate(R["inc_pairs"]):
         L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (st, cdim, bs))
         L.append("    const int r = t / %d, k = t - r * %d;" % (cdim, cdim))
