@@ -568,9 +568,13 @@ class Sparsity(base.Sparsity):
         return self._colidx
 
     def __del__(self):
-        h = getattr(self, "_handle", 0)
-        if h and _state['init'] and _lib._lib is not None:
-            _lib._lib.op2b_sparsity_free(h)
+        # at interpreter exit the module globals may already be gone
+        try:
+            h = getattr(self, "_handle", 0)
+            if h and _state['init'] and _lib._lib is not None:
+                _lib._lib.op2b_sparsity_free(h)
+        except Exception:
+            pass
 
 
 class Mat(DeviceDataMixin, base.Mat):
@@ -761,9 +765,13 @@ class DevicePlan(object):
         raise AttributeError(name)
 
     def __del__(self):
-        h = getattr(self, "_handle", 0)
-        if h and _state['init'] and _lib._lib is not None:
-            _lib._lib.op2b_plan_free(h)
+        # at interpreter exit the module globals may already be gone
+        try:
+            h = getattr(self, "_handle", 0)
+            if h and _state['init'] and _lib._lib is not None:
+                _lib._lib.op2b_plan_free(h)
+        except Exception:
+            pass
 
 
 _REGION_ARRAYS = ("order", "boff", "tlist", "toff", "tcnt", "loc", "thrcol", "nthrcol")
@@ -796,6 +804,7 @@ class RegionPlan(object):
         self.max_nthrcol = mt.value
         self.max_count = list(mc)[:ns]
         self.set_size, self.part_size, self.nstage = set_size, part_size, ns
+        self.region_size, self.stage_inc = region_size, stage_inc
         self._keep = [grow_map] + list(stage_maps)
         self.dptr, self.counts = {}, {}
         for k, name in enumerate(_REGION_ARRAYS):
@@ -815,9 +824,13 @@ class RegionPlan(object):
         raise AttributeError(name)
 
     def __del__(self):
-        h = getattr(self, "_handle", 0)
-        if h and _state['init'] and _lib._lib is not None:
-            _lib._lib.op2b_region_plan_free(h)
+        # at interpreter exit the module globals may already be gone
+        try:
+            h = getattr(self, "_handle", 0)
+            if h and _state['init'] and _lib._lib is not None:
+                _lib._lib.op2b_region_plan_free(h)
+        except Exception:
+            pass
 
 
 def region_plan(iterset, maps, region):

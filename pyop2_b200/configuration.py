@@ -72,9 +72,9 @@ _defaults = {
     'device': 0,
     'l2_fetch_granularity': 32,
     'min_blocks_per_sm': 0,
-    'inc_mode': 'atomic',
+    'inc_mode': 'staged',
     'region_size': 0,
-    'staged_min_size': 65536,
+    'staged_min_size': 262144,
     'staged_block_size': 128,
     'owner_mode': 'never',
     'kahan': False,

@@ -207,12 +207,15 @@ __global__ void rg_stage_kernel(const RgStage *__restrict__ stages, int nstage, 
 
 // One CTA per block: greedy thread colouring in position order over the
 // block-local targets of the INC staged Maps (masks of 32 colours per round,
-// as pyop2/plan.pyx:282-324); run by one thread, the masks in shared memory.
+// as pyop2/plan.pyx:282-324).  The CTA first gathers every element's INC
+// targets (block-local numbers, offset per staged Map) into shared memory;
+// one thread then colours from there.
 __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_t *__restrict__ inc,
-                                int nstage, int set_size, const int32_t *__restrict__ boff,
-                                const int32_t *__restrict__ tcnt, const int16_t *__restrict__ loc,
-                                int32_t *__restrict__ thrcol, int32_t *__restrict__ nthrcol) {
-  extern __shared__ uint32_t rg_masks[];
+                                int nstage, int set_size, int inc_rows, int part_size,
+                                const int32_t *__restrict__ boff, const int32_t *__restrict__ tcnt,
+                                const int16_t *__restrict__ loc, int32_t *__restrict__ thrcol,
+                                int32_t *__restrict__ nthrcol) {
+  extern __shared__ uint32_t rg_masks[];      // [mask words][part_size * inc_rows] targets
   const int blk = blockIdx.x;
   const int start = boff[blk], nelem = boff[blk + 1] - start;
   // local target numbering: the INC staged Maps' lists one after the other
@@ -228,7 +231,16 @@ __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_
   }
   __syncthreads();
   const int total = s_total;
-  for (int i = threadIdx.x; i < nelem; i += blockDim.x) thrcol[start + i] = -1;
+  int *tgt = reinterpret_cast<int *>(rg_masks + total);   // [nelem][inc_rows]
+  int row = 0;
+  for (int q = 0; q < nstage; ++q) {
+    if (!inc[q]) continue;
+    for (int r = 0; r < stages[q].arity; ++r, ++row)
+      for (int i = threadIdx.x; i < nelem; i += blockDim.x)
+        tgt[i * inc_rows + row] = s_base[q] + loc[(int64_t)(stages[q].loc_row + r) * set_size + start + i];
+  }
+  int *col = tgt + part_size * inc_rows;                   // [nelem]
+  for (int i = threadIdx.x; i < nelem; i += blockDim.x) col[i] = -1;
   __syncthreads();
   if (threadIdx.x == 0) {
     int base = 0, remaining = nelem, ncol = 0;
@@ -236,30 +248,24 @@ __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_
       for (int i = 0; i < total; ++i) rg_masks[i] = 0u;
       remaining = 0;
       for (int i = 0; i < nelem; ++i) {
-        if (thrcol[start + i] >= 0) continue;
+        if (col[i] >= 0) continue;
         uint32_t m = 0u;
-        for (int q = 0; q < nstage; ++q) {
-          if (!inc[q]) continue;
-          for (int r = 0; r < stages[q].arity; ++r)
-            m |= rg_masks[s_base[q] + loc[(int64_t)(stages[q].loc_row + r) * set_size + start + i]];
-        }
+        for (int k = 0; k < inc_rows; ++k) m |= rg_masks[tgt[i * inc_rows + k]];
         if (m == 0xffffffffu) {
           ++remaining;
           continue;
         }
         const int c = __ffs(~m) - 1;
-        thrcol[start + i] = base + c;
+        col[i] = base + c;
         ncol = max(ncol, base + c + 1);
-        for (int q = 0; q < nstage; ++q) {
-          if (!inc[q]) continue;
-          for (int r = 0; r < stages[q].arity; ++r)
-            rg_masks[s_base[q] + loc[(int64_t)(stages[q].loc_row + r) * set_size + start + i]] |= 1u << c;
-        }
+        for (int k = 0; k < inc_rows; ++k) rg_masks[tgt[i * inc_rows + k]] |= 1u << c;
       }
       base += 32;
     }
     nthrcol[blk] = ncol;
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nelem; i += blockDim.x) thrcol[start + i] = col[i];
 }
 
 __global__ void rg_compact_kernel(const RgStage *__restrict__ stages, int nstage,
@@ -480,12 +486,20 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
     RG_TRY(alloc((void **)&d_inc, sizeof(int32_t) * nstage, true));
     RG_CUDA(cudaMemcpyAsync(d_inc, stage_inc, sizeof(int32_t) * nstage, cudaMemcpyHostToDevice, s));
     int64_t mask_words = 0;
+    int inc_rows = 0;
     for (int q = 0; q < nstage; ++q)
-      if (stage_inc[q]) mask_words += P->max_count[q];
-    const int csmem = (int)sizeof(uint32_t) * (int)std::max<int64_t>(mask_words, 1);
+      if (stage_inc[q]) {
+        mask_words += P->max_count[q];
+        inc_rows += stage_arity[q];
+      }
+    const int64_t cwords = mask_words + (int64_t)part_size * inc_rows + part_size;
+    if (cwords * 4 > smem_optin())
+      return fail(set_error(OP2B_ERR_ARG, "region plan: colouring needs %lld bytes of shared memory",
+                            (long long)(cwords * 4)));
+    const int csmem = (int)sizeof(uint32_t) * (int)std::max<int64_t>(cwords, 1);
     RG_CUDA(cudaFuncSetAttribute(rg_color_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem));
-    rg_color_kernel<<<nblocks, 32, csmem, s>>>(d_st, d_inc, nstage, n, P->boff, P->tcnt, P->loc,
-                                               P->thrcol, P->nthrcol);
+    rg_color_kernel<<<nblocks, 128, csmem, s>>>(d_st, d_inc, nstage, n, inc_rows, part_size, P->boff,
+                                                P->tcnt, P->loc, P->thrcol, P->nthrcol);
     RG_CUDA(cudaGetLastError());
     std::vector<int32_t> h_nc(nblocks);
     RG_CUDA(cudaMemcpyAsync(h_nc.data(), P->nthrcol, sizeof(int32_t) * nblocks, cudaMemcpyDeviceToHost, s));
