@@ -724,8 +724,14 @@ def _staged_body(spec):
         L.append("%sfor (int c = 0; c < ncol; ++c) {" % ind)
         L.append("%s  if (col_%d == c) {" % (ind, j))
         for var, lrow, q, c in adds:
-            L.append("%s    { %s *dst = acc%d + %s * %d;" % (ind, R["inc_pairs"][q][2], q, lrow, c))
-            L.append("%s      for (int k = 0; k < %d; ++k) dst[k] += %s[k]; }" % (ind, c, var))
+            # read-modify-write of the accumulated row with vector accesses
+            # (the rows are 16-byte aligned when their size allows)
+            t = R["inc_pairs"][q][2]
+            L.append("%s    { %s *dst = acc%d + %s * %d;" % (ind, t, q, lrow, c))
+            L.append("%s      __align__(16) %s cur[%d]; op2b_load<%s, %d, false>(cur, dst);"
+                     % (ind, t, c, t, c))
+            L.append("%s      for (int k = 0; k < %d; ++k) cur[k] += %s[k];" % (ind, c, var))
+            L.append("%s      op2b_store(dst, cur); }" % ind)
         L.append("%s  }" % ind)
         L.append("%s  __syncthreads();" % ind)
         L.append("%s}" % ind)
