@@ -25,7 +25,8 @@ these bit for bit:
   in order), and each (position, row)'s number;
 * thread colours: per block, elements in position order take the lowest
   colour (of 32 per round) that no earlier element sharing one of its INC
-  staged targets holds (pyop2/plan.pyx:282-324).
+  staged targets holds (pyop2/plan.pyx:282-324); then the block's positions
+  are sorted by colour (stable): order, loc and thrcol follow.
 """
 
 import numpy as np
@@ -159,8 +160,12 @@ def region_plan(grow_values, ntargets, stage_values, part_size, region_size, sta
         el = order[boff[b]:boff[b + 1]]
         targets = [[(s, int(t)) for s, v in enumerate(stage_values) if inc[s] for t in v[i]]
                    for i in el]
-        col = _thread_colors(targets)
-        thrcol[boff[b]:boff[b + 1]] = col
-        nthrcol[b] = max(col) + 1 if col else 0
+        col = np.asarray(_thread_colors(targets), dtype=np.int32)
+        perm = np.argsort(col, kind="stable")
+        seg = slice(boff[b], boff[b + 1])
+        thrcol[seg] = col[perm]
+        order[seg] = order[seg][perm]
+        loc[:, seg] = loc[:, seg][:, perm]
+        nthrcol[b] = col.max() + 1 if col.size else 0
     return dict(order=order, boff=boff, tlist=tlist, toff=toff, tcnt=tcnt, loc=loc,
                 thrcol=thrcol, nthrcol=nthrcol, nregions=nregions, levels=levels + 1)

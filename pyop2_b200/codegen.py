@@ -612,6 +612,11 @@ def _staged_body(spec):
             L.append("  for (int r = 0; r < %d; ++r) sl%d_%d[r] = active_%d ? (int)p.rg_loc[(op2b_i64)(%d + r) * "
                      "set_size + pos_%d] : 0;" % (ar, st, j, j, R["row_base"][st], j))
         L.append("  const int col_%d = active_%d ? p.rg_thrcol[pos_%d] : -1;" % (j, j, j))
+        # positions are sorted by colour within the block: the pass's colours
+        # run from its first position's to its last position's
+        L.append("  const int clo_%d = %d < nelem ? p.rg_thrcol[start + %d] : 0;" % (j, j * bs, j * bs))
+        L.append("  const int chi_%d = %d < nelem ? p.rg_thrcol[start + min(nelem, %d) - 1] : -1;"
+                 % (j, j * bs, (j + 1) * bs))
         if any(a.kind == "direct" for a in spec.args):
             L.append("  const op2b_i64 e_%d = active_%d ? p.rg_order[pos_%d] : 0;" % (j, j, j))
     for q, (slot, st, t, c) in enumerate(R["read_pairs"]):
@@ -642,7 +647,6 @@ def _staged_body(spec):
         L.append("  op2b_cp_async_wait();")
     L.append("  __syncthreads();")
     _gbl_prologue(spec, L)
-    L.append("  const int ncol = p.rg_nthrcol[blk];")
     ind = "    "
     has_direct = any(a.kind == "direct" for a in spec.args)
     decl, pre, post, exprs, adds = [], [], [], [], []
@@ -721,7 +725,7 @@ def _staged_body(spec):
         L += _itspace_close(spec, ind + "  ")
         L += post
         L.append("%s}" % ind)
-        L.append("%sfor (int c = 0; c < ncol; ++c) {" % ind)
+        L.append("%sfor (int c = clo_%d; c <= chi_%d; ++c) {" % (ind, j, j))
         L.append("%s  if (col_%d == c) {" % (ind, j))
         for var, lrow, q, c in adds:
             # read-modify-write of the accumulated row with vector accesses

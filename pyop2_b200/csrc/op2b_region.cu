@@ -22,7 +22,8 @@
 //    (pyop2/plan.pyx:282-324: elements in order, 32-colour masks per round)
 //    over the targets of the staged Maps marked as INC targets, so elements
 //    of one colour never add to the same staged row (thrcol per position,
-//    nthrcol per block).
+//    nthrcol per block); then the block's positions are sorted by colour
+//    (stable), so a run of consecutive positions spans few colours.
 // A staged stub (see codegen) walks block b over positions
 // boff[b] .. boff[b+1], element order[pos], and finds row r of staged Map s
 // at tlist[toff[b][s] + loc[row_base(s) + r][pos]].
@@ -214,8 +215,9 @@ __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_
                                 int nstage, int set_size, int inc_rows, int part_size,
                                 const int32_t *__restrict__ boff, const int32_t *__restrict__ tcnt,
                                 const int16_t *__restrict__ loc, int32_t *__restrict__ thrcol,
-                                int32_t *__restrict__ nthrcol) {
-  extern __shared__ uint32_t rg_masks[];      // [mask words][part_size * inc_rows] targets
+                                int32_t *__restrict__ nthrcol, int32_t *__restrict__ newpos) {
+  extern __shared__ uint32_t rg_masks[];  // [mask words][part_size*inc_rows targets][part_size
+                                          //  colours][part_size+1 counts][part_size ranks]
   const int blk = blockIdx.x;
   const int start = boff[blk], nelem = boff[blk + 1] - start;
   // local target numbering: the INC staged Maps' lists one after the other
@@ -263,9 +265,31 @@ __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_
       base += 32;
     }
     nthrcol[blk] = ncol;
+    // stable counting sort of the positions by colour
+    int *cnt = col + part_size;
+    int *rank = cnt + part_size + 1;
+    for (int c = 0; c <= ncol; ++c) cnt[c] = 0;
+    for (int i = 0; i < nelem; ++i) ++cnt[col[i] + 1];
+    for (int c = 0; c < ncol; ++c) cnt[c + 1] += cnt[c];
+    for (int i = 0; i < nelem; ++i) rank[i] = cnt[col[i]]++;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < nelem; i += blockDim.x) thrcol[start + i] = col[i];
+  const int *rank = col + 2 * part_size + 1;
+  for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
+    thrcol[start + rank[i]] = col[i];
+    newpos[start + i] = start + rank[i];
+  }
+}
+
+// Move every position's element id and loc rows to its colour-sorted place.
+__global__ void rg_permute_kernel(int n, int loc_rows, const int32_t *__restrict__ newpos,
+                                  const int32_t *__restrict__ order, const int16_t *__restrict__ loc,
+                                  int32_t *__restrict__ order2, int16_t *__restrict__ loc2) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int q = newpos[p];
+    order2[q] = order[p];
+    for (int r = 0; r < loc_rows; ++r) loc2[(int64_t)r * n + q] = loc[(int64_t)r * n + p];
+  }
 }
 
 __global__ void rg_compact_kernel(const RgStage *__restrict__ stages, int nstage,
@@ -492,15 +516,29 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
         mask_words += P->max_count[q];
         inc_rows += stage_arity[q];
       }
-    const int64_t cwords = mask_words + (int64_t)part_size * inc_rows + part_size;
+    const int64_t cwords = mask_words + (int64_t)part_size * inc_rows + 3LL * part_size + 1;
     if (cwords * 4 > smem_optin())
       return fail(set_error(OP2B_ERR_ARG, "region plan: colouring needs %lld bytes of shared memory",
                             (long long)(cwords * 4)));
     const int csmem = (int)sizeof(uint32_t) * (int)std::max<int64_t>(cwords, 1);
     RG_CUDA(cudaFuncSetAttribute(rg_color_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem));
+    int32_t *newpos = nullptr, *order2 = nullptr;
+    int16_t *loc2 = nullptr;
+    RG_TRY(alloc((void **)&newpos, sizeof(int32_t) * n, true));
+    RG_TRY(alloc((void **)&order2, sizeof(int32_t) * n, true));
+    RG_TRY(alloc((void **)&loc2, sizeof(int16_t) * (size_t)loc_rows * n, true));
     rg_color_kernel<<<nblocks, 128, csmem, s>>>(d_st, d_inc, nstage, n, inc_rows, part_size, P->boff,
-                                                P->tcnt, P->loc, P->thrcol, P->nthrcol);
+                                                P->tcnt, P->loc, P->thrcol, P->nthrcol, newpos);
     RG_CUDA(cudaGetLastError());
+    rg_permute_kernel<<<grid, kRgThreads, 0, s>>>(n, loc_rows, newpos, P->order, P->loc, order2, loc2);
+    RG_CUDA(cudaGetLastError());
+    // the permuted arrays replace the originals, which become temporaries
+    temps.erase(std::remove(temps.begin(), temps.end(), (void *)order2), temps.end());
+    temps.erase(std::remove(temps.begin(), temps.end(), (void *)loc2), temps.end());
+    temps.push_back(P->order);
+    temps.push_back(P->loc);
+    P->order = order2;
+    P->loc = loc2;
     std::vector<int32_t> h_nc(nblocks);
     RG_CUDA(cudaMemcpyAsync(h_nc.data(), P->nthrcol, sizeof(int32_t) * nblocks, cudaMemcpyDeviceToHost, s));
     RG_CUDA(cudaStreamSynchronize(s));
