@@ -148,6 +148,20 @@ class Arg(object):
         return self._is_mat or isinstance(self.idx, IterationIndex)
 
 
+# ------------------------------------------------------------------- HDF5
+def _h5_value(slot):
+    """The whole content of an HDF5 dataset as a numpy array: ``slot[()]``
+    (h5py 2.1 and later), else the ``value`` property the reference uses."""
+    try:
+        return np.asarray(slot[()])
+    except (TypeError, KeyError, IndexError, ValueError):
+        return np.asarray(slot.value)
+
+
+def _h5_str(v):
+    return v.decode() if isinstance(v, bytes) else str(v)
+
+
 # ------------------------------------------------------------------------ Set
 class Set(object):
     """OP2 set.  ``size`` is an int or the four sizes core/owned/exec/total."""
@@ -179,6 +193,23 @@ class Set(object):
 
     def __call__(self, *dims):
         return IterationSpace(self, dims)
+
+    @classmethod
+    def fromhdf5(cls, f, name, dim=1):
+        """Construct a Set from the one-element dataset ``name`` of the HDF5
+        file ``f`` (an h5py File or an object with its interface); its
+        ``dim`` attribute, if present, overrides ``dim``
+        (pyop2/base.py:386-394)."""
+        slot = f[name]
+        if tuple(slot.shape) != (1,):
+            raise SizeTypeError("Shape of %s is incorrect" % name)
+        size = _h5_value(slot).astype(int)
+        dim = slot.attrs.get('dim', dim)
+        if isinstance(dim, np.ndarray):
+            dim = tuple(int(d) for d in dim.ravel()) if dim.size > 1 else int(dim.ravel()[0])
+        elif isinstance(dim, np.integer):
+            dim = int(dim)
+        return cls(int(size[0]), dim, name)
 
     @property
     def core_size(self):
@@ -358,6 +389,16 @@ class Dat(DataCarrier):
             self._id = uid
         self._name = name or "dat_%d" % self._id
 
+    @classmethod
+    def fromhdf5(cls, dataset, f, name):
+        """Construct a Dat on ``dataset`` from the dataset ``name`` of the
+        HDF5 file ``f``; a ``type`` attribute ending in ``:soa`` makes it an
+        SoA Dat (pyop2/base.py:842-849)."""
+        slot = f[name]
+        data = _h5_value(slot)
+        soa = _h5_str(slot.attrs['type']).find(':soa') > 0
+        return cls(dataset, data, name=name, soa=soa)
+
     @validate_in(('access', _modes, ModeValueError))
     def __call__(self, path, access):
         if isinstance(path, Map):
@@ -499,6 +540,17 @@ class Const(DataCarrier):
         Const._globalcount += 1
         Const._generation += 1
 
+    @classmethod
+    def fromhdf5(cls, f, name):
+        """Construct a Const from the dataset ``name`` of the HDF5 file
+        ``f``; its shape is the Const's dim (pyop2/base.py:918-926)."""
+        slot = f[name]
+        dim = tuple(slot.shape)
+        data = _h5_value(slot)
+        if len(dim) < 1:
+            raise DimTypeError("Invalid dimension value %s" % (dim,))
+        return cls(dim, data, name)
+
     @property
     def data(self):
         if len(self._data) == 0:
@@ -616,6 +668,18 @@ class Map(object):
                                       allow_none=True)
         self._name = name or "map_%d" % Map._globalcount
         Map._globalcount += 1
+
+    @classmethod
+    def fromhdf5(cls, iterset, dataset, f, name):
+        """Construct a Map from ``iterset`` to ``dataset`` from the
+        two-dimensional dataset ``name`` of the HDF5 file ``f`` (its second
+        extent is the arity; pyop2/base.py:1117-1125)."""
+        slot = f[name]
+        values = _h5_value(slot)
+        dim = tuple(slot.shape)[1:]
+        if len(dim) != 1:
+            raise DimTypeError("Unrecognised dimension value %s" % (dim,))
+        return cls(iterset, dataset, dim[0], values, name)
 
     @validate_type(('index', (int, np.integer, IterationIndex), IndexTypeError))
     def __getitem__(self, index):

@@ -169,6 +169,69 @@ def build(op2, nx, ny, seed=0, grid=None, consts=True, q0=None, qold0=None, zero
     return A
 
 
+MACH, ALPHA = 0.4, 0.0
+
+
+def hdf5_layout(g, q0=None, seed=0):
+    """The datasets of an OP2 airfoil mesh file (the names, shapes and
+    attributes pyop2/demo/airfoil.py:45-75 reads from ``new_grid.h5``) for
+    the grid ``g``: name -> (array, attributes).  Written to a file with
+    h5py's ``create_dataset`` (one dataset per entry, attributes set from the
+    dict), it is a mesh file the demo's reader accepts."""
+    q = initial_q(g.ncells, seed) if q0 is None else np.asarray(q0, dtype=np.float64)
+    dbl, i32 = {"type": "double"}, {"type": "int"}
+    one = lambda v: np.array([v])
+    return {
+        "nodes": (one(g.nnodes), {}), "edges": (one(g.nedges), {}),
+        "bedges": (one(g.nbedges), {}), "cells": (one(g.ncells), {}),
+        "pedge": (np.asarray(g.pedge, np.int32).reshape(-1, 2), {}),
+        "pecell": (np.asarray(g.pecell, np.int32).reshape(-1, 2), {}),
+        "pbedge": (np.asarray(g.pbedge, np.int32).reshape(-1, 2), {}),
+        "pbecell": (np.asarray(g.pbecell, np.int32).reshape(-1, 1), {}),
+        "pcell": (np.asarray(g.pcell, np.int32).reshape(-1, 4), {}),
+        "p_bound": (np.asarray(g.p_bound, np.int32).reshape(-1, 1), i32),
+        "p_x": (np.asarray(g.x, np.float64).reshape(-1, 2), dbl),
+        "p_q": (q.reshape(-1, 4), dbl), "p_qold": (q.reshape(-1, 4).copy(), dbl),
+        "p_adt": (np.zeros((g.ncells, 1)), dbl), "p_res": (np.zeros((g.ncells, 4)), dbl),
+        "gam": (one(GAM), {}), "gm1": (one(GM1), {}), "cfl": (one(CFL), {}),
+        "eps": (one(EPS), {}), "mach": (one(MACH), {}), "alpha": (one(ALPHA), {}),
+        "qinf": (freestream(), {}),
+    }
+
+
+def build_from_hdf5(op2, f):
+    """Declare the airfoil problem from an OP2 airfoil mesh file ``f`` (an
+    h5py File, or any object with its interface), with the declarations of
+    pyop2/demo/airfoil.py:45-75: Sets, Maps and Dats through ``fromhdf5``."""
+    A = Airfoil()
+    A.grid = None
+    A.vnodes = A.nodes = op2.Set.fromhdf5(f, "nodes", dim=2)
+    A.edges = op2.Set.fromhdf5(f, "edges")
+    A.bedges = op2.Set.fromhdf5(f, "bedges")
+    A.cells = op2.Set.fromhdf5(f, "cells")
+    A.vcells = op2.Set.fromhdf5(f, "cells", dim=4)
+    A.pedge = op2.Map.fromhdf5(A.edges, A.vnodes, f, "pedge")
+    A.pecell = op2.Map.fromhdf5(A.edges, A.cells, f, "pecell")
+    A.pevcell = op2.Map.fromhdf5(A.edges, A.vcells, f, "pecell")
+    A.pbedge = op2.Map.fromhdf5(A.bedges, A.vnodes, f, "pbedge")
+    A.pbecell = op2.Map.fromhdf5(A.bedges, A.cells, f, "pbecell")
+    A.pbevcell = op2.Map.fromhdf5(A.bedges, A.vcells, f, "pbecell")
+    A.pcell = op2.Map.fromhdf5(A.cells, A.vnodes, f, "pcell")
+    A.p_bound = op2.Dat.fromhdf5(A.bedges, f, "p_bound")
+    A.p_x = op2.Dat.fromhdf5(A.vnodes, f, "p_x")
+    A.p_q = op2.Dat.fromhdf5(A.vcells, f, "p_q")
+    A.p_qold = op2.Dat.fromhdf5(A.vcells, f, "p_qold")
+    A.p_adt = op2.Dat.fromhdf5(A.cells, f, "p_adt")
+    A.p_res = op2.Dat.fromhdf5(A.vcells, f, "p_res")
+    A.consts = [op2.Const.fromhdf5(f, n) for n in ("gam", "gm1", "cfl", "eps", "mach", "alpha", "qinf")]
+    A.k_save = op2.Kernel(SAVE_SOLN, "save_soln")
+    A.k_adt = op2.Kernel(ADT_CALC, "adt_calc")
+    A.k_res = op2.Kernel(RES_CALC, "res_calc")
+    A.k_bres = op2.Kernel(BRES_CALC, "bres_calc")
+    A.k_update = op2.Kernel(UPDATE, "update")
+    return A
+
+
 def save_soln(op2, A):
     op2.par_loop(A.k_save, A.cells, A.p_q(op2.IdentityMap, op2.READ),
                  A.p_qold(op2.IdentityMap, op2.WRITE))

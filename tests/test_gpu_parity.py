@@ -228,6 +228,49 @@ def test_p1_mass_regression_golden(op2):
     assert abs(gb.data_ro.sum() - float(z["b_sum"])) < 1e-12
 
 
+def test_p1_mass_regression_golden_via_triangle_files(op2, tmp_path):
+    """The same regression problem read through the Triangle reader
+    (pyop2/demo/mass2d_triangle.py reads its mesh with
+    demo/triangle_reader.py): mesh written as .node/.ele, read back into op2
+    objects, assembled, compared with the golden's invariants."""
+    import os
+    from pyop2_b200 import triangle_reader
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "mass2d_triangle_summary.npz"))
+    coords, elem = meshes.square_p1(100)
+    prefix = str(tmp_path / "square")
+    triangle_reader.write_triangle(prefix, coords, elem)
+    nodes, vnodes, x, els, en, evn = triangle_reader.read_triangle(prefix, op2)
+    f = op2.Dat(nodes, 2 * x.data_ro[:, 0] + 4 * x.data_ro[:, 1], np.float64, "f")
+    b = op2.Dat(nodes, np.zeros(nodes.size), np.float64, "b")
+    mat = op2.Mat(op2.Sparsity((en, en), "sp"), np.float64, "mat")
+    op2.par_loop(op2.Kernel(P1_MASS, "p1_mass"), els(3, 3), mat((en[op2.i[0]], en[op2.i[1]]), op2.INC),
+                 x(evn, op2.READ))
+    op2.par_loop(op2.Kernel(P1_RHS, "p1_rhs"), els(3), b(en[op2.i[0]], op2.INC), x(evn, op2.READ),
+                 f(en, op2.READ))
+    vals = np.sort(mat.array)
+    golden = np.sort(np.repeat(z["mat_values"], z["mat_counts"]))
+    assert vals.size == int(z["nnz"])
+    assert np.abs(vals - golden).max() < 1e-12 * np.abs(golden).max()
+    assert abs(b.data_ro.sum() - float(z["b_sum"])) < 1e-12
+
+
+def test_airfoil_from_mesh_file_layout_matches_oracle(op2):
+    """The airfoil problem declared from a mesh-file layout through
+    fromhdf5 (as pyop2/demo/airfoil.py:45-75 declares it) runs the chain to
+    the oracle's results."""
+    from test_mesh_io import H5File
+    _clear_consts(op2)
+    grid = meshes.airfoil_grid(40, 20, 5)
+    G = airfoil.build_from_hdf5(op2, H5File.from_layout(airfoil.hdf5_layout(grid, seed=5)))
+    O = airfoil.build(seq, 40, 20, 5, grid=grid)
+    for _ in range(2):
+        gr = airfoil.iteration(op2, G)
+        orr = airfoil.iteration(seq, O)
+    assert rel_err(G.p_q.data_ro, O.p_q.data) < 1e-11
+    assert rel_err(gr.data, orr.data) < 1e-11
+    _clear_consts(op2)
+
+
 def test_two_phase_is_bit_exact_and_launch_independent(op2):
     """inc_mode='lma' adds each target's contributions in element order
     starting from its current value -- the sequential backend's order -- so
