@@ -572,83 +572,57 @@ def staged_used(spec):
     return sorted({R["map_stage"][k] for k in used_maps})
 
 
-def _staged_body(spec):
-    """Indirect loop over a locality partition (op2b_region_plan_build), one
-    CTA per block of the reordered set.  The block's distinct target rows
-    of every READ (Dat, staged Map) pair are copied to shared memory once;
-    INC rows are added into shared accumulators colour by colour (the
-    plan's thread colours: no two elements of a colour share a target, so
-    the adds need no atomics) and added to the Dats once per distinct
-    target at the end, with global atomics since neighbouring blocks share
-    targets.  WRITE/RW indirect rows are global pointers (OP2 leaves their
-    conflicts to the user)."""
-    bs = spec.block_size
-    R = spec.region
-    ns = len(R["stage_arity"])
-    used = staged_used(spec)
-    read_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["read_pairs"])}
-    inc_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["inc_pairs"])}
-    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
-    L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
-    L.append("  const int blk = blockIdx.x;")
-    L.append("  const int start = p.rg_boff[blk];")
-    L.append("  const int nelem = p.rg_boff[blk + 1] - start;")
-    L.append("  const op2b_i64 set_size = p.set_size;")
-    L.append("  int smem_off = 0;")
-    for st in used:
-        L.append("  const int n_s%d = p.rg_tcnt[blk * %d + %d];" % (st, ns, st))
-        L.append("  const int *tl_s%d = p.rg_tlist + p.rg_toff[blk * %d + %d];" % (st, ns, st))
-    # every element of this thread (ept passes of bs): its loc rows, colour
-    # and element id are loaded now, while the staged rows are in flight
-    ept = R["ept"]
-    for j in range(ept):
-        L.append("  const int idx_%d = %d + threadIdx.x;" % (j, j * bs))
-        L.append("  const bool active_%d = idx_%d < nelem;" % (j, j))
-        L.append("  const op2b_i64 pos_%d = start + (active_%d ? idx_%d : 0);" % (j, j, j))
+def _staged_prefetch(spec, R, used, bs, ind):
+    """Every element of this thread (ept passes of bs threads): its loc
+    rows, colour and element id, loaded as early as possible."""
+    L = []
+    for j in range(R["ept"]):
+        L.append("%sconst int idx_%d = %d + threadIdx.x;" % (ind, j, j * bs))
+        L.append("%sconst bool active_%d = idx_%d < nelem;" % (ind, j, j))
+        L.append("%sconst op2b_i64 pos_%d = start + (active_%d ? idx_%d : 0);" % (ind, j, j, j))
         for st in used:
             ar = R["stage_arity"][st]
-            L.append("  int sl%d_%d[%d];" % (st, j, ar))
-            L.append("  #pragma unroll")
-            L.append("  for (int r = 0; r < %d; ++r) sl%d_%d[r] = active_%d ? (int)p.rg_loc[(op2b_i64)(%d + r) * "
-                     "set_size + pos_%d] : 0;" % (ar, st, j, j, R["row_base"][st], j))
-        L.append("  const int col_%d = active_%d ? p.rg_thrcol[pos_%d] : -1;" % (j, j, j))
+            L.append("%sint sl%d_%d[%d];" % (ind, st, j, ar))
+            L.append("%s#pragma unroll" % ind)
+            L.append("%sfor (int r = 0; r < %d; ++r) sl%d_%d[r] = active_%d ? (int)p.rg_loc[(op2b_i64)(%d + r) * "
+                     "set_size + pos_%d] : 0;" % (ind, ar, st, j, j, R["row_base"][st], j))
+        L.append("%sconst int col_%d = active_%d ? p.rg_thrcol[pos_%d] : -1;" % (ind, j, j, j))
         # positions are sorted by colour within the block: the pass's colours
         # run from its first position's to its last position's
-        L.append("  const int clo_%d = %d < nelem ? p.rg_thrcol[start + %d] : 0;" % (j, j * bs, j * bs))
-        L.append("  const int chi_%d = %d < nelem ? p.rg_thrcol[start + min(nelem, %d) - 1] : -1;"
-                 % (j, j * bs, (j + 1) * bs))
+        L.append("%sconst int clo_%d = %d < nelem ? p.rg_thrcol[start + %d] : 0;" % (ind, j, j * bs, j * bs))
+        L.append("%sconst int chi_%d = %d < nelem ? p.rg_thrcol[start + min(nelem, %d) - 1] : -1;"
+                 % (ind, j, j * bs, (j + 1) * bs))
         if any(a.kind == "direct" for a in spec.args):
-            L.append("  const op2b_i64 e_%d = active_%d ? p.rg_order[pos_%d] : 0;" % (j, j, j))
-    for q, (slot, st, t, c) in enumerate(R["read_pairs"]):
-        L.append("  %s *rd%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
-        L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
-    # staged READ rows: one target id per row, the rows of every READ pair of
-    # the staged Map copied asynchronously (cp.async) where their size allows
+            L.append("%sconst op2b_i64 e_%d = active_%d ? p.rg_order[pos_%d] : 0;" % (ind, j, j, j))
+    return L
+
+
+def _staged_copy_rows(R, used, bs, ind, dst, n, tl):
+    """cp.async copies of the staged READ rows: one target id per row, the
+    rows of every READ pair of the staged Map (dst % q: destination array of
+    pair q; n % st / tl % st: count and target list of staged Map st)."""
+    L = []
     for st in used:
         pairs = [(q, slot, t, c) for q, (slot, s_, t, c) in enumerate(R["read_pairs"]) if s_ == st]
         if not pairs:
             continue
-        L.append("  for (int r = threadIdx.x; r < n_s%d; r += %d) {" % (st, bs))
-        L.append("    const op2b_i64 g = tl_s%d[r];" % st)
+        L.append("%sfor (int r = threadIdx.x; r < %s; r += %d) {" % (ind, n % st, bs))
+        L.append("%s  const op2b_i64 g = %s[r];" % (ind, tl % st))
         for q, slot, t, c in pairs:
             nb = c * _CSIZE[t]
             if nb % 4 == 0:
-                L.append("    op2b_cp_async_row<%d>(rd%d + r * %d, p.d%d + g * %d);" % (nb, q, c, slot, c))
+                L.append("%s  op2b_cp_async_row<%d>(%s + r * %d, p.d%d + g * %d);" % (ind, nb, dst % q, c, slot, c))
             else:
-                L.append("    for (int k = 0; k < %d; ++k) rd%d[r * %d + k] = p.d%d[g * %d + k];"
-                         % (c, q, c, slot, c))
-        L.append("  }")
-    for q, (slot, st, t, c) in enumerate(R["inc_pairs"]):
-        L.append("  %s *acc%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
-        L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
-        L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) acc%d[t] = (%s)0;"
-                 % (st, c, bs, q, t))
-    if R["read_pairs"]:
-        L.append("  op2b_cp_async_wait();")
-    L.append("  __syncthreads();")
-    _gbl_prologue(spec, L)
-    ind = "    "
-    has_direct = any(a.kind == "direct" for a in spec.args)
+                L.append("%s  for (int k = 0; k < %d; ++k) %s[r * %d + k] = p.d%d[g * %d + k];"
+                         % (ind, c, dst % q, c, slot, c))
+        L.append("%s}" % ind)
+    return L
+
+
+def _staged_element(spec, R, ind):
+    """(decl, pre, post, exprs, adds) of one element of a staged stub."""
+    read_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["read_pairs"])}
+    inc_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["inc_pairs"])}
     decl, pre, post, exprs, adds = [], [], [], [], []
     for n, a in enumerate(spec.args):
         t, c = a.ctype, a.cdim
@@ -708,44 +682,102 @@ def _staged_body(spec):
                 exprs.append("a%d_v" % n)
             else:
                 exprs.append(row_ptr("i%d" % a.idx))
-    for j in range(ept):
-        L.append("  if (%d < nelem) {" % (j * bs))
-        L.append("%sconst bool active = active_%d;" % (ind, j))
+    return decl, pre, post, exprs, adds
+
+
+def _staged_passes(spec, R, used, bs, ind):
+    """The ept passes over the block's elements: compute, then add the INC
+    rows into the shared accumulators colour by colour."""
+    decl, pre, post, exprs, adds = _staged_element(spec, R, ind + "  ")
+    has_direct = any(a.kind == "direct" for a in spec.args)
+    inner = ind + "  "
+    L = []
+    for j in range(R["ept"]):
+        L.append("%sif (%d < nelem) {" % (ind, j * bs))
+        L.append("%sconst bool active = active_%d;" % (inner, j))
         if has_direct:
-            L.append("%sconst op2b_i64 e = e_%d;" % (ind, j))
+            L.append("%sconst op2b_i64 e = e_%d;" % (inner, j))
         for st in used:
             ar = R["stage_arity"][st]
-            L.append("%sconst int sl%d[%d] = {%s};" % (ind, st, ar, ", ".join(
+            L.append("%sconst int sl%d[%d] = {%s};" % (inner, st, ar, ", ".join(
                 "sl%d_%d[%d]" % (st, j, r) for r in range(ar))))
         L += decl
-        L.append("%sif (active) {" % ind)
+        L.append("%sif (active) {" % inner)
         L += pre
-        L += _itspace_open(spec, ind + "  ")
-        L.append(_kernel_call(spec, exprs, ind + "  " + "  " * len(spec.extents)))
-        L += _itspace_close(spec, ind + "  ")
+        L += _itspace_open(spec, inner + "  ")
+        L.append(_kernel_call(spec, exprs, inner + "  " + "  " * len(spec.extents)))
+        L += _itspace_close(spec, inner + "  ")
         L += post
-        L.append("%s}" % ind)
-        L.append("%sfor (int c = clo_%d; c <= chi_%d; ++c) {" % (ind, j, j))
-        L.append("%s  if (col_%d == c) {" % (ind, j))
+        L.append("%s}" % inner)
+        L.append("%sfor (int c = clo_%d; c <= chi_%d; ++c) {" % (inner, j, j))
+        L.append("%s  if (col_%d == c) {" % (inner, j))
         for var, lrow, q, c in adds:
             # read-modify-write of the accumulated row with vector accesses
             # (the rows are 16-byte aligned when their size allows)
             t = R["inc_pairs"][q][2]
-            L.append("%s    { %s *dst = acc%d + %s * %d;" % (ind, t, q, lrow, c))
+            L.append("%s    { %s *dst = acc%d + %s * %d;" % (inner, t, q, lrow, c))
             L.append("%s      __align__(16) %s cur[%d]; op2b_load<%s, %d, false>(cur, dst);"
-                     % (ind, t, c, t, c))
-            L.append("%s      for (int k = 0; k < %d; ++k) cur[k] += %s[k];" % (ind, c, var))
-            L.append("%s      op2b_store(dst, cur); }" % ind)
-        L.append("%s  }" % ind)
-        L.append("%s  __syncthreads();" % ind)
+                     % (inner, t, c, t, c))
+            L.append("%s      for (int k = 0; k < %d; ++k) cur[k] += %s[k];" % (inner, c, var))
+            L.append("%s      op2b_store(dst, cur); }" % inner)
+        L.append("%s  }" % inner)
+        L.append("%s  __syncthreads();" % inner)
+        L.append("%s}" % inner)
         L.append("%s}" % ind)
-        L.append("  }")
+    return L
+
+
+def _staged_flush(R, bs, ind):
+    L = []
     for q, (slot, st, ctype, cdim) in enumerate(R["inc_pairs"]):
-        L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (st, cdim, bs))
-        L.append("    const int r = t / %d, k = t - r * %d;" % (cdim, cdim))
-        L.append("    op2b_atomic_add(p.d%d + (op2b_i64)tl_s%d[r] * %d + k, acc%d[t]);"
-                 % (slot, st, cdim, q))
-        L.append("  }")
+        L.append("%sfor (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (ind, st, cdim, bs))
+        L.append("%s  const int r = t / %d, k = t - r * %d;" % (ind, cdim, cdim))
+        L.append("%s  op2b_atomic_add(p.d%d + (op2b_i64)tl_s%d[r] * %d + k, acc%d[t]);"
+                 % (ind, slot, st, cdim, q))
+        L.append("%s}" % ind)
+    return L
+
+
+def _staged_body(spec):
+    """Indirect loop over a locality partition (op2b_region_plan_build), one
+    CTA per block of the reordered set.  The block's distinct target rows
+    of every READ (Dat, staged Map) pair are copied to shared memory once;
+    INC rows are added into shared accumulators colour by colour (the
+    plan's thread colours: no two elements of a colour share a target, so
+    the adds need no atomics) and added to the Dats once per distinct
+    target at the end, with global atomics since neighbouring blocks share
+    targets.  WRITE/RW indirect rows are global pointers (OP2 leaves their
+    conflicts to the user)."""
+    bs = spec.block_size
+    R = spec.region
+    ns = len(R["stage_arity"])
+    used = staged_used(spec)
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
+    L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
+    L.append("  const int blk = blockIdx.x;")
+    L.append("  const int start = p.rg_boff[blk];")
+    L.append("  const int nelem = p.rg_boff[blk + 1] - start;")
+    L.append("  const op2b_i64 set_size = p.set_size;")
+    L.append("  int smem_off = 0;")
+    for st in used:
+        L.append("  const int n_s%d = p.rg_tcnt[blk * %d + %d];" % (st, ns, st))
+        L.append("  const int *tl_s%d = p.rg_tlist + p.rg_toff[blk * %d + %d];" % (st, ns, st))
+    L += _staged_prefetch(spec, R, used, bs, "  ")
+    for q, (slot, st, t, c) in enumerate(R["read_pairs"]):
+        L.append("  %s *rd%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
+        L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
+    L += _staged_copy_rows(R, used, bs, "  ", "rd%d", "n_s%d", "tl_s%d")
+    for q, (slot, st, t, c) in enumerate(R["inc_pairs"]):
+        L.append("  %s *acc%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
+        L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
+        L.append("  for (int t = threadIdx.x; t < n_s%d * %d; t += %d) acc%d[t] = (%s)0;"
+                 % (st, c, bs, q, t))
+    if R["read_pairs"]:
+        L.append("  op2b_cp_async_wait();")
+    L.append("  __syncthreads();")
+    _gbl_prologue(spec, L)
+    L += _staged_passes(spec, R, used, bs, "  ")
+    L += _staged_flush(R, bs, "  ")
     _gbl_epilogue(spec, L)
     L.append("}")
     return "\n".join(L)
