@@ -338,20 +338,27 @@ class Const(DeviceDataMixin, base.Const):
     """Global constant: a __constant__ symbol of each stub that names it,
     uploaded when its value changed (pyop2/cuda.py:303-323)."""
 
+    # bumped whenever any Const's value may have changed: a module whose
+    # symbols were synchronised at the current stamp needs no check
+    _stamp = 0
+
     def __init__(self, dim, data=None, name=None, dtype=None):
         base.Const.__init__(self, dim, data, name, dtype)
         self._version = 0
         self._state = HOST
+        Const._stamp += 1
 
     @property
     def data(self):
         self._version += 1
+        Const._stamp += 1
         return self._data
 
     @data.setter
     def data(self, value):
         self._data = verify_reshape(value, self.dtype, self.dim)
         self._version += 1
+        Const._stamp += 1
 
     def _from_device(self):
         raise RuntimeError("Copying Const %s from device not allowed" % self)
@@ -948,6 +955,7 @@ class _Module(object):
         self.fn = self.function(stub)
         self.smem_set = 48 * 1024
         self.const_versions = {}
+        self.const_stamp = None
 
     def function(self, name):
         fn = C.c_uint64()
@@ -1251,6 +1259,9 @@ def _sync_consts(mod, consts):
     """Copy Const values into the module's __constant__ symbols when they
     changed since the module last saw them (Const._to_device,
     pyop2/cuda.py:314-320)."""
+    stamp = (Const._stamp, base.Const._generation)
+    if mod.const_stamp == stamp:
+        return
     for c in consts:
         if mod.const_versions.get(c.name) != (id(c), c._version):
             ptr, nbytes = mod.const_ptr(c.name)
@@ -1260,6 +1271,7 @@ def _sync_consts(mod, consts):
                                    (c.name, arr.nbytes, nbytes))
             call("op2b_memcpy_h2d", ptr, arr.ctypes.data, arr.nbytes, 0)
             mod.const_versions[c.name] = (id(c), c._version)
+    mod.const_stamp = stamp
 
 
 class _BoundLoop(object):
@@ -1395,10 +1407,8 @@ class _BoundLoop(object):
         return 512
 
     def matches(self, loop):
-        objs = []
-        for a in loop.args:
-            if a._is_dat:
-                objs.append(a.data)
+        """The Dats, Maps and Mats the loop was bound to are all alive (the
+        key holds their ids, which a new object could reuse otherwise)."""
         return all(r() is not None for r in self.refs)
 
     def _prepare(self, loop):
@@ -1509,24 +1519,41 @@ def _env_key():
     return _ENV["key"]
 
 
+def _loop_key(kernel, iterset, extents, args):
+    """Cache key of a bound loop: the kernel's content, the iteration set
+    and extents, and per argument the identity of its Dat / Mat and Maps,
+    the index and the access mode (a Global only by type, so a fresh Global
+    per call reuses the loop), plus the Consts and configuration."""
+    k = [kernel.cache_key, id(iterset), extents]
+    for a in args:
+        d = a._dat
+        if isinstance(d, base.Global):
+            k.append(("g", d.dtype.str, d.cdim, a._access._mode))
+        elif isinstance(d, base.Mat):
+            m, ix = a._map, a._idx
+            k.append(("m", id(d), id(m[0]), id(m[1]), ix[0].index, ix[1].index, a._access._mode))
+        else:
+            ix = a._idx
+            its = isinstance(ix, IterationIndex)
+            k.append(("d", id(d), id(a._map), its, ix.index if its else ix, a._access._mode))
+    k.append(_env_key())
+    return tuple(k)
+
+
+class _Args(object):
+    """The argument list of a call that reuses a bound loop."""
+    __slots__ = ("args",)
+
+    def __init__(self, args):
+        self.args = args
+
+
 class ParLoop(base.ParLoop):
 
     _bound_cache = {}
 
     def _bound_key(self):
-        k = [self.kernel.cache_key, id(self.it_space.iterset), self.it_space.extents]
-        for a in self.args:
-            if a._is_global:
-                k.append(("g", a.data.dtype.str, a.data.cdim, a.access._mode))
-            elif a._is_mat:
-                k.append(("m", id(a.data), id(a.map[0]), id(a.map[1]), a.idx[0].index,
-                          a.idx[1].index, a.access._mode))
-            else:
-                ix = a.idx.index if isinstance(a.idx, IterationIndex) else a.idx
-                k.append(("d", id(a.data), id(a.map), isinstance(a.idx, IterationIndex), ix,
-                          a.access._mode))
-        k.append(_env_key())
-        return tuple(k)
+        return _loop_key(self.kernel, self.it_space.iterset, self.it_space.extents, self.args)
 
     def compute(self):
         key = self._bound_key()
@@ -1540,7 +1567,27 @@ class ParLoop(base.ParLoop):
 
 def par_loop(kernel, it_space, *args):
     """Run a parallel loop on the device (asynchronous; results are fetched
-    when the host reads them)."""
+    when the host reads them).
+
+    A call whose kernel, iteration space and argument objects (by identity)
+    match an already bound loop runs it directly: those objects passed the
+    reference's argument checks when the loop was bound, and the loop holds
+    weak references that must all still be alive."""
+    if isinstance(it_space, base.IterationSpace):
+        iterset, extents = it_space._iterset, it_space._extents
+    else:
+        iterset, extents = it_space, ()
+    try:
+        key = _loop_key(kernel, iterset, extents, args)
+    except (AttributeError, TypeError, IndexError):
+        key = None   # not well-formed: the full path raises the reference's error
+    bl = ParLoop._bound_cache.get(key) if key is not None else None
+    if bl is not None and bl.matches(None):
+        bl.run(_Args(args))
+        for a in args:
+            if a._access is not READ and isinstance(a._dat, base.Dat):
+                a._dat.needs_halo_update = True
+        return
     ParLoop(kernel, it_space, *args).compute()
 
 
