@@ -365,6 +365,8 @@ def run_gpu(args, ws, rank, local):
         if name == "res_calc":
             res_avg = statistics.mean(ts)
         breakdown[name] = {"ms": round(ms, 4), "GB/s": round(bytes_[name] / (ms * 1e-3) / 1e9, 1)}
+    # the form res_calc ran in (before other legs bind loops of that kernel)
+    res_form = _RES_FORM.get(_loop_mode("res_calc"), "all colour launches")
     # one-off cost of the staged form: building res_calc's locality partition
     partition_ms = None
     staged = [bl for bl in b200.ParLoop._bound_cache.values()
@@ -456,7 +458,7 @@ def run_gpu(args, ws, rank, local):
                        timing="CUDA graph replay, CUDA events per step on the op2 stream, "
                               "max over ranks"),
         "gpu_launches": launches * args.steps,
-        "roofline": {"kernel": "res_calc (%s)" % _RES_FORM.get(_loop_mode("res_calc"), "all colour launches"),
+        "roofline": {"kernel": "res_calc (%s)" % res_form,
                      "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,

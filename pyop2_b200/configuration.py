@@ -53,7 +53,11 @@ keys of the B200 backend:
   built once per Sparsity and Map pair: nelem x arity^2 int32 of device
   memory) instead of searching the CSR row for every entry;
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
-  admits meshes and requests against by default.
+  admits meshes and requests against by default;
+* ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
+  the stream-ordered allocation pool is grown to at initialisation; freed
+  memory stays in the pool, so allocations up to this size never map fresh
+  device memory later (0: grow on demand).
 """
 
 import os
@@ -80,6 +84,7 @@ _defaults = {
     'kahan': False,
     'mat_slots': True,
     'hbm_budget_gb': 120.0,
+    'pool_reserve_gb': 4.0,
 }
 
 _config = dict(_defaults)
