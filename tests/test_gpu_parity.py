@@ -163,6 +163,48 @@ def test_p1_mass_rhs_matches_oracle(op2, n, inc_mode):
     assert rel_err(gb.data_ro, ob.data) < TOL
 
 
+@pytest.mark.parametrize("dtype,cdim", [(np.float64, 3), (np.float32, 3), (np.int32, 1)])
+def test_staged_edge_cases_match_oracle(op2, dtype, cdim):
+    """The staged form on a random edge graph where some edges have both
+    ends at one node (a thread adds twice to one staged row), INC rows of
+    odd width and of float32 / int32, a direct READ arg (read at the
+    reordered element) and a Global MAX, against the sequential oracle."""
+    from pyop2_b200 import configuration as cfg
+    rng = np.random.default_rng(11)
+    nnodes, nedges = 3000, 20000
+    e2n = rng.integers(0, nnodes, size=(nedges, 2)).astype(np.int32)
+    e2n[::97, 1] = e2n[::97, 0]                       # degenerate edges
+    w = rng.integers(1, 5, size=nedges).astype(dtype)
+    ctype = {np.float64: "double", np.float32: "float", np.int32: "int"}[dtype]
+    code = """void k(%(t)s *a, %(t)s *b, %(t)s *w, %(t)s *g) {
+  for (int i = 0; i < %(c)d; ++i) { a[i] += (%(t)s)(i + 1) * w[0]; b[i] += w[0]; }
+  if (w[0] > g[0]) g[0] = w[0];
+}""" % {"t": ctype, "c": cdim}
+    old = (cfg.cfg['inc_mode'], cfg.cfg['staged_min_size'])
+    cfg.configure(inc_mode="staged", staged_min_size=0)
+    try:
+        res = []
+        for api in (op2, seq):
+            edges, nodes = api.Set(nedges, 1, "edges"), api.Set(nnodes, cdim, "nodes")
+            m = api.Map(edges, nodes, 2, e2n, "e2n")
+            x = api.Dat(nodes, np.zeros((nnodes, cdim), dtype), dtype, "x")
+            wd = api.Dat(edges, w.copy(), dtype, "w")
+            g = api.Global(1, 0, dtype, "g")
+            api.par_loop(api.Kernel(code, "k"), edges, x(m[0], api.INC), x(m[1], api.INC),
+                         wd(api.IdentityMap, api.READ), g(api.MAX))
+            res.append((np.array(x.data_ro if api is op2 else x.data), np.array(g.data)))
+        from pyop2_b200 import b200
+        assert any(bl.spec.mode == "staged" for bl in b200.ParLoop._bound_cache.values()
+                   if bl.spec.kernel_name == "k")
+        if dtype == np.int32:
+            np.testing.assert_array_equal(res[0][0], res[1][0])
+        else:
+            assert rel_err(res[0][0], res[1][0]) < (1e-12 if dtype == np.float64 else 1e-6)
+        np.testing.assert_array_equal(res[0][1], res[1][1])
+    finally:
+        cfg.configure(inc_mode=old[0], staged_min_size=old[1])
+
+
 def test_owner_mode_is_bit_exact(op2):
     """Owner-computes adds each target's contributions in element order
     starting from its current value -- the sequential backend's order -- so
