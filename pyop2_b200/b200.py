@@ -1283,12 +1283,17 @@ def _sync_consts(mod, consts):
     mod.const_stamp = stamp
 
 
+class _StagedTooLarge(Exception):
+    """The staged form of a loop needs more shared memory per CTA than the
+    device has: the loop is bound in the atomic form instead."""
+
+
 class _BoundLoop(object):
     """Everything about a par_loop that does not change between calls with
     the same objects: generated stub, plan, parameter block."""
 
-    def __init__(self, loop):
-        info = loop_spec(loop)
+    def __init__(self, loop, inc_mode=None):
+        info = loop_spec(loop, inc_mode=inc_mode)
         spec = info['spec']
         specs = info['specs']
         dats, maps, mats, gbls = info['dats'], info['maps'], info['mats'], info['gbls']
@@ -1369,8 +1374,7 @@ class _BoundLoop(object):
                 vals["rg_" + name] = rp.dptr[name]
             self.launch_smem = codegen.staged_smem(spec, rp.max_count)
             if self.launch_smem > _state['smem_optin']:
-                raise DeviceError("par_loop %s needs %d bytes of shared memory per block; "
-                                  "lower partition_size" % (loop.kernel.name, self.launch_smem))
+                raise _StagedTooLarge()
             self.module.ensure_smem(self.launch_smem)
             self.grid = rp.nblocks
             self.max_grid = max(1, rp.nblocks)
@@ -1568,7 +1572,10 @@ class ParLoop(base.ParLoop):
         key = self._bound_key()
         bl = ParLoop._bound_cache.get(key)
         if bl is None or not bl.matches(self):
-            bl = _BoundLoop(self)
+            try:
+                bl = _BoundLoop(self)
+            except _StagedTooLarge:
+                bl = _BoundLoop(self, inc_mode='atomic')
             ParLoop._bound_cache[key] = bl
         bl.run(self)
         self.maybe_set_halo_update_needed()

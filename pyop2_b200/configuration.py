@@ -27,8 +27,9 @@ keys of the B200 backend:
   partition: the set is reordered into compact regions grown on the GPU,
   each block's distinct targets are staged in shared memory and INC rows
   accumulated there, then added once per target with atomics; summation
-  order varies between runs within rounding; loops without indirect INC or
-  with Mats run as ``'atomic'``);
+  order varies between runs within rounding; loops without indirect INC,
+  with Mats, or whose staged rows would not fit a CTA's shared memory run
+  as ``'atomic'``);
 * ``region_size``: elements per region (one hashed seed per about this many
   elements) of the staged form's locality partition (0: half the partition
   size, whose default in the staged form is 384);

@@ -205,6 +205,35 @@ def test_staged_edge_cases_match_oracle(op2, dtype, cdim):
         cfg.configure(inc_mode=old[0], staged_min_size=old[1])
 
 
+def test_staged_too_wide_falls_back_to_atomic(op2):
+    """INC rows too wide for the staged form's shared memory (128 doubles
+    per row, ~380 distinct targets per block: ~390 KB) run in the atomic
+    form, with the oracle's results."""
+    from pyop2_b200 import b200
+    from pyop2_b200 import configuration as cfg
+    rng = np.random.default_rng(12)
+    nnodes, nedges, cdim = 20000, 60000, 128
+    e2n = rng.integers(0, nnodes, size=(nedges, 2)).astype(np.int32)
+    code = """void kw(double *a, double *b) {
+  for (int i = 0; i < 128; ++i) { a[i] += 1.0 + i; b[i] += 0.5 * i; }
+}"""
+    old = (cfg.cfg['inc_mode'], cfg.cfg['staged_min_size'])
+    cfg.configure(inc_mode="staged", staged_min_size=0)
+    try:
+        out = []
+        for api in (op2, seq):
+            edges, nodes = api.Set(nedges, 1, "edges"), api.Set(nnodes, cdim, "nodes")
+            m = api.Map(edges, nodes, 2, e2n, "e2n")
+            x = api.Dat(nodes, np.zeros((nnodes, cdim)), np.float64, "x")
+            api.par_loop(api.Kernel(code, "kw"), edges, x(m[0], api.INC), x(m[1], api.INC))
+            out.append(np.array(x.data_ro if api is op2 else x.data))
+        modes = {bl.spec.mode for bl in b200.ParLoop._bound_cache.values() if bl.spec.kernel_name == "kw"}
+        assert modes == {"atomic"}
+        assert rel_err(out[0], out[1]) < 1e-12
+    finally:
+        cfg.configure(inc_mode=old[0], staged_min_size=old[1])
+
+
 def test_owner_mode_is_bit_exact(op2):
     """Owner-computes adds each target's contributions in element order
     starting from its current value -- the sequential backend's order -- so
