@@ -11,6 +11,7 @@ written against the reference run unchanged: access descriptors (:56-90),
 parameters (:1591-1657).  Device behaviour lives in :mod:`pyop2_b200.b200`.
 """
 
+import math
 import operator
 from hashlib import md5
 
@@ -184,7 +185,7 @@ class Set(object):
         self._core_size, self._size, self._ieh_size, self._inh_size = size
         self._dim = as_tuple(dim, (int, np.integer))
         self._dim = tuple(int(d) for d in self._dim)
-        self._cdim = int(np.prod(self._dim))
+        self._cdim = math.prod(self._dim)
         self._name = name or "set_%d" % Set._globalcount
         self._halo = halo
         if self._halo is not None:
@@ -399,8 +400,16 @@ class Dat(DataCarrier):
         soa = _h5_str(slot.attrs['type']).find(':soa') > 0
         return cls(dataset, data, name=name, soa=soa)
 
-    @validate_in(('access', _modes, ModeValueError))
     def __call__(self, path, access):
+        if access is READ or access is INC or access is WRITE or access is RW:
+            return self._arg(path, access)
+        return self._call_checked(path, access)
+
+    @validate_in(('access', _modes, ModeValueError))
+    def _call_checked(self, path, access):
+        return self._arg(path, access)
+
+    def _arg(self, path, access):
         if isinstance(path, Map):
             if path._dataset != self._dataset and path is not IdentityMap:
                 raise MapValueError("Dataset of Map does not match Dataset of Dat.")
@@ -530,7 +539,7 @@ class Const(DataCarrier):
     def __init__(self, dim, data=None, name=None, dtype=None):
         self._dim = as_tuple(dim, (int, np.integer))
         self._dim = tuple(int(d) for d in self._dim)
-        self._cdim = int(np.prod(self._dim))
+        self._cdim = math.prod(self._dim)
         self._data = verify_reshape(data, dtype, self._dim, allow_none=True)
         self._name = name or "const_%d" % Const._globalcount
         if any(self._name == c._name for c in Const._defs):
@@ -594,7 +603,7 @@ class Global(DataCarrier):
     def __init__(self, dim, data=None, dtype=None, name=None):
         self._dim = as_tuple(dim, (int, np.integer))
         self._dim = tuple(int(d) for d in self._dim)
-        self._cdim = int(np.prod(self._dim))
+        self._cdim = math.prod(self._dim)
         self._data = verify_reshape(data, dtype, self._dim, allow_none=True)
         self._name = name or "global_%d" % Global._globalcount
         Global._globalcount += 1
@@ -681,8 +690,14 @@ class Map(object):
             raise DimTypeError("Unrecognised dimension value %s" % (dim,))
         return cls(iterset, dataset, dim[0], values, name)
 
-    @validate_type(('index', (int, np.integer, IterationIndex), IndexTypeError))
     def __getitem__(self, index):
+        # the common case first: a Python int within the arity
+        if type(index) is int and 0 <= index < self._dim:
+            return _make_object('Arg', map=self, idx=index)
+        return self._getitem_checked(index)
+
+    @validate_type(('index', (int, np.integer, IterationIndex), IndexTypeError))
+    def _getitem_checked(self, index):
         if isinstance(index, (int, np.integer)) and not (0 <= index < self._dim):
             raise IndexValueError("Index must be in interval [0,%d]" % (self._dim - 1))
         if isinstance(index, IterationIndex) and index.index not in [0, 1]:

@@ -122,6 +122,9 @@ def verify_reshape(data, dtype, shape, allow_none=False):
         return np.asarray([], dtype=t)
     elif data is None:
         raise DataValueError("Invalid data: None is not allowed!")
+    if isinstance(data, (int, float)) and shape in ((1,), 1):
+        # a scalar (a Global's or Const's usual value): no array round trip
+        return np.array([data], dtype=t if t is not None else np.asarray(data).dtype)
     try:
         a = np.asarray(data, dtype=t)
     except (ValueError, TypeError):
