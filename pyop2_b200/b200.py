@@ -1400,7 +1400,7 @@ class _BoundLoop(object):
                 for ix in st[4]:
                     mask |= 1 << ix
                 self.lma.append((buf, _incidence(mp), d, st[3], mp.dataset.size, mp.dim, mask))
-            self.grid = max(1, min((n + bs - 1) // bs, _state['sm_count'] * 8)) if n else 0
+            self.grid = self._wave_grid(n, bs)
             self.max_grid = self.grid
         elif spec.mode == "owner":
             # one warp per target of the owner Map
@@ -1412,12 +1412,21 @@ class _BoundLoop(object):
             self.grid = max(1, min((warps * 32 + bs - 1) // bs, _state['sm_count'] * 16)) if warps else 0
             self.max_grid = self.grid
         else:
-            self.grid = max(1, min((n + bs - 1) // bs, _state['sm_count'] * 8)) if n else 0
+            self.grid = self._wave_grid(n, bs)
             self.max_grid = self.grid
 
     @staticmethod
     def _default_part_size(stages):
         return 512
+
+    def _wave_grid(self, n, bs):
+        """Grid of a grid-stride stub: one wave of the CTAs that fit on the
+        device at once (the stub's own occupancy), fewer when the set is
+        smaller than that wave."""
+        if not n:
+            return 0
+        occ = max(1, self.module.occupancy(self.module.fn, bs, 0))
+        return max(1, min((n + bs - 1) // bs, occ * _state['sm_count']))
 
     def matches(self, loop):
         """The Dats, Maps and Mats the loop was bound to are all alive (the
