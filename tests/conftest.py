@@ -24,6 +24,19 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 GPU (runs the CUDA backend)")
 
 
+@pytest.fixture(autouse=True)
+def _configuration_restored():
+    """Every test starts from the configuration the previous one found: a
+    test that changes keys (inc_mode, staged_min_size ...) cannot leak them."""
+    from pyop2_b200 import configuration as cfg
+    saved = dict(cfg._config)
+    yield
+    if cfg._config != saved:
+        cfg._config.clear()
+        cfg._config.update(saved)
+        cfg._generation[0] += 1
+
+
 @pytest.fixture(scope="session")
 def backend():
     """The B200 backend, initialised once per session.  On a machine with a

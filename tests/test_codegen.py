@@ -162,7 +162,7 @@ def test_atomic_mode_stubs(host_op2, golden_matrices):
                                            op2.Global(1, 1.0, np.float64)(op2.READ)))
         assert info["spec"].mode == "plan"
     finally:
-        cfg.configure(inc_mode="atomic", owner_mode="auto")
+        cfg.configure(inc_mode="staged", owner_mode="never")
 
 
 def test_staged_mode_stubs(host_op2, golden_matrices):
@@ -228,7 +228,7 @@ def test_staged_mode_stubs(host_op2, golden_matrices):
                                         coords(evn, op2.READ)))
         assert m["spec"].mode == "atomic"
     finally:
-        cfg.configure(inc_mode="atomic", owner_mode="never", staged_min_size=65536)
+        cfg.configure(inc_mode="staged", owner_mode="never", staged_min_size=262144)
         for c in A.consts:
             c.remove_from_namespace()
 
@@ -263,7 +263,7 @@ def test_owner_mode_stubs(host_op2, golden_matrices):
                 assert "inc_list" in layout.fields
                 assert ("comp[" in src) == kahan
         finally:
-            cfg.configure(owner_mode="auto", kahan=False)
+            cfg.configure(owner_mode="never", kahan=False)
     # a Global reduction forbids owner-computes
     red = op2.Global(1, 0.0, np.float64)
     info = b200.loop_spec(b200.ParLoop(op2.Kernel("void kg(double *b, double *g) { }", "kg"), el,

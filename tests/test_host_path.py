@@ -44,7 +44,7 @@ def test_loop_key_identity_rules(op2):
     assert key(x, m, op2.INC, g3) != base          # a Global of another type
     old = cfg.cfg['inc_mode']
     try:
-        cfg.configure(inc_mode="atomic")
+        cfg.configure(inc_mode="lma" if old != "lma" else "atomic")
         assert key(x, m, op2.INC, g1) != base      # the configuration is part of the key
     finally:
         cfg.configure(inc_mode=old)
