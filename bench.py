@@ -265,6 +265,8 @@ def run_gpu(args, ws, rank, local):
         opts["inc_mode"] = args.inc_mode
     if args.staged_block_size:
         opts["staged_block_size"] = args.staged_block_size
+    if args.region_size:
+        opts["region_size"] = args.region_size
     op2.init(backend="b200", device=local, **opts)
     if args.assembly_only:
         # the Mat assembly legs alone (profiling their kernels); not a bench line
@@ -875,6 +877,8 @@ def main(argv=None):
     p.add_argument("--block-size", type=int, default=0, help="threads per CTA (0: backend default)")
     p.add_argument("--staged-block-size", type=int, default=0,
                    help="threads per CTA of staged loops (0: backend default)")
+    p.add_argument("--region-size", type=int, default=0,
+                   help="elements per region of the staged form's partition (0: backend default)")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     p.add_argument("--no-assembly", action="store_true", help="skip the Mat assembly legs")
     p.add_argument("--assembly-only", action="store_true",
