@@ -611,7 +611,7 @@ def _staged_copy_rows(R, used, bs, ind, dst, n, tl):
         for q, slot, t, c in pairs:
             nb = c * _CSIZE[t]
             if nb % 4 == 0:
-                L.append("%s  op2b_cp_async_row<%d>(%s + r * %d, p.d%d + g * %d);" % (ind, nb, dst % q, c, slot, c))
+                L.append("%s  op2b_cp_async_srow<%d>(%s, r, p.d%d + g * %d);" % (ind, nb, dst % q, slot, c))
             else:
                 L.append("%s  for (int k = 0; k < %d; ++k) %s[r * %d + k] = p.d%d[g * %d + k];"
                          % (ind, c, dst % q, c, slot, c))
@@ -636,19 +636,20 @@ def _staged_element(spec, R, ind):
         cnt = a.arity if a.kind == "vec" else a.ext
 
         def row_ptr(rowexpr):
-            if a.access == "READ":
-                return "rd%d + %s * %d" % (read_of[(a.slot, st)], "sl%d[%s]" % (st, rowexpr), c)
             return "p.d%d + (op2b_i64)tl_s%d[sl%d[%s]] * %d" % (a.slot, st, st, rowexpr, c)
+
+        def staged_row(rowexpr):
+            return "rd%d, sl%d[%s]" % (read_of[(a.slot, st)], st, rowexpr)
         if a.access == "READ":
             # staged rows into registers with vector shared-memory loads
             if a.kind == "ind":
                 pre.append("%s  __align__(16) %s a%d[%d];" % (ind, t, n, c))
-                pre.append("%s  op2b_load<%s, %d, false>(a%d, %s);" % (ind, t, c, n, row_ptr(str(a.idx))))
+                pre.append("%s  op2b_srow_load(a%d, %s);" % (ind, n, staged_row(str(a.idx))))
                 exprs.append("a%d" % n)
             else:
                 pre.append("%s  __align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
                 for r in range(cnt):
-                    pre.append("%s  op2b_load<%s, %d, false>(a%d[%d], %s);" % (ind, t, c, n, r, row_ptr(str(r))))
+                    pre.append("%s  op2b_srow_load(a%d[%d], %s);" % (ind, n, r, staged_row(str(r))))
                 if a.kind == "vec":
                     pre.append("%s  %s *a%d_v[%d] = {%s};" %
                                (ind, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
@@ -715,11 +716,10 @@ def _staged_passes(spec, R, used, bs, ind):
             # read-modify-write of the accumulated row with vector accesses
             # (the rows are 16-byte aligned when their size allows)
             t = R["inc_pairs"][q][2]
-            L.append("%s    { %s *dst = acc%d + %s * %d;" % (inner, t, q, lrow, c))
-            L.append("%s      __align__(16) %s cur[%d]; op2b_load<%s, %d, false>(cur, dst);"
-                     % (inner, t, c, t, c))
+            L.append("%s    { const int r = %s;" % (inner, lrow))
+            L.append("%s      __align__(16) %s cur[%d]; op2b_srow_load(cur, acc%d, r);" % (inner, t, c, q))
             L.append("%s      for (int k = 0; k < %d; ++k) cur[k] += %s[k];" % (inner, c, var))
-            L.append("%s      op2b_store(dst, cur); }" % inner)
+            L.append("%s      op2b_srow_store(acc%d, r, cur); }" % (inner, q))
         L.append("%s  }" % inner)
         L.append("%s  __syncthreads();" % inner)
         L.append("%s}" % inner)
@@ -732,8 +732,8 @@ def _staged_flush(R, bs, ind):
     for q, (slot, st, ctype, cdim) in enumerate(R["inc_pairs"]):
         L.append("%sfor (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (ind, st, cdim, bs))
         L.append("%s  const int r = t / %d, k = t - r * %d;" % (ind, cdim, cdim))
-        L.append("%s  op2b_atomic_add(p.d%d + (op2b_i64)tl_s%d[r] * %d + k, acc%d[t]);"
-                 % (ind, slot, st, cdim, q))
+        L.append("%s  op2b_atomic_add(p.d%d + (op2b_i64)tl_s%d[r] * %d + k, acc%d[op2b_srow_index<%s, %d>(r, k)]);"
+                 % (ind, slot, st, cdim, q, ctype, cdim))
         L.append("%s}" % ind)
     return L
 

@@ -100,6 +100,76 @@ __device__ __forceinline__ void op2b_store(T *__restrict__ dst, const T (&src)[N
   }
 }
 
+// Staged rows in shared memory (the staged form's READ rows and INC
+// accumulators).  Row r of B bytes starts at base + r * B.  When B is 32, 64
+// or 128 (m = B / 16 chunks of 16 bytes), chunk j of row r is kept at chunk
+// j ^ ((r / (8 / m)) mod m) of the row: otherwise chunk j of every row falls
+// in the same m-th of the 32 banks (rows of 32 bytes: only the even or only
+// the odd 16-byte bank groups), and eight threads reading chunk j of eight
+// rows conflict at least two ways.  Other sizes keep the plain layout.
+template <int B>
+struct op2b_srow_layout {
+  static constexpr int M = B / 16;
+  static constexpr bool swizzled = B % 16 == 0 && (M == 2 || M == 4 || M == 8);
+  static constexpr int L = swizzled ? 8 / M : 1;
+  static __device__ __forceinline__ int chunk(int r, int j) {
+    if constexpr (swizzled) return j ^ ((r / L) & (M - 1));
+    else return j;
+  }
+};
+
+// Row r of a staged array into registers.
+template <typename T, int N>
+__device__ __forceinline__ void op2b_srow_load(T (&dst)[N], const T *base, int r) {
+  using Lay = op2b_srow_layout<N * (int)sizeof(T)>;
+  if constexpr (Lay::swizzled) {
+    const uint4 *row = reinterpret_cast<const uint4 *>(base + (op2b_i64)r * N);
+#pragma unroll
+    for (int j = 0; j < Lay::M; ++j) reinterpret_cast<uint4 *>(dst)[j] = row[Lay::chunk(r, j)];
+  } else {
+    op2b_load<T, N, false>(dst, base + (op2b_i64)r * N);
+  }
+}
+
+// Registers into row r of a staged array.
+template <typename T, int N>
+__device__ __forceinline__ void op2b_srow_store(T *base, int r, const T (&src)[N]) {
+  using Lay = op2b_srow_layout<N * (int)sizeof(T)>;
+  if constexpr (Lay::swizzled) {
+    uint4 *row = reinterpret_cast<uint4 *>(base + (op2b_i64)r * N);
+#pragma unroll
+    for (int j = 0; j < Lay::M; ++j) row[Lay::chunk(r, j)] = reinterpret_cast<const uint4 *>(src)[j];
+  } else {
+    op2b_store(base + (op2b_i64)r * N, src);
+  }
+}
+
+// Index in a staged array of element k of row r.
+template <typename T, int N>
+__device__ __forceinline__ int op2b_srow_index(int r, int k) {
+  using Lay = op2b_srow_layout<N * (int)sizeof(T)>;
+  if constexpr (Lay::swizzled) {
+    constexpr int E = 16 / (int)sizeof(T);
+    return r * N + Lay::chunk(r, k / E) * E + k % E;
+  } else {
+    return r * N + k;
+  }
+}
+
+// cp.async of one row (B bytes at src) into row r of a staged array.
+template <int B>
+__device__ __forceinline__ void op2b_cp_async_srow(void *base, int r, const void *src) {
+  using Lay = op2b_srow_layout<B>;
+  char *row = reinterpret_cast<char *>(base) + (op2b_i64)r * B;
+  if constexpr (Lay::swizzled) {
+    const char *g = reinterpret_cast<const char *>(src);
+#pragma unroll
+    for (int j = 0; j < Lay::M; ++j) op2b_cp_async_row<16>(row + 16 * Lay::chunk(r, j), g + 16 * j);
+  } else {
+    op2b_cp_async_row<B>(row, src);
+  }
+}
+
 // SoA row: component k of element e lives at base[k * stride + e].
 template <typename T, int N>
 __device__ __forceinline__ void op2b_load_soa(T (&dst)[N], const T *__restrict__ base, op2b_i64 e,

@@ -205,6 +205,45 @@ def test_staged_edge_cases_match_oracle(op2, dtype, cdim):
         cfg.configure(inc_mode=old[0], staged_min_size=old[1])
 
 
+@pytest.mark.parametrize("dtype,cdim", [(np.float64, 4), (np.float64, 8), (np.float64, 16),
+                                        (np.float32, 8), (np.int32, 32)])
+def test_staged_wide_rows_match_oracle(op2, dtype, cdim):
+    """Staged READ rows and INC accumulators of 32, 64 and 128 bytes, whose
+    16-byte chunks the staged form keeps in a permuted order in shared
+    memory, against the sequential oracle."""
+    from pyop2_b200 import configuration as cfg
+    rng = np.random.default_rng(5)
+    nnodes, nedges = 2000, 15000
+    e2n = rng.integers(0, nnodes, size=(nedges, 2)).astype(np.int32)
+    e2n[::53, 1] = e2n[::53, 0]
+    y0 = rng.integers(-50, 50, size=(nnodes, cdim)).astype(dtype)
+    ctype = {np.float64: "double", np.float32: "float", np.int32: "int"}[dtype]
+    code = """void kwr(%(t)s *a, %(t)s *b, %(t)s *y0, %(t)s *y1) {
+  for (int i = 0; i < %(c)d; ++i) { a[i] += y1[i] * (%(t)s)(i + 1); b[i] += y0[i] - y1[(i + 1) %% %(c)d]; }
+}""" % {"t": ctype, "c": cdim}
+    old = (cfg.cfg['inc_mode'], cfg.cfg['staged_min_size'])
+    cfg.configure(inc_mode="staged", staged_min_size=0)
+    try:
+        res = []
+        for api in (op2, seq):
+            edges, nodes = api.Set(nedges, 1, "edges"), api.Set(nnodes, cdim, "nodes")
+            m = api.Map(edges, nodes, 2, e2n, "e2n")
+            x = api.Dat(nodes, np.zeros((nnodes, cdim), dtype), dtype, "x")
+            y = api.Dat(nodes, y0.copy(), dtype, "y")
+            api.par_loop(api.Kernel(code, "kwr"), edges, x(m[0], api.INC), x(m[1], api.INC),
+                         y(m[0], api.READ), y(m[1], api.READ))
+            res.append(np.array(x.data_ro if api is op2 else x.data))
+        from pyop2_b200 import b200
+        assert any(bl.spec.mode == "staged" for bl in b200.ParLoop._bound_cache.values()
+                   if bl.spec.kernel_name == "kwr")
+        if dtype == np.int32:
+            np.testing.assert_array_equal(res[0], res[1])
+        else:
+            assert rel_err(res[0], res[1]) < (1e-12 if dtype == np.float64 else 1e-6)
+    finally:
+        cfg.configure(inc_mode=old[0], staged_min_size=old[1])
+
+
 def test_staged_too_wide_falls_back_to_atomic(op2):
     """INC rows too wide for the staged form's shared memory (128 doubles
     per row, ~380 distinct targets per block: ~390 KB) run in the atomic
