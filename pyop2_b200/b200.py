@@ -1022,10 +1022,6 @@ def _get_module(spec):
 
 
 # ------------------------------------------------------------------ par_loop
-def _acc_name(acc):
-    return acc._mode
-
-
 def _slots_usable(specs):
     """Scatter-slot tables serve a loop whose Mats are scalar and each
     assembled through one (row Map, column Map) pair."""

@@ -222,15 +222,6 @@ def stub_name(spec):
     return "op2b_" + re.sub(r"[^A-Za-z0-9_]", "_", spec.kernel_name)
 
 
-def _kernel_source(spec):
-    """User kernel as a device function.  Every function of the user code is
-    compiled for the device (NVRTC -default-device) and the entry is forced
-    inline so its pointer arguments resolve to the stub's registers."""
-    code = spec.kernel_code
-    return ("#define OP2_STRIDE(a, idx) (a)[idx]\n"
-            "__forceinline__\n" + _mark_inline(code, spec.kernel_name) + "\n#undef OP2_STRIDE\n")
-
-
 def _mark_inline(code, name):
     import re
     pat = re.compile(r"(^|[;}\s])((?:static\s+|inline\s+)*void\s+%s\s*\()" % re.escape(name))

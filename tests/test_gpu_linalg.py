@@ -12,7 +12,7 @@ import pytest
 from numpy.testing import assert_allclose
 
 from conftest import rel_err
-from oracle import linalg, seq
+from oracle import linalg
 from pyop2_b200.workloads import fem, meshes
 
 pytestmark = pytest.mark.gpu

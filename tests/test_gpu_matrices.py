@@ -185,7 +185,6 @@ def test_insert_outside_sparsity_raises(op2):
     del mat3, m2
     with pytest.raises(MapValueError):
         from pyop2_b200 import b200
-        from pyop2_b200.codegen import ArgSpec  # noqa: F401
         # a Mat whose pattern lacks (0, 3): assemble through m3 columns
         sp_small = op2.Sparsity((m1, m1))
         matx = op2.Mat(sp_small, np.float64)

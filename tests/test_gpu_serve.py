@@ -5,7 +5,6 @@ Tolerances: P1 assembly results within 1e-12 normwise relative (atomic INC
 order differs between batches); airfoil chains (10 iterations, the
 res_calc INC order differs) within 1e-11 for q and rms."""
 
-import numpy as np
 import pytest
 
 from conftest import rel_err
