@@ -7,11 +7,17 @@
   present (``OP2B_REFERENCE`` or /root/reference).  The reference's build
   system is not used: its other native parts need OP2-Common and PETSc, which
   are not available, so only this one translation unit is compiled.
+* ``oracle/_ref/plan<ext>``: the reference's own ``pyop2/plan.pyx``
+  translated unmodified by Cython (``-2``: the Python 2 language level it was
+  written for; the generated C lives in a temporary directory removed after
+  the build) and compiled with gcc as a CPython extension.  ``oracle/reference.py`` imports it with
+  stand-ins for the two modules it imports (``base``, ``utils``).
 """
 
 import os
 import subprocess
 import sys
+import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
@@ -47,6 +53,35 @@ def build_ref(force=False):
     return out
 
 
+def build_ref_plan(force=False):
+    """Translate and compile the reference's plan.pyx; None if it is absent."""
+    src = os.path.join(REFERENCE, "pyop2", "plan.pyx")
+    if not os.path.exists(src):
+        return None
+    import shutil
+    import tempfile
+
+    import numpy
+    os.makedirs(REF_OUT, exist_ok=True)
+    out = os.path.join(REF_OUT, "plan" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if force or _stale(out, [src]):
+        tmp = tempfile.mkdtemp(prefix="op2b_refplan_")
+        try:
+            csrc = os.path.join(tmp, "plan.c")
+            subprocess.check_call([sys.executable, "-m", "cython", "-2", src, "-o", csrc])
+            subprocess.check_call(["gcc", "-O2", "-shared", "-fPIC", "-w",
+                                   "-I" + sysconfig.get_paths()["include"], "-I" + numpy.get_include(),
+                                   csrc, "-o", out])
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
+def ref_plan_path():
+    p = os.path.join(REF_OUT, "plan" + sysconfig.get_config_var("EXT_SUFFIX"))
+    return p if os.path.exists(p) else None
+
+
 def ref_lib_path():
     p = os.path.join(REF_OUT, "libref_sparsity.so")
     return p if os.path.exists(p) else None
@@ -55,3 +90,4 @@ def ref_lib_path():
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
+    print(build_ref_plan(force="--force" in sys.argv))
