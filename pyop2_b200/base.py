@@ -376,8 +376,11 @@ class Dat(DataCarrier):
     @validate_type(('dataset', Set, SetTypeError), ('name', str, NameTypeError))
     def __init__(self, dataset, data=None, dtype=None, name=None, soa=None, uid=None):
         if data is None:
-            data = np.zeros(dataset.total_size * dataset.cdim,
-                            dtype=np.dtype(dtype) if dtype is not None else np.float64)
+            try:
+                t = np.dtype(dtype) if dtype is not None else np.float64
+            except TypeError:
+                raise DataTypeError("Invalid data type: %s" % dtype)
+            data = np.zeros(dataset.total_size * dataset.cdim, dtype=t)
         self._dataset = dataset
         self._data = verify_reshape(data, dtype, (dataset.total_size,) + dataset.dim,
                                     allow_none=True)
@@ -694,6 +697,9 @@ class Map(object):
         # the common case first: a Python int within the arity
         if type(index) is int and 0 <= index < self._dim:
             return _make_object('Arg', map=self, idx=index)
+        if isinstance(index, slice):
+            # test/unit/test_api.py:655-660: slicing a Map is not supported
+            raise NotImplementedError("Slicing maps is not allowed")
         return self._getitem_checked(index)
 
     @validate_type(('index', (int, np.integer, IterationIndex), IndexTypeError))
