@@ -17,7 +17,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, os.path.dirname(HERE))
 
+from conftest import py2_shuffle, reference_seed  # noqa: E402
 from oracle import reference  # noqa: E402
 from pyop2_b200.workloads import meshes  # noqa: E402
 
@@ -68,6 +70,27 @@ def cases():
     out.append(("one_dat_two_maps", reference.plan_case(
         400, {"m1": (m1, 50), "m2": (m2, 50)}, {"v": (50, "float32", 3)},
         [("v", "m1", 0, "INC"), ("v", "m2", 0, "INC"), ("v", "m2", 1, "INC")]), 40, False))
+    # the loops of test/unit/test_plan.py: a shuffled one-to-one map written
+    # (:73-83, partition 128), a chain of 4095 edges reading both ends (:85-109,
+    # partition 96) and the two-element RHS (:111-142, partition 2)
+    n = 4096
+    u = np.arange(n, dtype=np.int32)
+    py2_shuffle(u, reference_seed)
+    out.append(("test_plan_onecolor_wo", reference.plan_case(
+        n, {"u": (u.reshape(n, 1), n)}, {"x": (n, "uint32", 1)}, [("x", "u", 0, "WRITE")]), 128, False))
+    e = np.array([(i, i + 1) for i in range(n - 1)], dtype=np.int32)
+    out.append(("test_plan_2d_map", reference.plan_case(
+        n - 1, {"e2n": (e, n)}, {"node_vals": (n, "uint32", 1), "edge_vals": (n - 1, "uint32", 1)},
+        [("node_vals", "e2n", 0, "READ"), ("node_vals", "e2n", 1, "READ"),
+         ("edge_vals", None, None, "WRITE")]), 96, False))
+    en = np.array([0, 1, 3, 2, 3, 1], dtype=np.int32).reshape(2, 3)
+    out.append(("test_plan_rhs", reference.plan_case(
+        2, {"elem_node": (en, 4)},
+        {"b": (4, "float64", 1), "coords": (4, "float64", 2), "f": (4, "float64", 1)},
+        [("b", "elem_node", 0, "INC"), ("b", "elem_node", 1, "INC"), ("b", "elem_node", 2, "INC"),
+         ("coords", "elem_node", 0, "READ"), ("coords", "elem_node", 1, "READ"),
+         ("coords", "elem_node", 2, "READ"), ("f", "elem_node", 0, "READ"),
+         ("f", "elem_node", 1, "READ"), ("f", "elem_node", 2, "READ")]), 2, False))
     return out
 
 

@@ -65,10 +65,12 @@ def _fixtures():
     return z, index
 
 
-@pytest.mark.parametrize("k", range(8))
+_NCASES = len(_fixtures()[1])
+
+
+@pytest.mark.parametrize("k", range(_NCASES))
 def test_oracle_plan_equals_reference_fixture(k):
     z, index = _fixtures()
-    assert len(index) == 8
     c = index[k]
     n = c["name"]
     maps = {m: (z["%s/map/%s" % (n, m)], t) for m, t in c["maps"].items()}
