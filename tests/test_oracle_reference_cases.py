@@ -1,0 +1,127 @@
+"""The sequential oracle on the cases of the reference's unit tests whose
+answers are exact: vector-map and iteration-space access to Dats (READ,
+WRITE, INC of 1- and 2-component rows through a 2-to-1 node-to-element Map;
+test/unit/test_vector_map.py and test_iteration_space_dats.py) and Global
+MIN / MAX / INC reductions over 4096 elements of several types
+(test/unit/test_global_reduction.py).  The expected values are the ones
+those tests state.  CPU only."""
+
+import numpy as np
+import pytest
+
+from oracle import seq
+
+NNODES = 4096
+NELE = NNODES // 2
+
+
+def _node2ele(dim):
+    node, ele = seq.Set(NNODES, dim, "node"), seq.Set(NELE, dim, "ele")
+    return node, ele, seq.Map(node, ele, 1, np.arange(NNODES) // 2, "node2ele")
+
+
+def _arg(vd, m, acc, itspace):
+    return vd(m[seq.i[0]], acc) if itspace else vd(m, acc)
+
+
+def _sig(itspace, dim):
+    """Kernel parameter for the element row: a pointer, or (vector Map) an
+    array of one row pointer."""
+    return ("int *vd", "vd[%d]") if itspace else ("int *vd[1]", "vd[0][%d]")
+
+
+def _loop(code, node, itspace, *args):
+    seq.par_loop(seq.Kernel(code, "k"), node(1) if itspace else node, *args)
+
+
+@pytest.mark.parametrize("itspace", [False, True])
+def test_sum_nodes_to_edges(itspace):
+    nedges = NNODES - 1
+    nodes, edges = seq.Set(NNODES, 1, "nodes"), seq.Set(nedges, 1, "edges")
+    node_vals = seq.Dat(nodes, np.arange(NNODES, dtype=np.uint32), np.uint32, "node_vals")
+    edge_vals = seq.Dat(edges, np.zeros(nedges, dtype=np.uint32), np.uint32, "edge_vals")
+    e2n = seq.Map(edges, nodes, 2, np.array([(i, i + 1) for i in range(nedges)]), "edge2node")
+    if itspace:
+        code = "void k(unsigned int *nodes, unsigned int *edge, int i) { *edge += nodes[0]; }"
+        seq.par_loop(seq.Kernel(code, "k"), edges(2), node_vals(e2n[seq.i[0]], seq.READ),
+                     edge_vals(seq.IdentityMap, seq.INC))
+    else:
+        code = "void k(unsigned int *nodes[1], unsigned int *edge) { *edge = nodes[0][0] + nodes[1][0]; }"
+        seq.par_loop(seq.Kernel(code, "k"), edges, node_vals(e2n, seq.READ),
+                     edge_vals(seq.IdentityMap, seq.WRITE))
+    np.testing.assert_array_equal(edge_vals.data.ravel(), np.arange(1, nedges * 2 + 1, 2))
+
+
+@pytest.mark.parametrize("itspace", [False, True])
+@pytest.mark.parametrize("dim", [1, 2])
+def test_read_rows(itspace, dim):
+    node, ele, m = _node2ele(dim)
+    d = seq.Dat(node, np.zeros(NNODES * dim), np.int32)
+    vd = seq.Dat(ele, np.arange(NELE * dim), np.int32)
+    p, r = _sig(itspace, dim)
+    body = " ".join("d[%d] = %s;" % (c, r % c) for c in range(dim))
+    _loop("void k(int *d, %s%s) { %s }" % (p, ", int i" if itspace else "", body), node, itspace,
+          d(seq.IdentityMap, seq.WRITE), _arg(vd, m, seq.READ, itspace))
+    np.testing.assert_array_equal(d.data[::2], vd.data)
+    np.testing.assert_array_equal(d.data[1::2], vd.data)
+
+
+@pytest.mark.parametrize("itspace", [False, True])
+@pytest.mark.parametrize("dim", [1, 2])
+def test_write_rows(itspace, dim):
+    node, ele, m = _node2ele(dim)
+    vd = seq.Dat(ele, np.zeros(NELE * dim), np.int32)
+    p, r = _sig(itspace, dim)
+    body = " ".join("%s = %d;" % (r % c, 2 + c) for c in range(dim))
+    _loop("void k(%s%s) { %s }" % (p, ", int i" if itspace else "", body), node, itspace,
+          _arg(vd, m, seq.WRITE, itspace))
+    for c in range(dim):
+        assert (vd.data.reshape(NELE, dim)[:, c] == 2 + c).all()
+
+
+@pytest.mark.parametrize("itspace", [False, True])
+@pytest.mark.parametrize("dim", [1, 2])
+def test_inc_rows(itspace, dim):
+    node, ele, m = _node2ele(dim)
+    d = seq.Dat(node, np.arange(NNODES * dim), np.int32)
+    start = [3, 4][:dim]
+    vd = seq.Dat(ele, np.tile(start, NELE), np.int32)
+    p, r = _sig(itspace, dim)
+    body = " ".join("%s += d[%d];" % (r % c, c) for c in range(dim))
+    _loop("void k(int *d, %s%s) { %s }" % (p, ", int i" if itspace else "", body), node, itspace,
+          d(seq.IdentityMap, seq.READ), _arg(vd, m, seq.INC, itspace))
+    got = vd.data.reshape(NELE, dim)
+    for c in range(dim):
+        want = start[c] + np.arange(c, dim * NNODES, 2 * dim) + np.arange(c + dim, dim * NNODES, 2 * dim)
+        np.testing.assert_array_equal(got[:, c], want)
+
+
+@pytest.mark.parametrize("dtype,ctype,fill,g0,mode,want", [
+    (np.uint32, "unsigned int", 12, 8, "MIN", 8),
+    (np.int32, "int", -12, 8, "MIN", -12),
+    (np.int32, "int", -12, -42, "MAX", -12),
+    (np.uint32, "unsigned int", 12, 42, "MAX", 42),
+    (np.float32, "float", -12.0, -42.0, "MAX", -12.0),
+    (np.float64, "double", -12.0, 8.0, "MIN", -12.0),
+    (np.uint32, "unsigned int", 12, 0, "INC", 12 * 4096),
+    (np.int32, "int", -12, 0, "INC", -12 * 4096),
+    (np.float64, "double", -12.0, 0.0, "INC", -12.0 * 4096),
+])
+def test_global_reductions(dtype, ctype, fill, g0, mode, want):
+    s = seq.Set(4096, 1, "set")
+    d = seq.Dat(s, [fill] * 4096, dtype, "d")
+    g = seq.Global(1, g0, dtype, "g")
+    op = {"MIN": "if (*x < *g) *g = *x;", "MAX": "if (*x > *g) *g = *x;", "INC": "*g += *x;"}[mode]
+    seq.par_loop(seq.Kernel("void k(%s *x, %s *g) { %s }" % (ctype, ctype, op), "k"), s,
+                 d(seq.IdentityMap, seq.READ), g(getattr(seq, mode)))
+    assert g.data[0] == want
+
+
+def test_global_two_components():
+    s = seq.Set(4096, 2, "set2")
+    d = seq.Dat(s, np.arange(2 * 4096) + 1, np.uint32, "d2")
+    g = seq.Global(2, [0, 0], np.uint32, "g")
+    seq.par_loop(seq.Kernel("void k(unsigned int *x, unsigned int *g) { g[0] += x[0]; g[1] += x[1]; }", "k"),
+                 s, d(seq.IdentityMap, seq.READ), g(seq.INC))
+    v = np.arange(2 * 4096) + 1
+    assert g.data[0] == v[0::2].sum() and g.data[1] == v[1::2].sum()
