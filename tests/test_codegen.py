@@ -22,10 +22,10 @@ def host_op2():
     return op2
 
 
-def nvrtc_compile(spec):
+def nvrtc_compile(spec, extra=(), want_log=False):
     from pyop2_b200 import _lib
     src, layout, _ = codegen.generate(spec)
-    opts = codegen.nvrtc_options()
+    opts = codegen.nvrtc_options(extra=extra)
     arr = (C.c_char_p * len(opts))(*[o.encode() for o in opts])
     out, n = C.c_void_p(), C.c_uint64()
     log = C.create_string_buffer(1 << 16)
@@ -33,6 +33,8 @@ def nvrtc_compile(spec):
                                       C.byref(n), log, len(log))
     assert rc == 0, _lib.last_error() + "\n" + src
     _lib._lib.op2b_cubin_free(out)
+    if want_log:
+        return src, layout, n.value, log.value.decode()
     return src, layout, n.value
 
 
@@ -125,6 +127,49 @@ def test_airfoil_stubs(host_op2):
         assert n > 0
     for c in A.consts:
         c.remove_from_namespace()
+
+
+def test_airfoil_stub_resources(host_op2):
+    """ptxas's resource report for the airfoil stubs as the bench runs them
+    (res_calc in the staged form): no stack frame and no spills in any, and
+    the staged res_calc within 64 registers, so 8 CTAs of 128 threads stay
+    resident per SM."""
+    import re
+    from pyop2_b200 import b200, base
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import airfoil
+    op2 = host_op2
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    A = airfoil.build(op2, 6, 3, 0)
+    cfg.configure(staged_min_size=0)
+    try:
+        loops = {
+            "adt_calc": (A.k_adt, A.cells, [A.p_x(A.pcell[k], op2.READ) for k in range(4)] +
+                         [A.p_q(op2.IdentityMap, op2.READ), A.p_adt(op2.IdentityMap, op2.WRITE)]),
+            "res_calc": (A.k_res, A.edges, [A.p_x(A.pedge[0], op2.READ), A.p_x(A.pedge[1], op2.READ),
+                                            A.p_q(A.pevcell[0], op2.READ), A.p_q(A.pevcell[1], op2.READ),
+                                            A.p_adt(A.pecell[0], op2.READ), A.p_adt(A.pecell[1], op2.READ),
+                                            A.p_res(A.pevcell[0], op2.INC), A.p_res(A.pevcell[1], op2.INC)]),
+            "update": (A.k_update, A.cells, [A.p_qold(op2.IdentityMap, op2.READ),
+                                             A.p_q(op2.IdentityMap, op2.WRITE),
+                                             A.p_res(op2.IdentityMap, op2.RW),
+                                             A.p_adt(op2.IdentityMap, op2.READ),
+                                             op2.Global(1, 0.0, np.float64)(op2.INC)])}
+        for name, (k, s, args) in loops.items():
+            spec = b200.loop_spec(b200.ParLoop(k, s, *args))["spec"]
+            if name == "res_calc":
+                assert spec.mode == "staged"
+            _, _, _, log = nvrtc_compile(spec, extra=["-Xptxas=-v"], want_log=True)
+            m = re.search(r"(\d+) bytes stack frame, (\d+) bytes spill stores, (\d+) bytes spill loads", log)
+            assert m and m.groups() == ("0", "0", "0"), (name, log)
+            regs = int(re.search(r"Used (\d+) registers", log).group(1))
+            if name == "res_calc":
+                assert regs <= 64, (name, regs)
+    finally:
+        # the configuration is put back by conftest's autouse fixture
+        for c in A.consts:
+            c.remove_from_namespace()
 
 
 def test_atomic_mode_stubs(host_op2, golden_matrices):
