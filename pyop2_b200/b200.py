@@ -304,7 +304,11 @@ class Dat(DeviceDataMixin, base.Dat):
         if np.isscalar(other):
             yptr, ys = 0, float(base.as_type(other, self.dtype))
         elif isinstance(other, Dat):
-            if other.dtype != self.dtype or other.dataset.total_size * other.cdim != n:
+            if (other.dtype != self.dtype or other.dataset.total_size * other.cdim != n
+                    or other.dataset.dim != self.dataset.dim):
+                # the reference's semantics: numpy broadcasting of the two
+                # value arrays, whose result must fit this Dat's shape
+                # (test/unit/test_linalg.py:86-100 expect ValueError)
                 return False
             other._to_device()
             yptr, ys = other._device.ptr, 0.0

@@ -144,6 +144,21 @@ def test_dat_read_only_then_writable(op2, aset):
     assert (d.data_ro[0] == -100).all()
 
 
+def test_dat_arithmetic_shape_mismatch(op2):
+    """test/unit/test_linalg.py:86-100, 175-189: operands of the same size
+    but different shapes, (1, 2) and (2, 1) per element, raise ValueError
+    (the values broadcast to (2, 2) per element, which fits neither Dat).
+    Such operands take the host path, so this runs without a device."""
+    import operator
+    n = 8
+    for op in (operator.add, operator.sub, operator.mul, operator.truediv,
+               operator.iadd, operator.isub, operator.imul, operator.itruediv):
+        x2 = op2.Dat(op2.Set(n, (1, 2)), np.arange(2 * n) + 1.0, np.float64, "x")
+        y2 = op2.Dat(op2.Set(n, (2, 1)), np.arange(2 * n) + 1.0, np.float64, "y")
+        with pytest.raises(ValueError):
+            op(x2, y2)
+
+
 # -------------------------------------------------------------- Sparsity
 def test_sparsity_map_arguments(op2, m):
     with pytest.raises(TypeError):
