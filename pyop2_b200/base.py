@@ -481,7 +481,17 @@ class Dat(DataCarrier):
     def _check_shape(self, other):
         pass
 
+    def _int_division(self, op):
+        """The reference ran under Python 2, where ``/`` between integer
+        arrays (the other operand is first cast to this Dat's type,
+        pyop2/base.py:749-763) is floor division: an integer Dat divides
+        that way, in place too."""
+        return (op in (operator.truediv, operator.itruediv)
+                and np.issubdtype(self.dtype, np.integer))
+
     def _op(self, other, op):
+        if self._int_division(op):
+            op = np.floor_divide
         if np.isscalar(other):
             return _make_object('Dat', self.dataset, op(self.data_ro, as_type(other, self.dtype)),
                                 self.dtype)
@@ -490,6 +500,8 @@ class Dat(DataCarrier):
                             self.dtype)
 
     def _iop(self, other, op):
+        if self._int_division(op):
+            op = lambda a, b: np.floor_divide(a, b, out=a)   # noqa: E731
         d = self.data
         if np.isscalar(other):
             op(d, as_type(other, self.dtype))

@@ -159,6 +159,35 @@ def test_dat_arithmetic_shape_mismatch(op2):
             op(x2, y2)
 
 
+@pytest.mark.parametrize("name", ["add", "sub", "mul", "truediv"])
+def test_dat_arithmetic_mixed_types(op2, name):
+    """test/unit/test_linalg.py:118-148, 205-243: the result keeps the left
+    operand's type (the right one is cast to it first), in place too; an
+    integer Dat divides by floor division, as ``/`` between integer arrays
+    did under the reference's Python 2.  Mixed-type operands take the host
+    path, so this runs without a device."""
+    import operator
+    s = op2.Set(8)
+
+    def pair():
+        return (op2.Dat(s, np.arange(1, 9), np.float64, "y"),
+                op2.Dat(s, [-4, -3, -2, -1, 1, 2, 3, 4], np.int64, "yi"))
+    op, iop = getattr(operator, name), getattr(operator, "i" + name)
+    y, yi = pair()
+    assert op(y, yi).data.dtype == np.float64
+    assert op(yi, y).data.dtype == np.int64
+    y, yi = pair()
+    assert iop(y, yi).data.dtype == np.float64
+    y, yi = pair()
+    r = iop(yi, y)
+    assert r is yi and yi.data.dtype == np.int64
+    a, b = np.array([-4, -3, -2, -1, 1, 2, 3, 4]), np.arange(1, 9)
+    want = {"add": a + b, "sub": a - b, "mul": a * b, "truediv": a // b}[name]
+    np.testing.assert_array_equal(yi.data.ravel(), want)
+    y, yi = pair()
+    np.testing.assert_array_equal(op(yi, y).data.ravel(), want)
+
+
 # -------------------------------------------------------------- Sparsity
 def test_sparsity_map_arguments(op2, m):
     with pytest.raises(TypeError):
