@@ -413,3 +413,39 @@ def test_solver_parameters(op2):
     assert s.parameters["linear_solver"] == "gmres" and s.parameters["maximum_iterations"] == 25
     with pytest.raises(RuntimeError):
         op2.Solver(params, linear_solver="cgs")
+
+
+# ------------------------------------------------- Kernel / Sparsity caches
+def test_kernel_cache(op2):
+    """test/unit/test_caching.py:542-580: a Kernel is cached by its code and
+    name together."""
+    cache = base.Kernel._cache
+    cache.clear()
+    code = "void k(void *x) {}"
+    assert op2.Kernel(code, "k") is op2.Kernel(code, "k") and len(cache) == 1
+    cache.clear()
+    assert op2.Kernel(code, "k") is not op2.Kernel(code, "l") and len(cache) == 2
+    cache.clear()
+    assert op2.Kernel("void k(void *x) {}", "k") is not op2.Kernel("void l(void *x) {}", "k")
+    assert len(cache) == 2
+    cache.clear()
+    assert op2.Kernel("void k(void *x) {}", "k") is not op2.Kernel("void l(void *x) {}", "l")
+    assert len(cache) == 2
+
+
+def test_sparsity_cache(op2):
+    """test/unit/test_caching.py:582-651: Sparsities of the same Maps (in
+    any order of the pairs) are one object; other Maps give another; Mats on
+    one Sparsity share its pattern."""
+    s1, s2 = op2.Set(5), op2.Set(5)
+    m1 = op2.Map(s1, s2, 1, [0, 1, 2, 3, 4])
+    m2 = op2.Map(s1, s2, 1, [1, 2, 3, 4, 0])
+    assert op2.Sparsity(m1) is not op2.Sparsity(m2)
+    assert op2.Sparsity((m1, m2)) is not op2.Sparsity((m2, m1))
+    assert op2.Sparsity(((m1, m1), (m2, m2))) is not op2.Sparsity(((m2, m2), (m2, m2)))
+    assert op2.Sparsity(m1) is op2.Sparsity(m1)
+    assert op2.Sparsity((m1, m1)) is op2.Sparsity((m1, m1))
+    assert op2.Sparsity(((m1, m1), (m2, m2))) is op2.Sparsity(((m1, m1), (m2, m2)))
+    assert op2.Sparsity(((m1, m1), (m2, m2))) is op2.Sparsity(((m2, m2), (m1, m1)))
+    sp = op2.Sparsity((m1, m1))
+    assert op2.Mat(sp, "float64").sparsity is op2.Mat(sp, "float64").sparsity
