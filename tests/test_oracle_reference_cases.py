@@ -125,3 +125,49 @@ def test_global_two_components():
                  s, d(seq.IdentityMap, seq.READ), g(seq.INC))
     v = np.arange(2 * 4096) + 1
     assert g.data[0] == v[0::2].sum() and g.data[1] == v[1::2].sum()
+
+
+# -------------------------------------------- direct loops (test_direct_loop.py)
+def _direct(code, name, s, *args):
+    seq.par_loop(seq.Kernel(code, name), s, *args)
+
+
+def test_direct_loops():
+    n = 4096
+    elems, elems2 = seq.Set(n, 1, "elems"), seq.Set(n, 2, "elems2")
+    x = seq.Dat(elems, np.arange(n, dtype=np.uint32), np.uint32, "x")
+    _direct("void kernel_wo(unsigned int *x) { *x = 42; }", "kernel_wo", elems, x(seq.IdentityMap, seq.WRITE))
+    assert (x.data == 42).all()
+    x = seq.Dat(elems, np.arange(n, dtype=np.uint32), np.uint32, "x")
+    _direct("void kernel_rw(unsigned int *x) { (*x) = (*x) + 1; }", "kernel_rw", elems,
+            x(seq.IdentityMap, seq.RW))
+    assert x.data.sum() == n * (n + 1) // 2
+    x = seq.Dat(elems, np.arange(n, dtype=np.uint32), np.uint32, "x")
+    g = seq.Global(1, 0, np.uint32, "g")
+    _direct("void kgi(unsigned int *x, unsigned int *inc) { (*x) = (*x) + 1; (*inc) += (*x); }", "kgi",
+            elems, x(seq.IdentityMap, seq.RW), g(seq.INC))
+    assert g.data[0] == n * (n + 1) // 2
+    g = seq.Global(1, 10, np.uint32, "g")
+    _direct("void k1(unsigned int *inc) { (*inc) += 1; }", "k1", elems, g(seq.INC))
+    assert g.data[0] == n + 10
+    x = seq.Dat(elems, np.arange(n, dtype=np.uint32), np.uint32, "x")
+    kmax = "void kmax(unsigned int *x, unsigned int *g) { if (*g < *x) { *g = *x; } }"
+    for g0, want in ((0, n - 1), (2 * n, 2 * n)):
+        g = seq.Global(1, g0, np.uint32, "g")
+        _direct(kmax, "kmax", elems, x(seq.IdentityMap, seq.READ), g(seq.MAX))
+        assert g.data[0] == want
+    kmin = "void kmin(unsigned int *x, unsigned int *g) { if (*g > *x) { *g = *x; } }"
+    g = seq.Global(1, 1000, np.uint32, "g")
+    _direct(kmin, "kmin", elems, x(seq.IdentityMap, seq.READ), g(seq.MIN))
+    assert g.data[0] == 0
+    h = seq.Global(1, 1, np.uint32, "h")
+    _direct("void kgr(unsigned int *x, unsigned int *h) { (*x) += (*h); }", "kgr", elems,
+            x(seq.IdentityMap, seq.RW), h(seq.READ))
+    assert x.data.sum() == n * (n + 1) // 2
+    y = seq.Dat(elems2, np.zeros(2 * n, np.uint32), np.uint32, "y")
+    _direct("void k2d(unsigned int *x) { x[0] = 42; x[1] = 43; }", "k2d", elems2, y(seq.IdentityMap, seq.WRITE))
+    assert (y.data[:, 0] == 42).all() and (y.data[:, 1] == 43).all()
+    soa = seq.Dat(elems2, np.zeros(2 * n, np.uint32), np.uint32, "soa", soa=True)
+    _direct("void ksoa(unsigned int *x) { OP2_STRIDE(x, 0) = 42; OP2_STRIDE(x, 1) = 43; }", "ksoa", elems2,
+            soa(seq.IdentityMap, seq.WRITE))
+    assert (soa.data[:, 0] == 42).all() and (soa.data[:, 1] == 43).all()
