@@ -9,6 +9,7 @@ those tests state.  CPU only."""
 import numpy as np
 import pytest
 
+from conftest import py2_shuffle, reference_seed
 from oracle import seq
 
 NNODES = 4096
@@ -171,3 +172,49 @@ def test_direct_loops():
     _direct("void ksoa(unsigned int *x) { OP2_STRIDE(x, 0) = 42; OP2_STRIDE(x, 1) = 43; }", "ksoa", elems2,
             soa(seq.IdentityMap, seq.WRITE))
     assert (soa.data[:, 0] == 42).all() and (soa.data[:, 1] == 43).all()
+
+
+# ---------------------------------------- indirect loops (test_indirect_loop.py)
+def test_indirect_loops():
+    n = 4096
+    iterset, indset = seq.Set(n, 1, "iterset"), seq.Set(n, 1, "indset")
+    u = np.arange(n, dtype=np.int32)
+    py2_shuffle(u, reference_seed)
+    m = seq.Map(iterset, indset, 1, u, "iterset2indset")
+
+    def fresh():
+        return seq.Dat(indset, np.arange(n, dtype=np.uint32), np.uint32, "x")
+    x = fresh()
+    _direct("void kernel_wo(unsigned int *x) { *x = 42; }", "kernel_wo", iterset, x(m[0], seq.WRITE))
+    assert (x.data == 42).all()
+    x = fresh()
+    _direct("void kernel_rw(unsigned int *x) { (*x) = (*x) + 1; }", "kernel_rw", iterset, x(m[0], seq.RW))
+    assert x.data.sum() == n * (n + 1) // 2
+    unitset = seq.Set(1, 1, "unitset")
+    ud = seq.Dat(unitset, np.array([0], np.uint32), np.uint32, "u")
+    mu = seq.Map(iterset, unitset, 1, np.zeros(n, np.int32), "iterset2unitset")
+    _direct("void kernel_inc(unsigned int *x) { (*x) = (*x) + 1; }", "kernel_inc", iterset, ud(mu[0], seq.INC))
+    assert ud.data[0] == n
+    x = fresh()
+    g = seq.Global(1, 2, np.uint32, "g")
+    _direct("void kgr(unsigned int *x, unsigned int *g) { (*x) /= (*g); }", "kgr", iterset,
+            x(m[0], seq.RW), g(seq.READ))
+    assert x.data.sum() == sum(v // 2 for v in range(n))
+    x = fresh()
+    g = seq.Global(1, 0, np.uint32, "g")
+    _direct("void kgi(unsigned int *x, unsigned int *inc) { (*x) = (*x) + 1; (*inc) += (*x); }", "kgi",
+            iterset, x(m[0], seq.RW), g(seq.INC))
+    assert x.data.sum() == n * (n + 1) // 2 and g.data[0] == n * (n + 1) // 2
+    indset2 = seq.Set(n, 2, "indset2")
+    x2 = seq.Dat(indset2, np.zeros(2 * n, np.uint32), np.uint32, "x2")
+    m2 = seq.Map(iterset, indset2, 1, u, "iterset2indset2")
+    _direct("void k2(unsigned int *x) { x[0] = 42; x[1] = 43; }", "k2", iterset, x2(m2[0], seq.WRITE))
+    assert (x2.data[:, 0] == 42).all() and (x2.data[:, 1] == 43).all()
+    nedges = n - 1
+    nodes, edges = seq.Set(n, 1, "nodes"), seq.Set(nedges, 1, "edges")
+    nv = seq.Dat(nodes, np.arange(n, dtype=np.uint32), np.uint32, "node_vals")
+    ev = seq.Dat(edges, np.zeros(nedges, np.uint32), np.uint32, "edge_vals")
+    e2n = seq.Map(edges, nodes, 2, np.array([(i, i + 1) for i in range(nedges)]), "edge2node")
+    _direct("void ksum(unsigned int *a, unsigned int *b, unsigned int *e) { *e = *a + *b; }", "ksum", edges,
+            nv(e2n[0], seq.READ), nv(e2n[1], seq.READ), ev(seq.IdentityMap, seq.WRITE))
+    np.testing.assert_array_equal(ev.data.ravel(), np.arange(1, nedges * 2 + 1, 2))
