@@ -218,3 +218,31 @@ def test_indirect_loops():
     _direct("void ksum(unsigned int *a, unsigned int *b, unsigned int *e) { *e = *a + *b; }", "ksum", edges,
             nv(e2n[0], seq.READ), nv(e2n[1], seq.READ), ev(seq.IdentityMap, seq.WRITE))
     np.testing.assert_array_equal(ev.data.ravel(), np.arange(1, nedges * 2 + 1, 2))
+
+
+# ---------------------------------------------- Consts (test_constants.py)
+@pytest.mark.parametrize("dim,vals,body", [(1, 100, "*x = myconstant;"),
+                                           (2, (100, 200), "*x = myconstant[0] + myconstant[1];")])
+def test_const_read(dim, vals, body):
+    s = seq.Set(8)
+    d = seq.Dat(s, np.zeros(8, np.int32), np.int32)
+    c = seq.Const(dim, vals, "myconstant", np.int32)
+    try:
+        _direct("void k(int *x) { %s }" % body, "k", s, d(seq.IdentityMap, seq.WRITE))
+    finally:
+        c.remove_from_namespace()
+    assert (d.data == np.sum(vals)).all()
+
+
+def test_const_change_is_seen():
+    s = seq.Set(8)
+    d = seq.Dat(s, np.zeros(8, np.int32), np.int32)
+    c = seq.Const(1, 10, "myconstant", np.int32)
+    try:
+        _direct("void k(int *x) { *x = myconstant; }", "k", s, d(seq.IdentityMap, seq.WRITE))
+        assert (d.data == 10).all()
+        c.data[...] = 11
+        _direct("void k(int *x) { *x = myconstant; }", "k", s, d(seq.IdentityMap, seq.WRITE))
+        assert (d.data == 11).all()
+    finally:
+        c.remove_from_namespace()
