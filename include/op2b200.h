@@ -321,7 +321,12 @@ int op2b_cg_solve(uint64_t rowptr, uint64_t colidx, uint64_t vals, int32_t nrows
  * Replaces cuda.Mat.zero_rows / zero (pyop2/cuda.py:289-301) and PETSc
  * MatZeroRowsLocal (pyop2/petsc_base.py:131-135).
  * ---------------------------------------------------------------------- */
-int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx,
+/* Every stored entry of rows[0 .. nrows_zero) becomes 0 and each row's
+ * diagonal entry, where the pattern stores one, becomes diag.  mat_rows is
+ * the CSR's row count (rowptr holds mat_rows + 1 entries): a listed row
+ * outside [0, mat_rows), or elem_bytes other than 4 or 8, is rejected with
+ * OP2B_ERR_ARG before anything is allocated, copied or launched. */
+int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx, int32_t mat_rows,
                        const int32_t *rows, int32_t nrows_zero, double diag,
                        int32_t elem_bytes, uint64_t stream);
 
@@ -348,7 +353,8 @@ int op2b_mat_slots_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64
  * array compiled into the library (OP2B_ZERO_ROWS_STATIC_MAX rows, 256 KiB,
  * held on every GPU that loads the library until the process exits).
  *  - More than OP2B_ZERO_ROWS_STATIC_MAX rows is rejected with OP2B_ERR_ARG
- *    (split the list, or call op2b_mat_zero_rows).
+ *    (split the list, or call op2b_mat_zero_rows); so are rows outside
+ *    [0, mat_rows) and elem_bytes other than 4 or 8, before any copy or launch.
  *  - The first call on a device looks up the scratch array's device address
  *    (cudaGetSymbolAddress); make that first call before any stream capture.
  *  - All calls share the one scratch array, which keeps the last call's row
@@ -356,7 +362,7 @@ int op2b_mat_slots_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64
  *    and must be serialised by the caller.  The call returns after its work
  *    has finished on the stream. */
 #define OP2B_ZERO_ROWS_STATIC_MAX 65536
-int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_t colidx,
+int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_t colidx, int32_t mat_rows,
                               const int32_t *rows, int32_t nrows_zero, double diag,
                               int32_t elem_bytes, uint64_t stream);
 

@@ -4,7 +4,8 @@
 * ``oracle/_ref/libref_sparsity.so``: the reference's own
   ``pyop2/sparsity_utils.cxx`` compiled unmodified with g++ against the shim
   header ``oracle/ref_shim/op_lib_core.h``, when the reference sources are
-  present (``OP2B_REFERENCE`` or /root/reference).  The reference's build
+  present (``OP2B_REFERENCE``, else the read-only checkout this recipe was
+  written against).  The reference's build
   system is not used: its other native parts need OP2-Common and PETSc, which
   are not available, so only this one translation unit is compiled.
 * ``oracle/_ref/plan<ext>``: the reference's own ``pyop2/plan.pyx``
@@ -22,6 +23,10 @@ import sysconfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
+# Where the reference sources are read from.  This recipe (and the fixture
+# generators under tests/golden/, which import this name) is the only code
+# that reads them; nothing at test or bench time does.  When the directory is
+# absent the reference builds are skipped and the prebuilt files are used.
 REFERENCE = os.environ.get("OP2B_REFERENCE", "/root/reference")
 
 

@@ -641,12 +641,23 @@ class Mat(DeviceDataMixin, base.Mat):
         self._is_zero = True
 
     def zero_rows(self, rows, diag_val):
-        """Zero the given rows except the diagonal, set to diag_val."""
-        rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).ravel())
+        """Zero the given rows except the diagonal, set to diag_val.
+
+        Rows are CSR row numbers.  A row outside [0, number of rows) raises
+        IndexError before anything runs on the device, as PETSc's
+        zeroRowsLocal does for the reference (pyop2/petsc_base.py:131-135);
+        the library checks the same bound again before its launch."""
+        rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int64).ravel())
+        self._sparsity._ensure()
+        nrows = self._sparsity._lsize
+        if rows.size and (rows.min() < 0 or rows.max() >= nrows):
+            bad = rows[(rows < 0) | (rows >= nrows)][0]
+            raise IndexError("zero_rows: row %d outside [0, %d)" % (bad, nrows))
+        rows = rows.astype(np.int32)
         vals = self._device_values()
         self._is_zero = False
         call("op2b_mat_zero_rows", vals.ptr, self._sparsity._d_rowptr, self._sparsity._d_colidx,
-             rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, float(diag_val),
+             nrows, rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, float(diag_val),
              self.dtype.itemsize, 0)
 
     def _assemble(self):

@@ -27,6 +27,24 @@ __global__ void zero_rows_kernel(T *__restrict__ vals, const int32_t *__restrict
   }
 }
 
+// Host-side checks shared by both zero_rows entry points, made before any
+// allocation, copy or launch: the kernel indexes rowptr by every listed row,
+// so a row outside [0, mat_rows) would read and write outside the CSR arrays.
+// PETSc's MatZeroRowsLocal (pyop2/petsc_base.py:131-135) raises on such a row
+// as well.
+static int check_zero_rows_args(const char *who, int32_t mat_rows, const int32_t *rows,
+                                int32_t nrows_zero, int32_t elem_bytes) {
+  if (elem_bytes != 8 && elem_bytes != 4)
+    return set_error(OP2B_ERR_ARG, "%s: elem_bytes %d", who, elem_bytes);
+  if (mat_rows < 0) return set_error(OP2B_ERR_ARG, "%s: mat_rows %d", who, mat_rows);
+  if (!rows) return set_error(OP2B_ERR_ARG, "%s: rows is NULL", who);
+  for (int32_t i = 0; i < nrows_zero; ++i)
+    if (rows[i] < 0 || rows[i] >= mat_rows)
+      return set_error(OP2B_ERR_ARG, "%s: row %d (entry %d) outside [0, %d)", who, rows[i], i,
+                       mat_rows);
+  return OP2B_OK;
+}
+
 // ---- scratch of op2b_mat_zero_rows_static: the row list lives in a fixed
 // device array instead of memory allocated per call.  Every GPU that loads
 // this library holds OP2B_ZERO_ROWS_STATIC_MAX * 4 bytes (256 KiB) for it
@@ -59,19 +77,22 @@ static int zero_rows_scratch(int32_t **out) {
 using namespace op2b;
 
 extern "C" int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_t colidx,
-                                         const int32_t *rows, int32_t nrows_zero, double diag,
-                                         int32_t elem_bytes, uint64_t stream) {
-  OP2B_REQUIRE_INIT();
+                                         int32_t mat_rows, const int32_t *rows,
+                                         int32_t nrows_zero, double diag, int32_t elem_bytes,
+                                         uint64_t stream) {
+  // Arguments are checked before anything touches the device (before the
+  // initialisation check too, so the checks also run on a host with no GPU).
   if (nrows_zero <= 0) return OP2B_OK;
   if (nrows_zero > OP2B_ZERO_ROWS_STATIC_MAX)
     return set_error(OP2B_ERR_ARG,
                      "op2b_mat_zero_rows_static: %d rows exceed its fixed scratch of %d rows; "
                      "use op2b_mat_zero_rows or split the list", nrows_zero,
                      OP2B_ZERO_ROWS_STATIC_MAX);
-  if (elem_bytes != 8 && elem_bytes != 4)
-    return set_error(OP2B_ERR_ARG, "op2b_mat_zero_rows_static: elem_bytes %d", elem_bytes);
+  int rc = check_zero_rows_args("op2b_mat_zero_rows_static", mat_rows, rows, nrows_zero, elem_bytes);
+  if (rc) return rc;
+  OP2B_REQUIRE_INIT();
   int32_t *d_rows = nullptr;
-  int rc = zero_rows_scratch(&d_rows);
+  rc = zero_rows_scratch(&d_rows);
   if (rc) return rc;
   cudaStream_t s = stream_of(stream);
   // The whole list is overwritten before use: nothing in the scratch needs to
@@ -91,13 +112,17 @@ extern "C" int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_
 }
 
 extern "C" int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx,
-                                  const int32_t *rows, int32_t nrows_zero, double diag,
-                                  int32_t elem_bytes, uint64_t stream) {
-  OP2B_REQUIRE_INIT();
+                                  int32_t mat_rows, const int32_t *rows, int32_t nrows_zero,
+                                  double diag, int32_t elem_bytes, uint64_t stream) {
+  // Arguments are checked before anything touches the device (before the
+  // initialisation check too, so the checks also run on a host with no GPU).
   if (nrows_zero <= 0) return OP2B_OK;
+  int rc = check_zero_rows_args("op2b_mat_zero_rows", mat_rows, rows, nrows_zero, elem_bytes);
+  if (rc) return rc;
+  OP2B_REQUIRE_INIT();
   cudaStream_t s = stream_of(stream);
   int32_t *d_rows = nullptr;
-  int rc = dev_alloc((void **)&d_rows, sizeof(int32_t) * nrows_zero, s);
+  rc = dev_alloc((void **)&d_rows, sizeof(int32_t) * nrows_zero, s);
   if (rc) return rc;
   cudaError_t e = cudaMemcpyAsync(d_rows, rows, sizeof(int32_t) * nrows_zero, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) {
@@ -108,13 +133,9 @@ extern "C" int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colid
   if (elem_bytes == 8)
     zero_rows_kernel<double><<<grid, 256, 0, s>>>((double *)vals, (const int32_t *)rowptr,
                                                   (const int32_t *)colidx, d_rows, nrows_zero, diag);
-  else if (elem_bytes == 4)
+  else
     zero_rows_kernel<float><<<grid, 256, 0, s>>>((float *)vals, (const int32_t *)rowptr,
                                                  (const int32_t *)colidx, d_rows, nrows_zero, (float)diag);
-  else {
-    dev_free(d_rows, s);
-    return set_error(OP2B_ERR_ARG, "op2b_mat_zero_rows: elem_bytes %d", elem_bytes);
-  }
   e = cudaGetLastError();
   // The pinned/pageable host rows buffer may be released by the caller as
   // soon as this returns, so complete the copy first.

@@ -1,7 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own tests.
 
-Run in a container that has the reference sources (OP2B_REFERENCE, default
-/root/reference); the output files are committed so tests never read the
+Run in a container that has the reference sources (found where
+oracle/build.py looks for them: ``OP2B_REFERENCE``, else the build recipe's
+own location); the output files are committed so tests never read the
 reference at run time.  Sources read (as text, never imported or executed):
 
 * test/unit/test_matrices.py: the Sparsity CSR golden (:54-62), the 2-element
@@ -22,11 +23,13 @@ import json
 import os
 import pickle
 import re
+import sys
 
 import numpy as np
 
-REF = os.environ.get("OP2B_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.build import REFERENCE as REF  # noqa: E402
 
 
 def _fixture_body(src, name):

@@ -2,9 +2,9 @@
 own Plan class (pyop2/plan.pyx, translated by Cython and compiled by
 oracle/build.py; run through oracle/reference.py) for a set of seeded loops.
 
-Run in a container that has the reference sources (OP2B_REFERENCE, default
-/root/reference); the output is committed so tests never need the reference
-at run time.  Each case stores its loop description (Map values, Dat sizes,
+Run in a container that has the reference sources (found where
+oracle/build.py looks for them); the output is committed so tests never need
+the reference at run time.  Each case stores its loop description (Map values, Dat sizes,
 the unwound arguments) and every array and scalar the reference Plan holds
 (partition, staging, thread and block colouring).
 """

@@ -47,3 +47,21 @@ def test_calls_before_init_fail_cleanly(lib):
     rc = _lib._lib.op2b_malloc(C.byref(p), 16)
     assert rc != 0
     assert "op2b_init" in _lib.last_error()
+
+
+@pytest.mark.parametrize("name", ["op2b_mat_zero_rows", "op2b_mat_zero_rows_static"])
+def test_zero_rows_rejects_bad_rows_on_the_host(lib, name):
+    """A listed row outside [0, mat_rows), or an element size other than 4 or
+    8, is rejected before the library touches the device: the check runs even
+    here, with no GPU and no op2b_init, and the device pointers (all 0) are
+    never used."""
+    import ctypes as C
+    import numpy as np
+    from pyop2_b200 import _lib
+    fn = getattr(_lib._lib, name)
+    for rows, elem_bytes, what in (([0, 3, 10], 8, "row 10"), ([-1], 8, "row -1"),
+                                   ([2], 2, "elem_bytes 2")):
+        r = np.asarray(rows, dtype=np.int32)
+        rc = fn(0, 0, 0, 10, r.ctypes.data_as(C.POINTER(C.c_int32)), r.size, 1.0, elem_bytes, 0)
+        assert rc == 3, (rows, rc)       # OP2B_ERR_ARG
+        assert what in _lib.last_error()

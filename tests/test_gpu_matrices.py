@@ -158,6 +158,19 @@ def test_zero_rows(op2, P):
     assert_allclose(P.mat.values, expected, 1e-5)
 
 
+def test_zero_rows_out_of_range_raises_before_launch(op2, P):
+    """A row outside the matrix raises IndexError on the host (PETSc's
+    zeroRowsLocal raises for the reference, pyop2/petsc_base.py:131-135) and
+    leaves every value as it was."""
+    op2.par_loop(P.K["mass"], P.elements(3, 3), P.mat((P.elem_node[op2.i[0]], P.elem_node[op2.i[1]]), op2.INC),
+                 P.coords(P.elem_vnode, op2.READ))
+    before = P.mat.array.copy()
+    for rows in ([4], [0, -1], [1, 2, 99]):
+        with pytest.raises(IndexError):
+            P.mat.zero_rows(rows, 1.0)
+    np.testing.assert_array_equal(P.mat.array, before)
+
+
 def test_zero_vector_matrix(op2, P):
     P.vecmat.zero()
     assert_allclose(P.vecmat.values, np.zeros((8, 8)), 1e-14)

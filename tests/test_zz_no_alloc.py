@@ -42,11 +42,27 @@ def _values(sp, seed):
     return np.random.default_rng(seed).standard_normal(sp.nz)
 
 
-def _run(lib, name, buf, sp, rows, diag):
+def _run(lib, name, buf, sp, rows, diag, elem_bytes=8):
     rows = np.ascontiguousarray(rows, dtype=np.int32)
-    rc = getattr(lib, name)(buf.ptr, sp._d_rowptr, sp._d_colidx,
-                            rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, float(diag), 8, 0)
+    rc = getattr(lib, name)(buf.ptr, sp._d_rowptr, sp._d_colidx, sp._lsize,
+                            rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, float(diag),
+                            elem_bytes, 0)
     return rc
+
+
+def _pool():
+    """The device's default stream-ordered memory pool, which the library's
+    allocating entry points draw from (cudaMallocAsync)."""
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    assert err == rt.cudaError_t.cudaSuccess
+    return rt, pool
+
+
+def _pool_attr(rt, pool, attr):
+    err, v = rt.cudaMemPoolGetAttribute(pool, attr)
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(v)
 
 
 def test_zero_rows_static_matches_allocating_entry_point(op2):
@@ -90,6 +106,46 @@ def test_zero_rows_static_rejects_oversized_lists(op2):
     too_many = np.zeros(65536 + 1, dtype=np.int32)
     assert _run(lib, "op2b_mat_zero_rows_static", buf, sp, too_many, 1.0) != 0
     assert "65536" in _lib.last_error()
+    # rows outside the matrix and unsupported element sizes are rejected on
+    # the host, before anything is copied or launched
+    assert _run(lib, "op2b_mat_zero_rows_static", buf, sp, [0, nrows], 1.0) != 0
+    assert "outside" in _lib.last_error()
+    assert _run(lib, "op2b_mat_zero_rows_static", buf, sp, [-5], 1.0) != 0
+    assert _run(lib, "op2b_mat_zero_rows_static", buf, sp, [0], 1.0, elem_bytes=2) != 0
+    assert "elem_bytes" in _lib.last_error()
     out = np.empty_like(vals)
     buf.to_host(out)
     np.testing.assert_array_equal(out, vals)
+
+
+def test_zero_rows_static_allocates_nothing(op2):
+    """Calls of the allocation-free entry point take nothing from the
+    stream-ordered pool: its high-water mark, reset before the calls, stays at
+    or below the memory in use before them.  The allocating entry point, run
+    the same way, does raise it (so the probe sees allocations)."""
+    import torch
+    from cuda.bindings.driver import cuuint64_t
+    from pyop2_b200 import _lib, b200
+    lib = _lib._lib
+    rt, pool = _pool()
+    used = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent
+    high = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
+    sp, nrows = _pattern(op2)
+    vals = _values(sp, 4)
+    buf = b200.DeviceBuffer(vals.nbytes)
+    buf.from_host(vals)
+    rows = np.arange(0, nrows, 3)
+    assert _run(lib, "op2b_mat_zero_rows_static", buf, sp, rows, 1.0) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+
+    def peak_over(name):
+        in_use = _pool_attr(rt, pool, used)
+        err, = rt.cudaMemPoolSetAttribute(pool, high, cuuint64_t(0))
+        assert err == rt.cudaError_t.cudaSuccess
+        for diag in (2.0, 3.0, 4.0):
+            assert _run(lib, name, buf, sp, rows, diag) == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        return _pool_attr(rt, pool, high) - in_use
+
+    assert peak_over("op2b_mat_zero_rows_static") <= 0
+    assert peak_over("op2b_mat_zero_rows") > 0
