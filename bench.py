@@ -12,14 +12,24 @@ time of the step.
 * ``value``: the step replayed as a CUDA graph recorded through the op2 API,
   inputs resident in HBM, L2 flushed (256 MB write) before every step; each
   step timed by its own pair of CUDA events on the op2 stream, summed.
-* ``e2e``: the same iterations run end to end through the public op2 API from
-  pinned host arrays: declaring the problem uploads maps and Dats (H2D inside
-  the timed region), every iteration issues its 9 par_loops from Python and
-  reads rms back (D2H), and the final solution is read back.
+* ``e2e``: the configuration's 100 iterations run end to end through the
+  public op2 API from pinned host arrays: declaring the problem uploads maps
+  and Dats (H2D inside the timed region), every iteration issues its 9
+  par_loops from Python and reads rms back (D2H), and the final solution is
+  read back.
 * ``roofline``: res_calc, the largest loop, timed alone with CUDA events per
-  launch (all its colour launches) after an L2 flush.
+  launch after an L2 flush.
 * ``cpu_baseline``: the oracle's restated OpenMP backend (pyop2/openmp.py) on
-  the host cores, a bounded sample of the same mesh.
+  all host cores (a bounded sample of the same mesh), beside the sequential
+  oracle (pyop2/sequential.py) on one core over the end-to-end run's 100
+  iterations and over the P2 1024 x 1024 FP64 assembly.
+* ``parity``: the end-to-end run's final q and its 100 rms values against the
+  sequential oracle's (max relative error; the bar is 1e-12).
+* ``mat_assembly`` / ``batching`` / ``serving``: summaries of the other
+  legs (Mat assembly nnz/s and fraction of HBM peak with the P2 errors
+  against the sequential oracle; batched and served requests/s against the
+  plain per-loop drop-in).  The full figures go to stderr (``bench
+  detail:``) and to ``--detail FILE``.
 
 ``--impl reference`` times the reference's CPU implementation of the path
 (the restated OpenMP backend; the Python 2 reference itself cannot run here)
@@ -177,12 +187,13 @@ def _peaks():
 
 
 # ----------------------------------------------------------------- CPU leg
+E2E_ITERS = 100   # the airfoil configuration's iteration count
+
+
 def workload_config(ws):
     """The workload both arms run (rank-independent description)."""
-    return {"workload": "airfoil 1200x600 (720000 cells, 1438200 edges, 3600 boundary "
-                        "edges), permuted numbering, FP64, one outer iteration (9 "
-                        "par_loops) per step",
-            "bytes_per_step": _bytes()["iteration"], "global_batch": ws, "seq_len": 0,
+    return {"workload": "airfoil %dx%d permuted FP64, 9 par_loops/step" % (NX, NY),
+            "bytes_per_step": _bytes()["iteration"],
             "parallelism": "replicas" if ws > 1 else "single"}
 
 
@@ -213,8 +224,60 @@ def cpu_airfoil(seconds=20.0, max_iters=50, threads=None, warmup=1):
             iters += 1
     finally:
         seq.par_loop = orig
+        seq._CONSTS.clear()
     bpi = _bytes()["iteration"]
     return bpi * iters / loop_time[0] / 1e9, iters, nthreads, loop_time[0]
+
+
+def cpu_sequential_airfoil(iters):
+    """The sequential oracle (one host thread) over ``iters`` outer
+    iterations of the full mesh from the initial state: element-loop time
+    summed (code generation excluded).  Returns (GB/s, loop seconds, final q,
+    per-iteration rms sums): the timed run doubles as the checker of the
+    GPU's end-to-end run of the same iterations."""
+    from oracle import seq
+    from pyop2_b200.workloads import airfoil
+    from pyop2_b200.workloads.meshes import airfoil_grid
+    seq._CONSTS.clear()
+    grid = airfoil_grid(NX, NY, SEED)
+    A = airfoil.build(seq, NX, NY, SEED, grid=grid)
+    loop_time = [0.0]
+    orig = seq.par_loop
+
+    def timed(*a, **k):
+        return orig(*a, timer=lambda dt: loop_time.__setitem__(0, loop_time[0] + dt), **k)
+    seq.par_loop = timed
+    rms = []
+    try:
+        for _ in range(iters):
+            rms.append(float(airfoil.iteration(seq, A).data[0]))
+    finally:
+        seq.par_loop = orig
+        seq._CONSTS.clear()
+    return (_bytes()["iteration"] * iters / loop_time[0] / 1e9, loop_time[0], A.p_q.data.copy(),
+            np.array(rms))
+
+
+def cpu_sequential_p2(n=1024):
+    """The sequential oracle's FP64 P2 stiffness + mass assembly on the
+    n x n grid, timed (element loops only).  Returns (nnz per second over
+    both Mats, seconds, K values, M values, nnz): the values are the checker
+    of the GPU's FP64 and precision-form assemblies."""
+    from oracle import seq
+    from pyop2_b200.workloads import fem
+    O = fem.build_p2(seq, n, seed=0)
+    t = [0.0]
+    orig = seq.par_loop
+
+    def timed(*a, **k):
+        return orig(*a, timer=lambda dt: t.__setitem__(0, t[0] + dt), **k)
+    seq.par_loop = timed
+    try:
+        fem.assemble_p2(seq, O)
+    finally:
+        seq.par_loop = orig
+    nz = O.sparsity.nz
+    return 2 * nz / t[0], t[0], O.K.array, O.M.array, nz
 
 
 def run_reference(args, ws, rank, local):
@@ -222,9 +285,7 @@ def run_reference(args, ws, rank, local):
     if rank != 0:
         return 0
     t0 = time.time()
-    vals = []
     steps = max(1, args.steps)
-    bpi = _bytes()["iteration"]
     # bounded: about 60 s of element-loop work in total
     gbs, iters, nthreads, secs = cpu_airfoil(seconds=min(60.0, 2.0 * steps), max_iters=steps,
                                              warmup=args.warmup)
@@ -237,8 +298,9 @@ def run_reference(args, ws, rank, local):
                            timing="host wall clock around each element loop, rank 0 only"),
             "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads,
                              "kind": "port",
-                             "sample": "%d airfoil iterations of the 1200x600 mesh, restated "
-                                       "OpenMP backend (oracle), element loops timed" % iters},
+                             "sample": "%d airfoil iterations of the %dx%d mesh, restated "
+                                       "OpenMP backend (oracle), element loops timed"
+                                       % (iters, NX, NY)},
             "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "wall_s": round(time.time() - t0, 1)}
@@ -389,15 +451,17 @@ def run_gpu(args, ws, rank, local):
                    and not args.no_permute and not args.block_size and not args.part_size)
     traffic = _traffic_from_profile() if default_run else None
 
-    e2e_val = e2e_ms = h2d = d2h = None
-    e2e_iters = args.steps
+    e2e_val = e2e_ms = h2d = d2h = q_out = None
+    e2e_iters = E2E_ITERS
     rms_hist = [0.0]
     if not args.no_e2e:
-        # ---------------- end to end through the public API
+        # ---------------- end to end through the public API: the
+        # configuration's 100 iterations from the initial state, the problem
+        # declared from pinned host arrays inside the timed region
         for c in list(base.Const._defs):
             c.remove_from_namespace()
         del graph
-        e2e_iters = args.steps
+
         def pin(src):
             dst = b200.pinned_empty(src.shape, src.dtype)
             dst[...] = src
@@ -429,10 +493,35 @@ def run_gpu(args, ws, rank, local):
                                                    "p_bound", "x")) +
                sum(v.nbytes for v in host.values()) + e2e_iters * 2 * 8)
         d2h = e2e_iters * 2 * 8 + q_out.nbytes
+        q_out = np.array(q_out)
+
+    # ---------------- CPU baseline (rank 0 at N=1): the restated OpenMP
+    # backend on all host cores, the sequential oracle on one core over the
+    # same 100 iterations as the end-to-end run (its results are the parity
+    # checker of that run), and the sequential FP64 P2 assembly (the checker
+    # of the GPU's P2 assemblies)
+    cpu = parity = p2_ref = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        gbs, iters, nthreads, secs = cpu_airfoil(seconds=args.cpu_seconds, max_iters=50)
+        seq_iters = e2e_iters if q_out is not None else 3
+        s_gbs, s_secs, s_q, s_rms = cpu_sequential_airfoil(seq_iters)
+        p2_nnz_s, p2_s, p2_k, p2_m, p2_nz = cpu_sequential_p2()
+        p2_ref = (p2_k, p2_m)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": "OpenMP port, %d iters" % iters,
+               "sequential": {"value": round(s_gbs, 3), "cores": 1, "iters": seq_iters,
+                              "p2_nnz_per_s": float("%.3g" % p2_nnz_s)}}
+        if q_out is not None:
+            rel = np.abs(np.array(rms_hist) - s_rms) / np.maximum(np.abs(s_rms), 1e-300)
+            parity = {"iters": seq_iters,
+                      "max_rel_q": float(np.abs(q_out - s_q).max() / np.abs(s_q).max()),
+                      "max_rel_rms": float(rel.max()), "tol": 1e-12}
+        del s_q
 
     assembly = None
     if not args.no_assembly:
-        assembly = bench_assembly(op2, b200)
+        assembly = bench_assembly(op2, b200, p2_ref=p2_ref)
+    del p2_ref
     batching = None
     if args.batch_meshes > 0:
         batching = bench_batching(op2, b200, args.batch_meshes)
@@ -440,49 +529,51 @@ def run_gpu(args, ws, rank, local):
     if args.serve_requests > 0:
         serving = bench_serving(op2, b200, args.serve_requests, args.serve_rate)
     solve = None
-    if not args.no_solve:
+    if args.solve:
         solve = bench_solve(op2, b200)
 
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
-        gbs, iters, nthreads, secs = cpu_airfoil(seconds=args.cpu_seconds, max_iters=50)
-        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
-               "sample": "%d iterations of the full 1200x600 airfoil mesh (%.1f s of element "
-                         "loops), restated OpenMP backend (oracle)" % (iters, secs)}
     line = {
         "metric": "par_loop achieved HBM GB/s (airfoil chain)",
         "value": round(value, 2), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": dict(workload_config(ws),
-                       l2="flushed (256 MB write) before every step",
-                       timing="CUDA graph replay, CUDA events per step on the op2 stream, "
-                              "max over ranks"),
+        "config": dict(workload_config(ws), l2="256 MB flush before each step"),
         "gpu_launches": launches * args.steps,
-        "roofline": {"kernel": "res_calc (%s)" % res_form,
-                     "bound": "hbm",
+        "roofline": {"kernel": "res_calc", "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes": res_bytes, "avg_ms": round(res_avg, 4),
-                     "traffic": traffic},
+                     "frac": round(achieved / peak, 4), "traffic": traffic},
         "e2e": None if e2e_val is None else {
             "value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": int(h2d // e2e_iters),
-            "d2h_bytes_per_step": int(d2h // e2e_iters), "iterations": e2e_iters,
-            "ms": round(e2e_ms, 3)},
-        "clocks": clocks,
-        "loops": breakdown,
-        "res_calc_partition_build_ms": partition_ms,
-        "mat_assembly": assembly,
-        "batching": batching,
-        "serving": serving,
-        "solve": solve,
-        "inc_mode": op2_cfg_inc_mode(),
-        "check": {"rms": final_rms, "rms_e2e_last": float(np.sqrt(rms_hist[-1] / grid.ncells))},
+            "d2h_bytes_per_step": int(d2h // e2e_iters), "iters": e2e_iters},
+        "clocks": {k: clocks.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if parity is not None:
+        line["parity"] = {k: (float("%.3g" % v) if isinstance(v, float) else v)
+                          for k, v in parity.items()}
+    if assembly is not None:
+        line["mat_assembly"] = assembly["summary"]
+    if batching is not None:
+        line["batching"] = batching["summary"]
+    if serving is not None:
+        line["serving"] = serving["summary"]
+    detail = {"peak_kind": peak_kind, "res_calc_form": res_form, "res_calc_avg_ms": round(res_avg, 4),
+              "res_calc_algorithmic_bytes": res_bytes, "loops": breakdown,
+              "res_calc_partition_build_ms": partition_ms, "inc_mode": op2_cfg_inc_mode(),
+              "clocks": clocks, "e2e_ms": e2e_ms, "cpu_baseline": cpu, "parity": parity,
+              "rms_graph_final": final_rms,
+              "mat_assembly": assembly, "batching": batching, "serving": serving,
+              "solve": solve}
     if rank == 0:
+        # the full figures go to stderr (and to --detail), the one bench line
+        # to stdout
+        text = json.dumps(detail, default=str)
+        sys.stderr.write("bench detail: " + text + "\n")
+        if args.detail:
+            with open(args.detail, "w") as f:
+                f.write(text + "\n")
         print(json.dumps(line))
     d.close()
     return 0
@@ -599,7 +690,11 @@ def bench_batching(op2, b200, nmesh, reps=5, seed=0):
         for a, b in zip(got[i], (P.mat.array, P.stiff.array, P.b.data_ro)):
             err = max(err, float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)))
     g.close()
-    return {"meshes": nmesh, "elements": elements, "nnz_per_mat": nnz,
+    peak, _ = _peaks()
+    summary = {"req_per_s_ratio": round(plain_ms / batched_ms, 1),
+               "frac": round(nbytes / (batched_ms * 1e-3) / 1e9 / peak, 3),
+               "err_vs_plain": float("%.3g" % err)}
+    return {"summary": summary, "meshes": nmesh, "elements": elements, "nnz_per_mat": nnz,
             "loops_per_mesh": 3, "algorithmic_bytes": nbytes,
             "batched_ms": round(batched_ms, 4),
             "batched_req_per_s": round(nmesh / (batched_ms * 1e-3), 1),
@@ -695,7 +790,13 @@ def bench_serving(op2, b200, nreq, rate, seed=0, n_p1=16, n_quad=16):
     del consts
     for c in list(base.Const._defs):
         c.remove_from_namespace()
-    return {"trace": {"requests": nreq, "rate_per_s": rate, "p1_meshes": n_p1,
+    ratio = round(s_eng["req_per_s"] / s_plain["req_per_s"], 2)
+    summary = {"req_per_s_ratio": ratio, "req_per_s": s_eng["req_per_s"],
+               "p50_ms": s_eng["p50_ms"], "p99_ms": s_eng["p99_ms"],
+               "plain_p99_ms": s_plain["p99_ms"],
+               "err_vs_plain": float("%.3g" % max(err.values()))}
+    return {"summary": summary,
+            "trace": {"requests": nreq, "rate_per_s": rate, "p1_meshes": n_p1,
                       "quad_meshes": n_quad, "iters_per_chain": 10, "hbm_budget_gb": 120,
                       "p1_triangles": [int(2 * v[1] * v[2]) for v in pool.values() if v[0] == "p1"],
                       "quad_cells": [int(v[1] * v[2]) for v in pool.values() if v[0] == "quad"]},
@@ -713,9 +814,9 @@ def bench_solve(op2, b200, n=1024, reps=20):
     grid (48.25 M nonzeros at n = 1024), Jacobi-preconditioned CG from x = 0
     to rtol 1e-8 (op2.solve), and the CSR SpMV alone.  SpMV algorithmic
     bytes: values and column indices (12 B per nonzero), row pointers, x
-    read once, y written once.  CPU leg: the oracle's numpy SpMV on the same
-    matrix (a bounded sample of 3 products)."""
-    from oracle import linalg
+    read once, y written once.  The residual of the solution is checked with
+    scipy's CSR product on the host."""
+    import scipy.sparse
     from pyop2_b200._lib import call
     from pyop2_b200.workloads import fem
     P = fem.build_p2(op2, n, seed=0)
@@ -738,8 +839,8 @@ def bench_solve(op2, b200, n=1024, reps=20):
         e1.synchronize()
         ts.append(e0.elapsed_ms(e1))
     solve_ms = statistics.median(ts)
-    resid = float(np.abs(linalg.csr_matvec(sp.rowptr, sp.colidx, P.M.array, x.data_ro.ravel())
-                         - rhs).max() / np.abs(rhs).max())
+    host_m = scipy.sparse.csr_matrix((P.M.array, sp.colidx, sp.rowptr), shape=(rows, rows))
+    resid = float(np.abs(host_m @ x.data_ro.ravel() - rhs).max() / np.abs(rhs).max())
     vals = P.M._device_values().ptr
     xd, yd = b._device.ptr, b200.DeviceBuffer(rows * 8)
 
@@ -751,11 +852,6 @@ def bench_solve(op2, b200, n=1024, reps=20):
         by_group[group] = _timed(spmv, reps, b200)
     spmv_ms = by_group[0]
     spmv_bytes = nnz * 12 + (rows + 1) * 4 + rows * 16
-    mvals = P.M.array
-    t0 = time.time()
-    for _ in range(3):
-        linalg.csr_matvec(sp.rowptr, sp.colidx, mvals, rhs)
-    cpu_s = (time.time() - t0) / 3
     peak, _ = _peaks()
     return {"matrix": "P2 mass %dx%d" % (n, n), "rows": rows, "nnz": nnz,
             "solver": "cg + jacobi, rtol 1e-8, x0 = 0", "iterations": solver.iterations,
@@ -765,18 +861,27 @@ def bench_solve(op2, b200, n=1024, reps=20):
             "spmv_ms": round(spmv_ms, 4), "spmv_GBps": round(spmv_bytes / (spmv_ms * 1e-3) / 1e9, 1),
             "spmv_frac_of_measured_peak": round(spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak, 3),
             "spmv_algorithmic_bytes": spmv_bytes,
-            "spmv_ms_by_lanes_per_row": {str(k): round(v, 4) for k, v in by_group.items()},
-            "cpu_spmv": {"GBps": round(spmv_bytes / cpu_s / 1e9, 2), "cores": 1,
-                         "kind": "port", "sample": "3 numpy CSR products (oracle)"}}
+            "spmv_ms_by_lanes_per_row": {str(k): round(v, 4) for k, v in by_group.items()}}
 
 
-def bench_assembly(op2, b200, reps=5):
-    """Mat assembly legs: P1 256x256 mass + RHS and P2 1024x1024
-    stiffness + mass in FP64 and in the precision form (FP32 element math and
-    geometry, FP64 Kahan-compensated accumulation)."""
+def bench_assembly(op2, b200, reps=5, p2_ref=None):
+    """Mat assembly legs.
+
+    * P1 256 x 256 mass + RHS (FP64), the drop-in's default forms.
+    * P2 1024 x 1024 stiffness + mass on one Sparsity: FP64 (default atomic
+      form), FP64 in the two-phase form (adds in the sequential order), and
+      the precision form (FP32 element math and geometry differences from
+      FP64 coordinates, FP64 Kahan-compensated two-phase accumulation).
+
+    Bytes: P1 per loop (map, coordinates, values read and written, CSR);
+    P2 K+M on one Sparsity (map and coordinates once, CSR once, both Mats'
+    values read and written: 1.871 GB).  ``p2_ref`` = the sequential
+    oracle's FP64 (K, M) values (from the CPU-baseline leg): each P2 form's
+    max relative error per Mat is stated against them."""
     from pyop2_b200 import base
     from pyop2_b200 import configuration as cfg
     from pyop2_b200.workloads import fem
+    peak, _ = _peaks()
     out = {}
     for c in list(base.Const._defs):
         c.remove_from_namespace()
@@ -796,55 +901,65 @@ def bench_assembly(op2, b200, reps=5):
     def rhs():
         op2.par_loop(P.k_rhs, P.elements(3), P.b(P.elem_node[op2.i[0]], op2.INC),
                      P.coords(P.elem_vnode, op2.READ), P.f(P.elem_node, op2.READ))
+
+    def both():
+        mass()
+        rhs()
     ms_m = _timed(mass, reps, b200)
     ms_r = _timed(rhs, reps, b200)
+    ms_b = _timed(both, reps, b200)
     bm = fem.assembly_bytes(P.n_elem, 3, P.n_nodes, nz)
     br = fem.rhs_bytes(P.n_elem, P.n_nodes)
     out["p1_256"] = {"nnz": nz, "elements": P.n_elem, "sparsity_build_s": round(sp_s, 4),
                      "mass_ms": round(ms_m, 4), "mass_nnz_per_s": round(nz / (ms_m * 1e-3), 1),
                      "mass_GBps": round(bm / (ms_m * 1e-3) / 1e9, 1),
                      "rhs_ms": round(ms_r, 4), "rhs_GBps": round(br / (ms_r * 1e-3) / 1e9, 1),
+                     "mass_rhs_ms": round(ms_b, 4),
+                     "mass_rhs_GBps": round((bm + br) / (ms_b * 1e-3) / 1e9, 1),
                      "mass_mode": _loop_mode(P.k_mass.name), "rhs_mode": _loop_mode(P.k_rhs.name)}
     del P
-    # ---- P2, FP64 and precision form
+    # ---- P2: the FP64 drop-in, its two-phase form, the precision form
     res = {}
-    vals = {}
     inc0 = cfg.cfg['inc_mode']
-    # default form (atomic accumulation), then the deterministic two-phase
-    # form that sums in the sequential backend's order (inc_mode 'lma'), with
-    # Kahan for FP32 element math (the precision form)
-    variants = (("f64", "atomic", False), ("f32", "atomic", False),
-                ("f64", "lma", False), ("f32", "lma", True), ("f32g", "lma", True))
+    variants = (("f64", None, False), ("f64", "lma", False), ("f32", "lma", True))
     for prec, mode, kahan in variants:
         tag = prec + ("_lma" if mode == "lma" else "") + ("_kahan" if kahan else "")
-        cfg.configure(kahan=kahan, inc_mode=mode)
+        cfg.configure(kahan=kahan, inc_mode=mode or inc0)
         Q = fem.build_p2(op2, 1024, seed=0, precision=prec)
         t0 = time.time()
         nz = Q.sparsity.nz
         sp_s = time.time() - t0
-        fem.assemble_p2(op2, Q)   # compile, incidence, warm-up: values once
+        fem.assemble_p2(op2, Q)   # compile, slot tables or incidence, values once
         b200.synchronize()
-        vals[tag] = (Q.K.array, Q.M.array)
+        if p2_ref is not None:
+            errs = [float(np.abs(got - ref).max() / np.abs(ref).max())
+                    for got, ref in zip((Q.K.array, Q.M.array), p2_ref)]
+        else:
+            errs = [None, None]
         ms = _timed(lambda: fem.assemble_p2(op2, Q), reps, b200)
-        nbytes = fem.assembly_bytes(Q.n_elem, 6, Q.n_dofs, nz, 4 if prec == "f32g" else 8, nmats=2)
+        nbytes = fem.km_bytes(Q.n_elem, 6, Q.n_dofs, nz)
         res[tag] = {"nnz": nz, "elements": Q.n_elem, "sparsity_build_s": round(sp_s, 3),
                     "K_plus_M_ms": round(ms, 3), "nnz_per_s": round(2 * nz / (ms * 1e-3), 1),
                     "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "algorithmic_bytes": nbytes,
-                    "kahan": kahan, "element_math": "f64" if prec == "f64" else "f32",
-                    "coordinates": "f32" if prec == "f32g" else "f64",
-                    "mode": "two-phase (sequential order)" if mode == "lma" else "atomic"}
+                    "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
+                    "kahan": kahan, "element_math": prec, "mode": mode or inc0,
+                    "max_rel_err_K_vs_oracle": errs[0], "max_rel_err_M_vs_oracle": errs[1]}
         del Q
     cfg.configure(kahan=False, inc_mode=inc0)
-    for tag in vals:
-        if tag == "f64_lma":
-            continue
-        for i, nm in enumerate(("K", "M")):
-            a, b = vals[tag][i], vals["f64_lma"][i]
-            res[tag]["max_rel_err_" + nm] = float(np.abs(a - b).max() / np.abs(b).max())
-    res["error_reference"] = ("max|A - A_f64| / max|A_f64| against the FP64 two-phase assembly of "
-                              "the same Mat, which adds in the sequential oracle's order (equal to it "
-                              "bit for bit)")
     out["p2_1024"] = res
+    p1, f64, prec = out["p1_256"], res["f64"], res["f32_lma_kahan"]
+
+    def e(v):
+        return None if v is None else float("%.3g" % v)
+    out["summary"] = {
+        "p1_nnz_per_s": float("%.3g" % p1["mass_nnz_per_s"]),
+        "p1_frac": round(p1["mass_rhs_GBps"] / peak, 3),
+        "p2_nnz_per_s": float("%.3g" % f64["nnz_per_s"]), "p2_frac": f64["frac"],
+        "p2_err": e(max(f64["max_rel_err_K_vs_oracle"] or 0, f64["max_rel_err_M_vs_oracle"] or 0)
+                    if p2_ref is not None else None),
+        "prec_frac": prec["frac"],
+        "prec_err": e(max(prec["max_rel_err_K_vs_oracle"], prec["max_rel_err_M_vs_oracle"])
+                      if p2_ref is not None else None)}
     return out
 
 
@@ -893,7 +1008,8 @@ def main(argv=None):
                    help="mean Poisson arrival rate of the serving leg (requests/s)")
     p.add_argument("--serving-only", action="store_true",
                    help="run only the serving leg and print its figures")
-    p.add_argument("--no-solve", action="store_true", help="skip the linear-solve leg")
+    p.add_argument("--solve", action="store_true", help="add the linear-solve leg")
+    p.add_argument("--detail", default="", help="also write the full figures (JSON) to this file")
     p.add_argument("--solve-only", action="store_true",
                    help="run only the linear-solve leg and print its figures")
     p.add_argument("--l2-fetch", type=int, default=-1,

