@@ -580,6 +580,7 @@ def run_gpu(args, ws, rank, local):
 
 
 _RES_FORM = {"staged": "one launch over the locality partition", "atomic": "one atomic launch",
+             "gather": "thread per cell over its incidence",
              "lma": "contribution launch + per-target reduction"}
 
 
@@ -641,8 +642,7 @@ def bench_batching(op2, b200, nmesh, reps=5, seed=0):
     for name, insts in (("mass", mass), ("stiffness", stiff), ("rhs", rhs)):
         best, times = autotune.tune(insts, reps=3)
         tuned[name] = {"best": best, "candidates_ms": times}
-        from pyop2_b200.batch import BatchLoop
-        loops.append(BatchLoop(insts, **best))
+        loops.append(autotune.build(insts, best))
     tune_s = time.time() - t1
     for bl in loops:
         bl.launch()
@@ -746,7 +746,9 @@ def bench_serving(op2, b200, nreq, rate, seed=0, n_p1=16, n_quad=16):
     for mkind, loops in kinds.items():
         meshes = [store.get(m) for m in sorted(pool) if pool[m][0] == mkind]
         for name, attr in loops:
-            configs[name], _ = autotune.tune([getattr(m, attr) for m in meshes], reps=2)
+            # patched request instances run the atomic batched form
+            configs[name], _ = autotune.tune([getattr(m, attr) for m in meshes], reps=2,
+                                             candidates=autotune.DEFAULT_CANDIDATES)
     tune_s = time.time() - t1
     b200.synchronize()
     # results reach the consumer as views of pinned host memory; every 16th
@@ -1017,7 +1019,7 @@ def main(argv=None):
     p.add_argument("--min-blocks", type=int, default=-1, help="stub __launch_bounds__ min blocks per SM")
     p.add_argument("--no-permute", action="store_true",
                    help="structured (unpermuted) cell/node numbering instead of the random one")
-    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic", "lma", "staged"],
+    p.add_argument("--inc-mode", default="", choices=["", "color", "atomic", "lma", "staged", "gather"],
                    help="INC conflict resolution of indirect loops (default: backend default)")
     args = p.parse_args(argv)
     _set_mesh(args.nx, args.ny)

@@ -250,6 +250,16 @@ int op2b_incidence_build(uint64_t map, int32_t nelem, int32_t arity, int32_t nta
 int op2b_incidence_arrays(uint64_t incidence, uint64_t *ptr, uint64_t *list,
                           int32_t *max_degree);
 int op2b_incidence_free(uint64_t incidence);
+/* Targets of a Map [nelem][arity] in order of first use along an element
+ * order: position q = pos*arity + k stands for row k of element
+ * elem_order[pos] (elem_order 0: element pos); target_order receives the
+ * ntargets ids sorted by their smallest q, targets no element uses last in
+ * increasing id.  The thread-per-target gather stubs walk targets in this
+ * order so that neighbouring threads gather neighbouring rows.  No direct
+ * reference counterpart (the reference walks elements in set order,
+ * pyop2/plan.pyx:107-110). */
+int op2b_first_use_order(uint64_t map, int32_t arity, int64_t nelem, uint64_t elem_order,
+                         int32_t ntargets, uint64_t target_order, uint64_t stream);
 
 /* ------------------------------------------------------------------------
  * Two-phase deterministic INC.  A generated stub writes every element's INC

@@ -1,10 +1,13 @@
 """Launch-configuration autotuner for batched loops.
 
 For a batch of loop instances (one signature) the tuner times each candidate
-configuration -- threads per CTA (block shape), elements per thread (the tile,
-i.e. the partition of each mesh handed to one CTA), the stub's minimum
-resident CTAs per SM (register cap) and the persistent grid's CTAs per SM --
-on the batch itself, with CUDA events after one untimed launch, and keeps the
+configuration -- the colouring granularity (element-level atomics, or the
+coloured form: each mesh partitioned into blocks of ``part_size`` elements
+with block and thread colours, pyop2/plan.pyx:214-376), the partition size
+(``part_size`` of the coloured form; threads per CTA x elements per thread,
+the tile handed to one CTA, of the atomic form), threads per CTA (block
+shape), the stub's minimum resident CTAs per SM (register cap) and the
+persistent grid's CTAs per SM -- on the batch itself, with CUDA events after one untimed launch, and keeps the
 fastest.  Results are cached in memory and in ``<cache_dir>/autotune.json``
 under a key made of the loop signature and the batch's size class, so a
 served or repeated batch of the same kind is not re-tuned.
@@ -25,6 +28,25 @@ from . import configuration as cfg
 DEFAULT_CANDIDATES = tuple(
     dict(block_size=bs, elems_per_thread=ept, min_blocks=mb, ctas_per_sm=0)
     for bs in (128, 256, 512) for ept in (1, 2, 4) for mb in (0,))
+
+# The coloured form's candidates: partition size (elements per block of each
+# instance's plan) x threads per CTA; the colouring granularity is the
+# choice between these and the element-level atomics above.
+COLOURED_CANDIDATES = tuple(
+    dict(form="color", part_size=ps, block_size=bs, min_blocks=0, ctas_per_sm=0)
+    for ps in (128, 512) for bs in (128, 256) if bs <= ps)
+
+
+def candidates_for(instances):
+    """The search space of a batch: atomic launch shapes, plus the coloured
+    form's partition sizes where the loop has indirect INC (a plan applies)
+    and no Global reduction."""
+    spec = instances[0].spec
+    out = list(DEFAULT_CANDIDATES)
+    if spec.mode == "atomic" and instances[0].form == "atomic" and not any(
+            a.kind == "gbl" and a.access != "READ" for a in spec.args):
+        out += list(COLOURED_CANDIDATES)
+    return tuple(out)
 
 _MEM = {}
 
@@ -88,12 +110,17 @@ def time_launch(runner, reps=3, flush=True, before=None):
     return statistics.median(ts)
 
 
-def tune(instances, candidates=DEFAULT_CANDIDATES, reps=3, use_cache=True, restore=None):
+def tune(instances, candidates=None, reps=3, use_cache=True, restore=None):
     """Best BatchLoop configuration for ``instances``: returns (config dict,
-    {config repr: ms}).  Each timed launch really runs the loops, so INC
-    targets accumulate: ``restore`` (a callable, untimed) is invoked before
-    every launch if the caller needs the data reset (e.g. zeroing Mats)."""
+    {config repr: ms}).  Candidates with ``form='color'`` run the coloured
+    form (the instances recast with a plan of ``part_size`` elements per
+    block); the others the atomic form.  Each timed launch really runs the
+    loops, so INC targets accumulate: ``restore`` (a callable, untimed) is
+    invoked before every launch if the caller needs the data reset (e.g.
+    zeroing Mats)."""
     from .batch import BatchLoop
+    if candidates is None:
+        candidates = candidates_for(instances)
     key = tuning_key(instances)
     if use_cache:
         hit = _MEM.get(key) or _load().get(key)
@@ -110,9 +137,25 @@ def tune(instances, candidates=DEFAULT_CANDIDATES, reps=3, use_cache=True, resto
         def launch(self):
             self.bl.launch(sync_host=False)
 
+    recast = {}
     for c in candidates:
-        bl = BatchLoop(instances, **c)
+        c = dict(c)
+        form = c.pop("form", "atomic")
+        ps = c.pop("part_size", None)
+        if form == "color":
+            if ps not in recast:
+                try:
+                    recast[ps] = [i.recast("color", ps) for i in instances]
+                except NotImplementedError:
+                    recast[ps] = None
+            if recast[ps] is None:
+                continue
+            bl = BatchLoop(recast[ps], **c)
+        else:
+            bl = BatchLoop(instances, **c)
         ms = time_launch(_Runner(bl), reps=reps, before=restore)
+        if form == "color":
+            c = dict(c, form=form, part_size=ps)
         times[json.dumps(c, sort_keys=True)] = round(ms, 5)
         if best_ms is None or ms < best_ms:
             best, best_ms = dict(c), ms
@@ -124,8 +167,19 @@ def tune(instances, candidates=DEFAULT_CANDIDATES, reps=3, use_cache=True, resto
     return dict(best), times
 
 
+def build(instances, config):
+    """A BatchLoop over ``instances`` in the form and shape ``config`` names
+    (a tuning result)."""
+    from .batch import BatchLoop
+    c = dict(config)
+    form = c.pop("form", "atomic")
+    ps = c.pop("part_size", None)
+    if form == "color":
+        instances = [i.recast("color", ps) for i in instances]
+    return BatchLoop(instances, **c)
+
+
 def tuned_batch(instances, **kw):
     """A BatchLoop over ``instances`` with the tuned configuration."""
-    from .batch import BatchLoop
     best, _ = tune(instances, **kw)
-    return BatchLoop(instances, **best)
+    return build(instances, best)

@@ -864,6 +864,26 @@ class RegionPlan(object):
             pass
 
 
+_GATHER_ORDER_CACHE = {}
+
+
+def gather_order(iterset, maps, region, omap):
+    """Targets of ``omap`` in order of first use along the element order of
+    the loop's locality partition (op2b_first_use_order), cached per
+    partition and Map: the target order of the gather form."""
+    rp = region_plan(iterset, maps, region)
+    key = (id(rp), id(omap))
+    hit = _GATHER_ORDER_CACHE.get(key)
+    if hit is not None and hit[0] is rp and hit[1] is omap:
+        return hit[2]
+    n = omap.dataset.size
+    order = DeviceBuffer(max(n, 1) * 4)
+    call("op2b_first_use_order", omap._to_device().ptr, omap.dim, iterset.size, rp.dptr["order"],
+         n, order.ptr, 0)
+    _GATHER_ORDER_CACHE[key] = (rp, omap, order)
+    return order
+
+
 def region_plan(iterset, maps, region):
     """The cached locality partition of a staged loop."""
     ps = region["part_size"]
@@ -1049,6 +1069,22 @@ def _slots_usable(specs):
     return bool(pairs) and all(len(v) == 1 for v in pairs.values())
 
 
+def mat_alias(specs, mats):
+    """For each Mat slot, the first Mat slot on the same Sparsity assembled
+    through the same (row Map, column Map) pair: their scatter-slot tables
+    are one table, read once."""
+    pair = {}
+    for s in specs:
+        if s.kind == "mat":
+            pair.setdefault(s.slot, (s.mslot, s.cmslot))
+    alias = []
+    for j, m in enumerate(mats):
+        same = [j0 for j0 in range(j)
+                if mats[j0].sparsity is m.sparsity and pair.get(j0) == pair.get(j)]
+        alias.append(same[0] if same else j)
+    return tuple(alias)
+
+
 def mat_slot_values(specs, maps, mats):
     """Parameter values ms<j>: the scatter-slot table of each Mat slot."""
     vals = {}
@@ -1199,12 +1235,31 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
             w = spec.args[owner["arg"]]
             if owner["kind"] == "dat" and w.kind != "its":
                 owner = None
+    req = inc_mode or cfg.cfg['inc_mode']
+    gather = None
+    if (owner is None and indirect and req == 'gather'
+            and iterset.size >= int(cfg.cfg['staged_min_size'])):
+        gather = codegen.owner_plan(spec, None)
+        if gather is not None and gather["kind"] != "dat":
+            gather = None
     if owner is not None:
         owner["kahan"] = bool(cfg.cfg['kahan'])
         spec.owner = owner
         spec.mode = "owner"
         indirect = False
-    elif (indirect and (inc_mode or cfg.cfg['inc_mode']) == 'staged' and codegen.staged_capable(spec)
+    elif gather is not None:
+        # thread per target over the owner Map's incidence, targets in
+        # first-use order along the locality partition (the partition the
+        # staged form would use; only its element order is used here)
+        gather["kahan"] = bool(cfg.cfg['kahan'])
+        spec.owner = gather
+        spec.mode = "gather"
+        R = _region_layout(specs, maps)
+        ps = int(cfg.cfg['partition_size']) or 384
+        R["part_size"] = max(1, min(ps, 16384 // max(R["stage_arity"])))
+        gather_region = R
+        indirect = False
+    elif (indirect and req in ('staged', 'gather') and codegen.staged_capable(spec)
           and iterset.size >= int(cfg.cfg['staged_min_size'])):
         spec.mode = "staged"
         spec.region = R = _region_layout(specs, maps)
@@ -1218,15 +1273,21 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
     elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'lma' and codegen.lma_capable(spec):
         spec.mode = "lma"
         indirect = False   # launched like a direct loop, then reduced per target
-    elif (indirect and (inc_mode or cfg.cfg['inc_mode']) in ('atomic', 'staged')
+    elif (indirect and req in ('atomic', 'staged', 'gather')
           and codegen.atomic_capable(spec)):
         spec.mode = "atomic"
         indirect = False   # launched like a direct loop: no plan
         spec.mat_slots = bool(cfg.cfg['mat_slots']) and _slots_usable(specs)
+        if spec.mat_slots:
+            spec.mat_alias = mat_alias(specs, mats)
+            # entries added one by one (scalar Mats only; the kernel of one
+            # (i0, i1) writes its own entry)
+            spec.mat_per_entry = bool(cfg.cfg['mat_per_entry'])
     gspecs = [s for s in specs if s.kind == "gbl"]
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
-                iterset=iterset, block_size=bs)
+                iterset=iterset, block_size=bs,
+                gather_region=gather_region if spec.mode == "gather" else None)
 
 
 def _same_values(m1, m2):
@@ -1412,6 +1473,16 @@ class _BoundLoop(object):
                     mask |= 1 << ix
                 self.lma.append((buf, _incidence(mp), d, st[3], mp.dataset.size, mp.dim, mask))
             self.grid = self._wave_grid(n, bs)
+            self.max_grid = self.grid
+        elif spec.mode == "gather":
+            # one thread per target of the owner Map, in first-use order
+            omap = maps[spec.owner["mslot"]]
+            inc = _incidence(omap)
+            order = gather_order(iterset, maps, info['gather_region'], omap)
+            vals["inc_ptr"], vals["inc_list"], vals["inc_order"] = inc.ptr, inc.list, order.ptr
+            self.gather_order = order
+            self.range_end = omap.dataset.size
+            self.grid = self._wave_grid(self.range_end, bs)
             self.max_grid = self.grid
         elif spec.mode == "owner":
             # one warp per target of the owner Map

@@ -115,13 +115,31 @@ class LoopInstance(object):
     :meth:`like` makes the same loop over other objects (another mesh, other
     Dats) without re-deriving the loop signature."""
 
-    def __init__(self, kernel, it_space, *args):
+    def __init__(self, kernel, it_space, *args, form="atomic", part_size=256):
         loop = b200.ParLoop(kernel, it_space, *args)
-        info = b200.loop_spec(loop, owner_mode='never', inc_mode='atomic', min_blocks=0)
-        spec = info['spec']
-        if spec.mode not in ("direct", "atomic"):
-            raise NotImplementedError("batched loops need direct access or atomic INC "
-                                      "(kernel %s)" % kernel.name)
+        self._loop_args = (kernel, it_space) + tuple(args)
+        self.form = form
+        self.plan = None
+        if form == "color":
+            info = b200.loop_spec(loop, owner_mode='never', inc_mode='color', min_blocks=0)
+            spec = info['spec']
+            if spec.mode != "plan" or any(s.kind == "gbl" and s.access != "READ"
+                                          for s in info['specs']):
+                raise NotImplementedError("the coloured batched form runs indirect loops "
+                                          "without Global reductions (kernel %s)" % kernel.name)
+            if b200._slots_usable(info['specs']):
+                spec.mat_slots = True
+                spec.mat_alias = b200.mat_alias(info['specs'], info['mats'])
+            self.plan = _instance_plan(info, int(part_size))
+            spec.batch_part_size = int(part_size)
+        elif form == "atomic":
+            info = b200.loop_spec(loop, owner_mode='never', inc_mode='atomic', min_blocks=0)
+            spec = info['spec']
+            if spec.mode not in ("direct", "atomic"):
+                raise NotImplementedError("batched loops need direct access or atomic INC "
+                                          "(kernel %s)" % kernel.name)
+        else:
+            raise ValueError("batched form %r (atomic or color)" % form)
         self.spec = spec
         self.key = spec.key()
         self.iterset = info['iterset']
@@ -140,14 +158,29 @@ class LoopInstance(object):
     def _finish(self):
         self.size = int(self.iterset.size)
         self.vals = _bind(self.fields)
+        if self.plan is not None:
+            d = self.plan.dptr
+            self.vals.update(blkmap=d["blkmap"], offset=d["offset"], nelems=d["nelems"],
+                             nthrcol=d["nthrcol"], thrcol=d["thrcol"], ind_map=d["ind_map"],
+                             ind_sizes=d["ind_sizes"], ind_offs=d["ind_offs"],
+                             loc_map=d["loc_map"])
         self.params = codegen.ParamLayout(self.spec).pack(self.size, 0, self.size, self.vals)
+
+    def recast(self, form, part_size=256):
+        """The same loop over the same objects in another batched form."""
+        return LoopInstance(*self._loop_args, form=form, part_size=part_size)
 
     def like(self, subs):
         """The same loop with objects replaced: ``subs`` maps each object of
         this instance (iteration Set, Maps, Dats, Mats, Globals) to its
         replacement; objects not listed are shared.  Replacements must have
-        the types, dims and arities of the originals."""
+        the types, dims and arities of the originals (atomic form only: a
+        coloured instance's plan belongs to its own Maps)."""
+        if self.plan is not None:
+            raise NotImplementedError("like() of a coloured batched instance")
         new = object.__new__(LoopInstance)
+        new.form, new.plan = self.form, None
+        new._loop_args = None
         new.spec, new.key = self.spec, self.key
         by_id = {id(k): v for k, v in subs.items()}   # Maps compare by structure
         r = lambda o: by_id.get(id(o), o)  # noqa: E731
@@ -168,6 +201,11 @@ class LoopInstance(object):
         return new
 
     def patch(self, ptrs):
+        if self.plan is not None:
+            raise NotImplementedError("patch() of a coloured batched instance")
+        return self._patch(ptrs)
+
+    def _patch(self, ptrs):
         """A :class:`PatchedInstance` of this loop whose arguments bound to
         the objects in ``ptrs`` (object -> device address) read and write the
         given addresses instead: raw device memory of the same layout (e.g.
@@ -245,8 +283,14 @@ class BatchLoop(object):
         if spec.batch < 1:
             raise ValueError("elems_per_thread must be >= 1")
         self.spec = spec
+        self.form = self.instances[0].form
         self.config = dict(block_size=spec.block_size, elems_per_thread=spec.batch,
                            min_blocks=spec.min_blocks, ctas_per_sm=int(ctas_per_sm))
+        if self.form == "color":
+            self.config = dict(form="color", part_size=spec.batch_part_size,
+                               block_size=spec.block_size, min_blocks=spec.min_blocks,
+                               ctas_per_sm=int(ctas_per_sm))
+        self.smem = max((i.plan.nshared for i in self.instances if i.plan is not None), default=0)
         ckey = (key, spec.block_size, spec.batch, spec.min_blocks)
         hit = _COMPILED.get(ckey)
         if hit is None:
@@ -254,9 +298,15 @@ class BatchLoop(object):
             layout = codegen.BatchLayout(spec)
             has_fin = len(layout.fields) > 5
             fin = module.function(codegen.batch_stub_names(spec)[1]) if has_fin else 0
-            occ = module.occupancy(module.fn, spec.block_size)
-            hit = _COMPILED[ckey] = (module, layout, has_fin, fin, occ)
-        self.module, self.layout, self.has_fin, self.fin, occ = hit
+            hit = _COMPILED[ckey] = (module, layout, has_fin, fin)
+        self.module, self.layout, self.has_fin, self.fin = hit
+        if self.smem > b200._state['smem_optin']:
+            raise DeviceError("coloured batch needs %d bytes of shared memory per block" % self.smem)
+        self.module.ensure_smem(self.smem)
+        occ = self.module.occupancy(self.module.fn, spec.block_size, self.smem)
+        if self.form == "color":
+            self._init_colored(occ, int(ctas_per_sm))
+            return
         # segments and tiles
         sizes = np.array([inst.size for inst in self.instances], dtype=np.int64)
         tiles, tile_first = build_tiles(sizes, spec.block_size * spec.batch)
@@ -292,9 +342,64 @@ class BatchLoop(object):
         self.fin_grid = (self.nsegs * 32 + 255) // 256
         self.consts = b200.base.Const._definitions()
 
+    def _init_colored(self, occ, ctas_per_sm):
+        """Tiles of the coloured form: for colour c, every segment's blocks
+        of colour c (positions in its blkmap); one launch per colour."""
+        spec = self.spec
+        sizes = np.array([inst.size for inst in self.instances], dtype=np.int64)
+        self.nsegs = len(sizes)
+        self.elements = int(sizes.sum())
+        ncol = max((i.plan.ncolors for i in self.instances), default=0)
+        per = []
+        for c in range(ncol):
+            segs, firsts = [], []
+            for s, inst in enumerate(self.instances):
+                pl = inst.plan
+                if c >= pl.ncolors:
+                    continue
+                ncb = list(pl.ncolblk_host)[:pl.ncolors]
+                c0 = sum(ncb[:c])
+                segs += [s] * ncb[c]
+                firsts += list(range(c0, c0 + ncb[c]))
+            t = np.zeros(max(len(segs), 1), dtype=TILE_DTYPE)
+            if segs:
+                t["seg"][:len(segs)] = segs
+                t["first"][:len(segs)] = firsts
+            per.append((t, len(segs)))
+        segs_b = b"".join(i.params for i in self.instances)
+        o_tiles = (len(segs_b) + 15) // 16 * 16
+        total = o_tiles + sum(t.nbytes for t, _ in per)
+        host = np.zeros(max(total, 16), dtype=np.uint8)
+        host[:len(segs_b)] = np.frombuffer(segs_b, dtype=np.uint8)
+        offs, o = [], o_tiles
+        for t, _ in per:
+            host[o:o + t.nbytes] = t.view(np.uint8)
+            offs.append(o)
+            o += t.nbytes
+        self._meta = b200._upload(host)
+        base = self._meta.ptr
+        if occ < 1:
+            raise DeviceError("batched stub %s cannot be resident at block size %d"
+                              % (spec.kernel_name, spec.block_size))
+        if ctas_per_sm:
+            occ = min(occ, ctas_per_sm)
+        self._gpart = []
+        self._colour_launches = []
+        for (t, n), off in zip(per, offs):
+            if n == 0:
+                continue
+            params = self.layout.pack(dict(segs=base, tiles=base + off, tile_first=0, ntiles=n,
+                                           nsegs=self.nsegs))
+            self._colour_launches.append((int(min(n, occ * b200._state['sm_count'])), params))
+        self.ntiles = sum(n for _, n in per)
+        self.grid = max((g for g, _ in self._colour_launches), default=0)
+        self.consts = b200.base.Const._definitions()
+
     @property
     def launches(self):
         """Kernels one :meth:`launch` issues."""
+        if self.form == "color":
+            return len(self._colour_launches)
         return (1 if self.grid else 0) + (1 if self.has_fin and self.nsegs else 0)
 
     def launch(self, sync_host=True):
@@ -305,7 +410,11 @@ class BatchLoop(object):
             for inst in self.instances:
                 inst.sync()
         b200._sync_consts(self.module, self.consts)
-        if self.grid:
+        if self.form == "color":
+            for grid, params in self._colour_launches:
+                call("op2b_launch", self.module.fn, grid, self.spec.block_size, self.smem, 0,
+                     params, self.layout.nbytes)
+        elif self.grid:
             call("op2b_launch", self.module.fn, self.grid, self.spec.block_size, 0, 0,
                  self._params, self.layout.nbytes)
         if self.has_fin and self.nsegs:
@@ -313,6 +422,30 @@ class BatchLoop(object):
         if sync_host:
             for inst in self.instances:
                 inst.mark()
+
+
+_PLANS = {}
+
+
+def _instance_plan(info, part_size):
+    """The GPU plan (block partition, block and thread colours, INC staging)
+    of a coloured batched instance, cached per (Maps, partition size)."""
+    maps, dats, stages, races = info['maps'], info['dats'], info['stages'], info['races']
+    iterset = info['iterset']
+    key = (iterset.size, part_size, tuple((id(maps[st[1]]), tuple(st[4])) for st in stages),
+           tuple((tuple((id(m), ix) for m, ix in ents), size) for ents, size in races))
+    hit = _PLANS.get(key)
+    if hit is not None and all(r() is not None for r in hit[1]):
+        return hit[0]
+    import weakref
+    plan = b200.DevicePlan(iterset.size, part_size,
+                           [(maps[st[1]], st[4], np.dtype(dats[st[0]].dtype).itemsize * st[3])
+                            for st in stages],
+                           [(ents, size) for ents, size in races], staging=True,
+                           thread_coloring=True)
+    plan._keep = list(maps)
+    _PLANS[key] = (plan, [weakref.ref(m) for m in maps])
+    return plan
 
 
 _CTYPES = {"double": np.float64, "float": np.float32, "int": np.int32, "unsigned int": np.uint32,

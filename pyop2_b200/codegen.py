@@ -79,6 +79,13 @@ class LoopSpec(object):
         # scalar Mats found through scatter-slot tables (op2b_mat_slots_build)
         # instead of a row search per entry (atomic and batched forms)
         self.mat_slots = False
+        # Mat slot whose scatter-slot table each Mat slot reads (Mats on one
+        # Sparsity through the same Map pair share one table and one load)
+        self.mat_alias = ()
+        # scalar Mat entries added right after the kernel call of their
+        # (i0, i1) instead of after the whole local tensor (atomic form with
+        # slot tables): one entry live at a time instead of the whole tensor
+        self.mat_per_entry = False
         # staged form over a locality partition (mode 'staged'): map_stage
         # {map slot: staged Map}, stage_arity, row_base (first loc row of each
         # staged Map), read_pairs / inc_pairs [(Dat slot, staged Map, ctype,
@@ -105,7 +112,8 @@ class LoopSpec(object):
                 tuple((s[0], s[1], s[2], s[3], tuple(s[4])) for s in self.stages),
                 self.block_size, self.fmad, self.min_blocks, self.mode,
                 tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
-                self.mat_slots, _freeze(self.region))
+                self.mat_slots, _freeze(self.region), tuple(self.mat_alias),
+                self.mat_per_entry)
 
     @property
     def needs_coloring(self):
@@ -132,6 +140,8 @@ class ParamLayout(object):
         f = []
         if spec.mode == "owner":
             f += ["inc_ptr", "inc_list"]
+        if spec.mode == "gather":
+            f += ["inc_ptr", "inc_list", "inc_order"]
         if spec.mode == "plan":
             f += ["blkmap", "offset", "nelems", "nthrcol", "thrcol", "ind_map", "ind_sizes",
                   "ind_offs", "loc_map"]
@@ -178,6 +188,7 @@ def _struct_decl(spec, layout):
              "nthrcol": "const int *", "thrcol": "const int *", "ind_map": "const int *",
              "ind_sizes": "const int *", "ind_offs": "const int *", "loc_map": "const short *",
              "err": "int *", "inc_ptr": "const int *", "inc_list": "const int *",
+             "inc_order": "const int *",
              "rg_order": "const int *", "rg_boff": "const int *", "rg_tlist": "const int *",
              "rg_toff": "const int *", "rg_tcnt": "const int *", "rg_loc": "const short *",
              "rg_thrcol": "const int *", "rg_nthrcol": "const int *"}
@@ -251,10 +262,11 @@ def generate(spec):
     w("}  // namespace op2b_user")
     w("#undef OP2_STRIDE")
     if spec.batch:
-        w(_batch_body(spec))
+        w(_batch_plan_body(spec) if spec.mode == "plan" else _batch_body(spec))
         return "\n".join(out), layout, batch_stub_names(spec)[0]
     body = {"plan": _indirect_body, "atomic": _atomic_body, "lma": _atomic_body,
-            "direct": _direct_body, "owner": _owner_body, "staged": _staged_body}[spec.mode](spec)
+            "direct": _direct_body, "owner": _owner_body, "staged": _staged_body,
+            "gather": _gather_body}[spec.mode](spec)
     w(body)
     return "\n".join(out), layout, stub_name(spec)
 
@@ -360,17 +372,35 @@ def _itspace_close(spec, indent):
 
 
 def _indirect_body(spec):
-    bs = spec.block_size
-    ninds = len(spec.stages)
-    coloured = spec.needs_coloring
     L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
     L.append("  if ((int)blockIdx.x >= p.col_n) return;")
     L.append("  const int blk = p.blkmap[p.col_first + blockIdx.x];")
+    L += _plan_block(spec)
+    L.append("}")
+    return "\n".join(L)
+
+
+def _plan_block(spec, batched=False):
+    """Lines running block ``blk`` of a plan (coloured form): the body of
+    the reference's indirect-loop template (cuda_indirect_loop.jinja2)
+    restated -- INC rows staged in shared memory at the plan's loc_map slots,
+    thread colours serialising the shared adds and the Mat adds, the block's
+    rows added to the Dats once at the end (block colours keep concurrently
+    running blocks apart).  ``batched``: the block is one tile of a batched
+    coloured launch (no Global reductions; a barrier before the block reuses
+    shared memory)."""
+    bs = spec.block_size
+    ninds = len(spec.stages)
+    coloured = spec.needs_coloring
+    L = []
+    if batched:
+        L.append("  __syncthreads();")
     L.append("  const int start = p.offset[blk];")
     L.append("  const int nelem = p.nelems[blk];")
     L.append("  const op2b_i64 set_size = p.set_size;")
     if ninds:
-        L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
+        if not batched:
+            L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
         L.append("  int smem_off = 0;")
         nidx_prefix = 0
         for s, (dslot, mslot, t, c, idxs) in enumerate(spec.stages):
@@ -383,7 +413,8 @@ def _indirect_body(spec):
                      % (s, c, bs, s, t))
             nidx_prefix += len(idxs)
         L.append("  __syncthreads();")
-    _gbl_prologue(spec, L)
+    if not batched:
+        _gbl_prologue(spec, L)
     if coloured:
         L.append("  const int ncol = p.nthrcol[blk];")
     L.append("  for (int base = 0; base < nelem; base += %d) {" % bs)
@@ -507,9 +538,9 @@ def _indirect_body(spec):
             L.append("    const int r = t / %d, k = t - r * %d;" % (c, c))
             L.append("    p.d%d[(op2b_i64)ind_s%d[r] * %d + k] += inc_s%d[t];" % (dslot, s, c, s))
             L.append("  }")
-    _gbl_epilogue(spec, L)
-    L.append("}")
-    return "\n".join(L)
+    if not batched:
+        _gbl_epilogue(spec, L)
+    return L
 
 
 def _atomic_body(spec):
@@ -843,27 +874,59 @@ def _atomic_element(spec, ind):
                     exprs.append("p.d%d + (op2b_i64)mr%d[%s] * %d" % (a.slot, a.mslot, var, c))
         elif a.kind == "mat":
             e0, e1 = spec.extents[0], spec.extents[1]
-            if a.rm * a.cm == 1:
+            if spec.mat_per_entry:
+                exprs.append("(%s (*)[1])&A%d" % (t, n))
+            elif a.rm * a.cm == 1:
                 pre.append("%s%s A%d[%d][%d];" % (ind, t, n, e0, e1))
                 exprs.append("(%s (*)[1])&A%d[i0][i1]" % (t, n))
             else:
                 pre.append("%s%s A%d[%d][%d][%d][%d];" % (ind, t, n, e0, e1, a.rm, a.cm))
                 exprs.append("A%d[i0][i1]" % n)
-            apply += _mat_addto(spec, n, a, ind, atomic=True, lma=spec.mode == "lma")
+            if not spec.mat_per_entry:
+                apply += _mat_addto(spec, n, a, ind, atomic=True, lma=spec.mode == "lma")
     L += pre
     L += _itspace_open(spec, ind)
     deep = ind + "  " * len(spec.extents)
     for n, a in enumerate(spec.args):
         if a.kind == "mat":
-            if a.rm * a.cm == 1:
+            if spec.mat_per_entry:
+                L.append("%s%s A%d = (%s)0;" % (deep, a.ctype, n, a.ctype))
+            elif a.rm * a.cm == 1:
                 L.append("%sA%d[i0][i1] = (%s)0;" % (deep, n, a.ctype))
             else:
                 L.append("%sfor (int r = 0; r < %d; ++r) for (int c = 0; c < %d; ++c) A%d[i0][i1][r][c] = (%s)0;"
                          % (deep, a.rm, a.cm, n, a.ctype))
     L.append(_kernel_call(spec, exprs, deep))
+    if spec.mat_per_entry:
+        L += _mat_add_entry(spec, deep)
     L += _itspace_close(spec, ind)
     L += post
     L += apply
+    return L
+
+
+def _mat_add_entry(spec, ind):
+    """Add the entries (i0, i1) of the loop's scalar Mat args (locals A<n>)
+    into their CSR positions, read from the scatter-slot tables -- one load
+    per table, shared by the Mats that alias it."""
+    L = []
+    loaded = set()
+    for n, a in enumerate(spec.args):
+        if a.kind != "mat":
+            continue
+        j = a.slot
+        tab = spec.mat_alias[j] if spec.mat_alias else j
+        ri, ci = "i%d" % a.idx, "i%d" % a.cidx
+        if tab not in loaded:
+            loaded.add(tab)
+            L.append("%sconst int pos%d = __ldg(p.ms%d + (op2b_i64)(%s * %d + %s) * p.set_size + e);"
+                     % (ind, tab, tab, ri, a.carity, ci))
+            L.append("%sif (pos%d < 0) op2b_flag_missing(p.err, mr%d[%s], mr%d[%s]);"
+                     % (ind, tab, a.mslot, ri, a.cmslot, ci))
+        if a.access == "WRITE":
+            L.append("%sif (pos%d >= 0) p.mv%d[pos%d] = A%d;" % (ind, tab, j, tab, n))
+        else:
+            L.append("%sif (pos%d >= 0) op2b_atomic_add(&p.mv%d[pos%d], A%d);" % (ind, tab, j, tab, n))
     return L
 
 
@@ -963,6 +1026,37 @@ def _batch_body(spec):
     return "\n".join(L)
 
 
+def _batch_plan_body(spec):
+    """A batched coloured loop: every instance (segment) carries its own
+    plan (block partition of ``part_size`` elements, block colours, thread
+    colours, INC staging), and each launch runs the blocks of ONE colour of
+    every segment -- tiles (segment, position in the segment's blkmap) --
+    so no two concurrently running blocks of a segment share a target, and
+    blocks of different segments never do.  Inside a block the plan's thread
+    colours order the adds (no atomics); the block's staged INC rows are
+    added to the Dats at its end.  No Global reductions (their loops use the
+    atomic batched form)."""
+    names = batch_stub_names(spec)
+    L = ["struct op2b_batch_tile { int seg; int pad; op2b_i64 first; };",
+         "struct op2b_batch_params {", "  const op2b_params *segs;",
+         "  const op2b_batch_tile *tiles;", "  const op2b_i64 *tile_first;",
+         "  op2b_i64 ntiles, nsegs;", "};"]
+    L.append("extern \"C\" __global__ void %s %s(const op2b_batch_params bp) {"
+             % (_bounds(spec), names[0]))
+    if spec.stages:
+        L.append("  extern __shared__ __align__(16) unsigned char op2b_smem[];")
+    L.append("  for (op2b_i64 t = blockIdx.x; t < bp.ntiles; t += gridDim.x) {")
+    L.append("    const op2b_batch_tile td = bp.tiles[t];")
+    L.append("    const op2b_params p = bp.segs[td.seg];")
+    L.append("    const int blk = p.blkmap[td.first];")
+    L.append("    {")
+    L += ["    " + x for x in _plan_block(spec, batched=True)]
+    L.append("    }")
+    L.append("  }")
+    L.append("}")
+    return "\n".join(L)
+
+
 def _owner_body(spec):
     """Owner computes: one warp per target t of the owner Map (a row node of
     the Mat, or an element of the INC Dat's set).  The warp walks t's
@@ -1034,54 +1128,8 @@ def _owner_body(spec):
         ar = spec.maps[kk]
         L.append("%s__align__(16) int mr%d[%d];" % (ind2, kk, ar))
         L.append("%sop2b_load<int, %d, true>(mr%d, p.m%d + e * %d);" % (ind2, ar, kk, kk, ar))
-    pre, exprs, select = [], [], []
-    for n, a in enumerate(spec.args):
-        t, c = a.ctype, a.cdim
-        if a.kind == "gbl":
-            exprs.append("g%d_l" % n)
-        elif a.kind == "direct":
-            pre.append("%s__align__(16) %s a%d[%d];" % (ind2, t, n, c))
-            pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + e * %d);" % (ind2, t, c, _ro(a), n, a.slot, c))
-            exprs.append("a%d" % n)
-        elif a.kind == "ind":
-            pre.append("%s__align__(16) %s a%d[%d];" % (ind2, t, n, c))
-            if a.access == "INC":
-                pre.append("%sop2b_zero(a%d);" % (ind2, n))
-                select.append("%sif (k == %d) for (int q = 0; q < %d; ++q) contrib[q] += a%d[q];"
-                              % (ind2, a.idx, c, n))
-            else:
-                pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + (op2b_i64)mr%d[%d] * %d);"
-                           % (ind2, t, c, _ro(a), n, a.slot, a.mslot, a.idx, c))
-            exprs.append("a%d" % n)
-        elif a.kind == "vec":
-            cnt = a.arity
-            pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind2, t, n, cnt, c))
-            for r in range(cnt):
-                if a.access == "INC":
-                    pre.append("%sop2b_zero(a%d[%d]);" % (ind2, n, r))
-                    select.append("%sif (k == %d) for (int q = 0; q < %d; ++q) contrib[q] += a%d[%d][q];"
-                                  % (ind2, r, c, n, r))
-                else:
-                    pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
-                               % (ind2, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
-            pre.append("%s%s *a%d_v[%d] = {%s};" % (ind2, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
-            exprs.append("a%d_v" % n)
-        elif a.kind == "its":
-            if a.access == "INC":
-                # 1-d iteration space: the kernel runs once, at i0 = k
-                pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind2, t, n, c, n))
-                select.append("%sfor (int q = 0; q < %d; ++q) contrib[q] += a%d[q];" % (ind2, c, n))
-                exprs.append("a%d" % n)
-            else:
-                cnt = a.ext
-                pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind2, t, n, cnt, c))
-                for r in range(cnt):
-                    pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
-                               % (ind2, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
-                exprs.append("a%d[i%d]" % (n, a.idx))
-        elif a.kind == "mat":
-            pre.append("%s%s Aloc;" % (ind2, t))
-            exprs.append("(%s (*)[1])&Aloc" % t)
+    pre, exprs, select = _owner_args(
+        spec, ind2, lambda src, c: "for (int q = 0; q < %d; ++q) contrib[q] += %s[q];" % (c, src))
     L += pre
     if ow["kind"] == "dat":
         nx = len(spec.extents)
@@ -1145,6 +1193,122 @@ def _owner_body(spec):
     L.append("  }")
     L.append("}")
     return "\n".join(L)
+
+
+def _gather_body(spec):
+    """Dat INC gathered per target, one thread per target ("gather" form).
+
+    The loop's only writes are INC into one Dat through one Map (the owner
+    Map, ``owner_plan``).  Thread i takes target t = inc_order[i] (targets in
+    order of first use along the locality partition's element order, so the
+    threads of a warp own neighbouring targets and gather overlapping rows
+    through L1) and walks t's incidence (flat positions e*arity + k, in
+    increasing order): for each it evaluates the kernel for element e and
+    keeps the contribution for map index k.  The target's row is read once,
+    the contributions added in registers in the order the sequential
+    backend adds them (element order, then map index,
+    pyop2/sequential.py:55-72), optionally Kahan-compensated, and the row
+    is written once: no atomics, no colouring, no shared memory.  An
+    element whose targets differ is evaluated once per target."""
+    bs = spec.block_size
+    ow = spec.owner
+    A = ow["arity"]
+    oarg = spec.args[ow["arg"]]
+    T, C = oarg.ctype, oarg.cdim
+    kahan = ow.get("kahan")
+    L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
+    _gbl_prologue(spec, L)
+    L.append("  for (op2b_i64 i = (op2b_i64)blockIdx.x * %d + threadIdx.x; i < p.end;"
+             " i += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
+    L.append("    const op2b_i64 t = p.inc_order[i];")
+    L.append("    const int p0 = p.inc_ptr[t], p1 = p.inc_ptr[t + 1];")
+    L.append("    __align__(16) %s acc[%d];" % (T, C))
+    L.append("    op2b_load<%s, %d, false>(acc, p.d%d + t * %d);" % (T, C, oarg.slot, C))
+    if kahan:
+        L.append("    %s comp[%d];" % (T, C))
+        L.append("    for (int q = 0; q < %d; ++q) comp[q] = (%s)0;" % (C, T))
+
+    def sink(src, c):
+        if not kahan:
+            return "for (int q = 0; q < %d; ++q) acc[q] += %s[q];" % (c, src)
+        return ("for (int q = 0; q < %d; ++q) { %s y_ = %s[q] - comp[q]; %s t_ = acc[q] + y_;"
+                " comp[q] = (t_ - acc[q]) - y_; acc[q] = t_; }" % (c, T, src, T))
+    L.append("    for (int ii = p0; ii < p1; ++ii) {")
+    L.append("      const int pos = p.inc_list[ii];")
+    L.append("      const op2b_i64 e = pos / %d;" % A)
+    L.append("      const int k = pos - (int)e * %d;" % A)
+    ind2 = "      "
+    used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its")})
+    for kk in used_maps:
+        ar = spec.maps[kk]
+        L.append("%s__align__(16) int mr%d[%d];" % (ind2, kk, ar))
+        L.append("%sop2b_load<int, %d, true>(mr%d, p.m%d + e * %d);" % (ind2, ar, kk, kk, ar))
+    pre, exprs, select = _owner_args(spec, ind2, sink)
+    L += pre
+    if spec.extents:
+        L.append("%sconst int i0 = k;" % ind2)
+    L.append(_kernel_call(spec, exprs, ind2))
+    L += select
+    L.append("    }")
+    L.append("    op2b_store(p.d%d + t * %d, acc);" % (oarg.slot, C))
+    L.append("  }")
+    L.append("}")
+    return "\n".join(L)
+
+
+def _owner_args(spec, ind2, sink):
+    """(pre, exprs, select) of one kernel evaluation of an owner-computes
+    stub for element e and owner map index k: READ rows loaded through the
+    element's map rows (mr<slot>), INC args of the owner Dat zeroed locals
+    whose row for index k is handed to ``sink(local row expression, cdim)``
+    (the line that keeps the owner's share), a Mat arg one local entry."""
+    pre, exprs, select = [], [], []
+    for n, a in enumerate(spec.args):
+        t, c = a.ctype, a.cdim
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n)
+        elif a.kind == "direct":
+            pre.append("%s__align__(16) %s a%d[%d];" % (ind2, t, n, c))
+            pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + e * %d);" % (ind2, t, c, _ro(a), n, a.slot, c))
+            exprs.append("a%d" % n)
+        elif a.kind == "ind":
+            pre.append("%s__align__(16) %s a%d[%d];" % (ind2, t, n, c))
+            if a.access == "INC":
+                pre.append("%sop2b_zero(a%d);" % (ind2, n))
+                select.append("%sif (k == %d) { %s }" % (ind2, a.idx, sink("a%d" % n, c)))
+            else:
+                pre.append("%sop2b_load<%s, %d, %s>(a%d, p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                           % (ind2, t, c, _ro(a), n, a.slot, a.mslot, a.idx, c))
+            exprs.append("a%d" % n)
+        elif a.kind == "vec":
+            cnt = a.arity
+            pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind2, t, n, cnt, c))
+            for r in range(cnt):
+                if a.access == "INC":
+                    pre.append("%sop2b_zero(a%d[%d]);" % (ind2, n, r))
+                    select.append("%sif (k == %d) { %s }" % (ind2, r, sink("a%d[%d]" % (n, r), c)))
+                else:
+                    pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                               % (ind2, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
+            pre.append("%s%s *a%d_v[%d] = {%s};" % (ind2, t, n, cnt, ", ".join("a%d[%d]" % (n, r) for r in range(cnt))))
+            exprs.append("a%d_v" % n)
+        elif a.kind == "its":
+            if a.access == "INC":
+                # 1-d iteration space: the kernel runs once, at i0 = k
+                pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind2, t, n, c, n))
+                select.append("%s%s" % (ind2, sink("a%d" % n, c)))
+                exprs.append("a%d" % n)
+            else:
+                cnt = a.ext
+                pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind2, t, n, cnt, c))
+                for r in range(cnt):
+                    pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], p.d%d + (op2b_i64)mr%d[%d] * %d);"
+                               % (ind2, t, c, _ro(a), n, r, a.slot, a.mslot, r, c))
+                exprs.append("a%d[i%d]" % (n, a.idx))
+        elif a.kind == "mat":
+            pre.append("%s%s Aloc;" % (ind2, t))
+            exprs.append("(%s (*)[1])&Aloc" % t)
+    return pre, exprs, select
 
 
 def owner_plan(spec, mat_row_nnz_max=None):
@@ -1238,9 +1402,10 @@ def _mat_addto(spec, n, a, ind, atomic=False, lma=False):
         return L
     if a.rm * a.cm == 1:
         L.append("%s  const int row = mr%d[%s], colj = mr%d[%s];" % (ind, a.mslot, ri, a.cmslot, ci))
-        if spec.mat_slots and atomic:
+        if spec.mat_slots:
+            tab = spec.mat_alias[j] if spec.mat_alias else j
             L.append("%s  const int pos = __ldg(p.ms%d + (op2b_i64)(%s * %d + %s) * p.set_size + e);"
-                     % (ind, j, ri, a.carity, ci))
+                     % (ind, tab, ri, a.carity, ci))
         else:
             L.append("%s  const int pos = op2b_csr_find(p.mr%d, p.mc%d, row, colj);" % (ind, j, j))
         L.append("%s  if (pos < 0) op2b_flag_missing(p.err, row, colj);" % ind)

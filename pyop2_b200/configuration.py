@@ -29,7 +29,13 @@ keys of the B200 backend:
   accumulated there, then added once per target with atomics; summation
   order varies between runs within rounding; loops without indirect INC,
   with Mats, or whose staged rows would not fit a CTA's shared memory run
-  as ``'atomic'``);
+  as ``'atomic'``) or ``'gather'`` (loops whose only writes are INC into
+  one Dat through one Map: one thread per target walks the target's
+  incidence in element order, evaluates the kernel for each incident element
+  and keeps its own share, then writes the target once -- no atomics, no
+  colouring, the sequential backend's summation order; targets run in order
+  of first use along the locality partition, so a warp's threads own
+  neighbouring targets; other loops run as with ``'staged'``);
 * ``region_size``: elements per region (one hashed seed per about this many
   elements) of the staged form's locality partition (0: half the partition
   size, whose default in the staged form is 384);
@@ -53,6 +59,10 @@ keys of the B200 backend:
   scatter-slot table (the CSR position of every element's local entries,
   built once per Sparsity and Map pair: nelem x arity^2 int32 of device
   memory) instead of searching the CSR row for every entry;
+* ``mat_per_entry``: with slot tables, add each scalar Mat entry right after
+  the kernel call that computed it instead of after the whole local tensor
+  (one entry live in registers instead of the tensor; Mats on one Sparsity
+  through one Map pair share one slot load);
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;
 * ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
@@ -84,6 +94,7 @@ _defaults = {
     'owner_mode': 'never',
     'kahan': False,
     'mat_slots': True,
+    'mat_per_entry': True,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

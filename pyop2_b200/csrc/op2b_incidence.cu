@@ -110,6 +110,73 @@ inc_sort_kernel(const int32_t *__restrict__ ptr, int32_t *__restrict__ list, int
   if (lane == 0) atomicMax(max_deg, local_max);
 }
 
+// ---- first-use order of a Map's targets along an element order.
+// Position q = pos * arity + k stands for map row k of element order[pos]
+// (order == nullptr: element pos).  first[t] = the smallest q whose target
+// is t; a target is listed at the rank of its first use among all first
+// uses, and targets no element uses follow in increasing id.
+__global__ void fu_first_kernel(const int32_t *__restrict__ map, int arity, int64_t nelem,
+                                const int32_t *__restrict__ order, int32_t *__restrict__ first) {
+  const int64_t tot = nelem * arity;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pos = q / arity;
+    const int k = (int)(q - pos * arity);
+    const int64_t e = order ? order[pos] : pos;
+    atomicMin(&first[map[e * arity + k]], (int32_t)q);
+  }
+}
+
+__global__ void fu_flag_kernel(const int32_t *__restrict__ map, int arity, int64_t nelem,
+                               const int32_t *__restrict__ order, const int32_t *__restrict__ first,
+                               int32_t *__restrict__ flag) {
+  const int64_t tot = nelem * arity;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pos = q / arity;
+    const int k = (int)(q - pos * arity);
+    const int64_t e = order ? order[pos] : pos;
+    flag[q] = first[map[e * arity + k]] == (int32_t)q;
+  }
+}
+
+__global__ void fu_scatter_kernel(const int32_t *__restrict__ map, int arity, int64_t nelem,
+                                  const int32_t *__restrict__ order,
+                                  const int32_t *__restrict__ first,
+                                  const int32_t *__restrict__ rank, int32_t *__restrict__ out) {
+  const int64_t tot = nelem * arity;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pos = q / arity;
+    const int k = (int)(q - pos * arity);
+    const int64_t e = order ? order[pos] : pos;
+    const int32_t t = map[e * arity + k];
+    if (first[t] == (int32_t)q) out[rank[q]] = t;
+  }
+}
+
+__global__ void fu_unused_flag_kernel(const int32_t *__restrict__ first, int32_t ntargets,
+                                      int32_t *__restrict__ flag) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntargets;
+       t += (int64_t)gridDim.x * blockDim.x)
+    flag[t] = first[t] == INT_MAX;
+}
+
+__global__ void fu_unused_scatter_kernel(const int32_t *__restrict__ first, int32_t ntargets,
+                                         const int32_t *__restrict__ rank,
+                                         const int32_t *__restrict__ nused,
+                                         int32_t *__restrict__ out) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntargets;
+       t += (int64_t)gridDim.x * blockDim.x)
+    if (first[t] == INT_MAX) out[*nused + rank[t]] = (int32_t)t;
+}
+
+__global__ void fu_fill_kernel(int32_t *__restrict__ a, int64_t n, int32_t v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
 }  // namespace op2b
 
 using namespace op2b;
@@ -177,6 +244,50 @@ int op2b_incidence_arrays(uint64_t inc, uint64_t *ptr, uint64_t *list, int32_t *
   if (list) *list = reinterpret_cast<uint64_t>(I->list);
   if (max_degree) *max_degree = I->max_degree;
   return OP2B_OK;
+}
+
+int op2b_first_use_order(uint64_t map, int32_t arity, int64_t nelem, uint64_t elem_order,
+                         int32_t ntargets, uint64_t target_order, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (arity <= 0 || nelem < 0 || ntargets < 0 || (ntargets > 0 && !target_order) ||
+      (nelem > 0 && !map))
+    return set_error(OP2B_ERR_ARG, "first_use_order: arity %d nelem %lld targets %d", arity,
+                     (long long)nelem, ntargets);
+  const int64_t tot = nelem * arity;
+  if (tot >= INT_MAX) return set_error(OP2B_ERR_ARG, "first_use_order: %lld map entries", (long long)tot);
+  if (ntargets == 0) return OP2B_OK;
+  cudaStream_t s = stream_of(stream);
+  int32_t *first = nullptr, *flag = nullptr, *tflag = nullptr, *scal = nullptr;
+  const int32_t *m = reinterpret_cast<const int32_t *>(map);
+  const int32_t *ord = reinterpret_cast<const int32_t *>(elem_order);
+  int32_t *out = reinterpret_cast<int32_t *>(target_order);
+  int rc = dev_alloc((void **)&first, sizeof(int32_t) * (size_t)ntargets, s);
+  if (!rc) rc = dev_alloc((void **)&flag, sizeof(int32_t) * (size_t)std::max<int64_t>(tot, 1), s);
+  if (!rc) rc = dev_alloc((void **)&tflag, sizeof(int32_t) * (size_t)ntargets, s);
+  if (!rc) rc = dev_alloc((void **)&scal, sizeof(int32_t) * 2, s);
+  auto done = [&](int code) {
+    dev_free(first, s);
+    dev_free(flag, s);
+    dev_free(tflag, s);
+    dev_free(scal, s);
+    return code;
+  };
+  if (rc) return done(rc);
+  const int g1 = std::max(1, std::min<int>((int)((tot + 255) / 256), sm_count() * 8));
+  const int g2 = std::max(1, std::min<int>((int)((ntargets + 255) / 256), sm_count() * 8));
+  fu_fill_kernel<<<g2, 256, 0, s>>>(first, ntargets, INT_MAX);
+  if (tot > 0) {
+    fu_first_kernel<<<g1, 256, 0, s>>>(m, arity, nelem, ord, first);
+    fu_flag_kernel<<<g1, 256, 0, s>>>(m, arity, nelem, ord, first, flag);
+  }
+  rc = device_excl_scan(flag, flag, tot, scal, s);
+  if (rc) return done(rc);
+  if (tot > 0) fu_scatter_kernel<<<g1, 256, 0, s>>>(m, arity, nelem, ord, first, flag, out);
+  fu_unused_flag_kernel<<<g2, 256, 0, s>>>(first, ntargets, tflag);
+  rc = device_excl_scan(tflag, tflag, ntargets, scal + 1, s);
+  if (rc) return done(rc);
+  fu_unused_scatter_kernel<<<g2, 256, 0, s>>>(first, ntargets, tflag, scal, out);
+  return done(check_cuda(cudaGetLastError(), "op2b_first_use_order"));
 }
 
 int op2b_incidence_free(uint64_t inc) {

@@ -144,6 +144,26 @@ def p2_kernels(precision="f64"):
     return (stiff, "p2_stiffness_" + suffix), (mass, "p2_mass_" + suffix)
 
 
+def p2_km_kernel(precision="f64"):
+    """(code, name) of ONE kernel computing the stiffness entry into A and
+    the mass entry into M of local position (j, k): the two Mats of the P2
+    workload assembled by one par_loop, so the map, the coordinates and the
+    scatter positions are read once for both.  Each entry is computed by the
+    same arithmetic as :func:`p2_kernels`."""
+    real, xt, suffix = {"f64": ("double", "double", "f64"), "f32": ("float", "double", "f32"),
+                        "f32g": ("float", "float", "f32g")}[precision]
+    head = "#define REAL %s\n" % real + (_P2_COMMON % {"S": suffix}).replace("static __inline__ ", "static inline ")
+    stiff = (_P2_STIFF % {"name": "p2_km_stiff_" + suffix, "X": xt, "S": suffix}).replace(
+        "\nvoid ", "\nstatic inline void ", 1)
+    mass = (_P2_MASS % {"name": "p2_km_mass_" + suffix, "X": xt, "S": suffix}).replace(
+        "\nvoid ", "\nstatic inline void ", 1)
+    name = "p2_km_" + suffix
+    entry = ("\nvoid %s(double A[1][1], double M[1][1], %s *x[2], int j, int k) {\n"
+             "  p2_km_stiff_%s(A, x, j, k);\n  p2_km_mass_%s(M, x, j, k);\n}\n"
+             % (name, xt, suffix, suffix))
+    return head + stiff + mass + entry + "#undef REAL\n", name
+
+
 class Problem(object):
     pass
 
@@ -204,15 +224,22 @@ def build_p2(op2, n, seed=0, precision="f64", coords=None, elem=None):
     (ks, ns), (km, nm) = p2_kernels(precision)
     P.k_stiff = op2.Kernel(ks, ns)
     P.k_mass = op2.Kernel(km, nm)
+    kkm, nkm = p2_km_kernel(precision)
+    P.k_km = op2.Kernel(kkm, nkm)
     P.n_elem, P.n_dofs = len(elem), len(coords)
     return P
 
 
-def assemble_p2(op2, P):
-    for mat, k in ((P.K, P.k_stiff), (P.M, P.k_mass)):
-        op2.par_loop(k, P.elements(6, 6),
-                     mat((P.elem_dof[op2.i[0]], P.elem_dof[op2.i[1]]), op2.INC),
+def assemble_p2(op2, P, fused=True):
+    """K and M: by one par_loop computing both (``fused``, the default), or
+    by one par_loop per Mat."""
+    rows = (P.elem_dof[op2.i[0]], P.elem_dof[op2.i[1]])
+    if fused:
+        op2.par_loop(P.k_km, P.elements(6, 6), P.K(rows, op2.INC), P.M(rows, op2.INC),
                      P.coords(P.elem_vdof, op2.READ))
+        return
+    for mat, k in ((P.K, P.k_stiff), (P.M, P.k_mass)):
+        op2.par_loop(k, P.elements(6, 6), mat(rows, op2.INC), P.coords(P.elem_vdof, op2.READ))
 
 
 def assembly_bytes(n_elem, arity, n_nodes, nnz, coord_bytes=8, nmats=1):

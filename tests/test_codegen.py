@@ -427,3 +427,73 @@ def test_two_phase_forms(host_op2):
     spec = b200.loop_spec(b200.ParLoop(ki, e, b(em[0], op2.INC), b(em[0], op2.INC)),
                           inc_mode='lma', owner_mode='never')["spec"]
     assert spec.mode == "plan"
+
+
+def test_gather_form_of_the_airfoil_flux_loop(host_op2):
+    """The gather form (thread per target over the owner Map's incidence):
+    res_calc's two INC args through one Map qualify; a Global reduction or a
+    second INC Map does not (those loops keep another form)."""
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import airfoil
+    op2 = host_op2
+    cfg.configure(inc_mode="gather", staged_min_size=0)
+    A = airfoil.build(op2, 8, 4, 0, consts=False)
+    op2.Const(1, 1.4, "gam", np.float64), op2.Const(1, 0.4, "gm1", np.float64)
+    op2.Const(1, 0.05, "eps", np.float64), op2.Const(1, 0.9, "cfl", np.float64)
+    op2.Const(4, airfoil.freestream(), "qinf", np.float64)
+    try:
+        spec = spec_of(op2, A.k_res, A.edges,
+                       A.p_x(A.pedge[0], op2.READ), A.p_x(A.pedge[1], op2.READ),
+                       A.p_q(A.pevcell[0], op2.READ), A.p_q(A.pevcell[1], op2.READ),
+                       A.p_adt(A.pecell[0], op2.READ), A.p_adt(A.pecell[1], op2.READ),
+                       A.p_res(A.pevcell[0], op2.INC), A.p_res(A.pevcell[1], op2.INC))
+        assert spec.mode == "gather"
+        src, layout, _ = nvrtc_compile(spec)
+        assert "inc_order" in layout.fields and "atomic" not in src.split("op2b_res_calc")[-1]
+        for kahan in (False, True):
+            cfg.configure(kahan=kahan)
+            nvrtc_compile(spec_of(op2, A.k_res, A.edges,
+                                  A.p_x(A.pedge[0], op2.READ), A.p_x(A.pedge[1], op2.READ),
+                                  A.p_q(A.pevcell[0], op2.READ), A.p_q(A.pevcell[1], op2.READ),
+                                  A.p_adt(A.pecell[0], op2.READ), A.p_adt(A.pecell[1], op2.READ),
+                                  A.p_res(A.pevcell[0], op2.INC), A.p_res(A.pevcell[1], op2.INC)))
+        rms = op2.Global(1, 0.0, np.float64, "rms")
+        k = op2.Kernel("void k(double *a, double *b, double *g) { a[0] += 1.0; b[0] += 1.0; g[0] += 1.0; }", "k")
+        spec2 = spec_of(op2, k, A.edges, A.p_adt(A.pecell[0], op2.INC), A.p_adt(A.pecell[1], op2.INC),
+                        rms(op2.INC))
+        assert spec2.mode != "gather"
+    finally:
+        from pyop2_b200 import base
+        for c in list(base.Const._defs):
+            c.remove_from_namespace()
+
+
+def test_batched_coloured_form_compiles(host_op2):
+    """The coloured batched stub (a plan per instance, one launch per block
+    colour, thread colours inside a block) for the batching workload's three
+    loops: P1 mass and stiffness into Mats, RHS INC into a Dat."""
+    from pyop2_b200 import codegen as cg
+    from pyop2_b200.workloads import fem
+    op2 = host_op2
+    P = fem.build_p1(op2, 4, stiffness=True)
+    rows = (P.elem_node[op2.i[0]], P.elem_node[op2.i[1]])
+    for k, its, args in ((P.k_mass, P.elements(3, 3), (P.mat(rows, op2.INC), P.coords(P.elem_vnode, op2.READ))),
+                         (P.k_rhs, P.elements(3), (P.b(P.elem_node[op2.i[0]], op2.INC),
+                                                   P.coords(P.elem_vnode, op2.READ),
+                                                   P.f(P.elem_node, op2.READ)))):
+        spec = spec_of(op2, k, its, *args)
+        spec.mode = "plan"
+        spec.batch = 1
+        spec.mat_slots = any(a.kind == "mat" for a in spec.args)
+        spec.mat_alias = (0,) if spec.mat_slots else ()
+        src, layout, _ = nvrtc_compile(spec)
+        assert "p.blkmap[td.first]" in src
+        assert ("__ldg(p.ms0" in src) == spec.mat_slots
+    # a fused two-Mat loop shares one slot table load per entry
+    Q = fem.build_p2(op2, 2)
+    rows = (Q.elem_dof[op2.i[0]], Q.elem_dof[op2.i[1]])
+    spec = spec_of(op2, Q.k_km, Q.elements(6, 6), Q.K(rows, op2.INC), Q.M(rows, op2.INC),
+                   Q.coords(Q.elem_vdof, op2.READ))
+    assert spec.mode == "atomic" and spec.mat_alias == (0, 0) and spec.mat_per_entry
+    src, _, _ = nvrtc_compile(spec)
+    assert "p.ms1" not in src.split("extern \"C\"")[-1]

@@ -138,7 +138,7 @@ def test_autotuned_batch_and_graph_replay(op2):
     for insts in (mass, stiff, rhs):
         best, times = autotune.tune(insts, candidates=cands, reps=2, use_cache=False)
         assert best in [dict(c) for c in cands] and len(times) == 2
-        loops.append(batch.BatchLoop(insts, **best))
+        loops.append(autotune.build(insts, best))
     for P in G:
         P.mat.zero(); P.stiff.zero(); P.b.zero()
     for bl in loops:
@@ -158,3 +158,29 @@ def test_autotuned_batch_and_graph_replay(op2):
         assert rel_err(m, P.mat.array) < TOL
         assert rel_err(k, P.stiff.array) < TOL
         assert rel_err(b, P.b.data_ro) < TOL
+
+
+@pytest.mark.parametrize("part_size,bs", [(128, 128), (512, 256)])
+def test_coloured_batch_matches_oracle(op2, part_size, bs):
+    """The coloured batched form: every mesh carries its own plan (blocks of
+    ``part_size`` elements, block colours, thread colours), each launch runs
+    one block colour of every mesh; Mats and the RHS against the oracle."""
+    from pyop2_b200 import b200, batch
+    from pyop2_b200.workloads import batching
+    shapes = batching.mesh_shapes(24, seed=8)
+    G = batching.build(op2, shapes, seed=8)
+    loops = [batch.BatchLoop([i.recast("color", part_size) for i in insts], block_size=bs)
+             for insts in batching.instances(op2, G)]
+    assert all(bl.form == "color" and bl.launches >= 1 for bl in loops)
+    for P in G:
+        P.mat.zero(); P.stiff.zero(); P.b.zero()
+    for bl in loops:
+        bl.launch()
+    b200.synchronize()
+    for P in G:
+        Q = fem.build_p1(seq, 0, coords=P.coords.data_ro, elem=P.elem_node.values, stiffness=True)
+        fem.assemble_p1(seq, Q)
+        fem.assemble_p1_stiffness(seq, Q)
+        assert rel_err(P.mat.array, Q.mat.array) < TOL
+        assert rel_err(P.stiff.array, Q.stiff.array) < TOL
+        assert rel_err(P.b.data_ro, Q.b.data) < TOL

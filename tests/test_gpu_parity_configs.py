@@ -220,3 +220,42 @@ def test_served_requests_match_oracle(op2):
         checked[j.kind] += 1
     assert checked == {"quad": 3, "p1": 3}
     del consts, oconsts
+
+
+def _reference_kernels(api, A):
+    """Swap the chain's kernels for the reference demo's own kernel strings
+    (demo/airfoil_kernels.py), unchanged."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "airfoil_kernels.json")) as f:
+        code = json.load(f)["kernels"]
+    A.k_save = api.Kernel(code["save_soln"], "save_soln")
+    A.k_adt = api.Kernel(code["adt_calc"], "adt_calc")
+    A.k_res = api.Kernel(code["res_calc"], "res_calc")
+    A.k_bres = api.Kernel(code["bres_calc"], "bres_calc")
+    A.k_update = api.Kernel(code["update"], "update")
+    return A
+
+
+def test_reference_airfoil_kernel_strings_1200x600(op2):
+    """The reference user's airfoil kernels, exactly as its demo passes them
+    to op2.Kernel (float literals, its own local names), compiled by NVRTC
+    into the stubs and run on the 1200 x 600 permuted mesh in the default
+    forms, against the oracle running the same strings."""
+    grid = meshes.airfoil_grid(1200, 600, 0)
+    G = _reference_kernels(op2, airfoil.build(op2, 1200, 600, 0, grid=grid))
+    O = _reference_kernels(seq, airfoil.build(seq, 1200, 600, 0, grid=grid))
+    airfoil.save_soln(op2, G)
+    airfoil.save_soln(seq, O)
+    np.testing.assert_array_equal(G.p_qold.data_ro, O.p_qold.data)
+    airfoil.adt_calc(op2, G)
+    airfoil.adt_calc(seq, O)
+    np.testing.assert_array_equal(G.p_adt.data_ro, O.p_adt.data)
+    airfoil.res_calc(op2, G)
+    airfoil.res_calc(seq, O)
+    assert rel_err(G.p_res.data_ro, O.p_res.data) < TOL
+    for _ in range(2):
+        gr = airfoil.iteration(op2, G)
+        orr = airfoil.iteration(seq, O)
+        assert rel_err(gr.data, orr.data) < TOL
+    assert rel_err(G.p_q.data_ro, O.p_q.data) < TOL

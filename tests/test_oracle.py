@@ -188,3 +188,30 @@ def test_oracle_openmp_matches_sequential():
         seq.par_loop = orig
     assert np.abs(A.p_q.data - B.p_q.data).max() <= 1e-12 * np.abs(A.p_q.data).max()
     assert abs(ra.data[0] - rb.data[0]) <= 1e-12 * abs(ra.data[0])
+
+
+def test_reference_airfoil_kernel_strings_match_restated_kernels():
+    """The reference demo's airfoil kernels (tests/golden/airfoil_kernels.json,
+    from demo/airfoil_kernels.py) and this package's restated airfoil kernels
+    compute the same chain: three outer iterations on the oracle agree to
+    1e-13 (they differ only in operation order and float-literal spelling)."""
+    import json
+    from conftest import rel_err
+    from pyop2_b200.workloads import airfoil
+    with open(os.path.join(GOLDEN, "airfoil_kernels.json")) as f:
+        code = json.load(f)["kernels"]
+    seq._CONSTS.clear()
+    grid = meshes.airfoil_grid(40, 20, 5)
+    A = airfoil.build(seq, 40, 20, 5, grid=grid)
+    B = airfoil.build(seq, 40, 20, 5, grid=grid, consts=False)
+    B.k_save = seq.Kernel(code["save_soln"], "save_soln")
+    B.k_adt = seq.Kernel(code["adt_calc"], "adt_calc")
+    B.k_res = seq.Kernel(code["res_calc"], "res_calc")
+    B.k_bres = seq.Kernel(code["bres_calc"], "bres_calc")
+    B.k_update = seq.Kernel(code["update"], "update")
+    for _ in range(3):
+        ra = airfoil.iteration(seq, A)
+        rb = airfoil.iteration(seq, B)
+    assert rel_err(B.p_q.data, A.p_q.data) < 1e-13
+    assert rel_err(rb.data, ra.data) < 1e-13
+    seq._CONSTS.clear()
