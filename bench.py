@@ -923,7 +923,8 @@ def bench_assembly(op2, b200, reps=5, p2_ref=None):
     # ---- P2: the FP64 drop-in, its two-phase form, the precision form
     res = {}
     inc0 = cfg.cfg['inc_mode']
-    variants = (("f64", None, False), ("f64", "lma", False), ("f32", "lma", True))
+    variants = (("f64", None, False), ("f64", "lma", False), ("f32", "lma", False),
+                ("f32", "lma", True))
     for prec, mode, kahan in variants:
         tag = prec + ("_lma" if mode == "lma" else "") + ("_kahan" if kahan else "")
         cfg.configure(kahan=kahan, inc_mode=mode or inc0)

@@ -260,6 +260,18 @@ int op2b_incidence_free(uint64_t incidence);
  * pyop2/plan.pyx:107-110). */
 int op2b_first_use_order(uint64_t map, int32_t arity, int64_t nelem, uint64_t elem_order,
                          int32_t ntargets, uint64_t target_order, uint64_t stream);
+/* READ replicas in first-use order.  dst row i = src row index[i] (n rows of
+ * row_bytes, a multiple of 4); and dst_map[q] = r where order[r] ==
+ * map[q] (order a permutation of [0, ntargets)).  With order from
+ * op2b_first_use_order, a loop that only reads a Dat through a Map reads a
+ * copy of the Dat in order of first use through the renumbered Map: rows
+ * that neighbouring elements read lie next to each other.  No direct
+ * reference counterpart (the reference gathers through the user's
+ * numbering, pyop2/assets/cuda_indirect_loop.jinja2:105-150). */
+int op2b_rows_gather(uint64_t dst, uint64_t src, uint64_t index, int64_t n, int32_t row_bytes,
+                     uint64_t stream);
+int op2b_map_renumber(uint64_t dst_map, uint64_t map, int64_t n_entries, uint64_t order,
+                      int32_t ntargets, uint64_t stream);
 
 /* ------------------------------------------------------------------------
  * Two-phase deterministic INC.  A generated stub writes every element's INC

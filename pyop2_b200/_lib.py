@@ -81,6 +81,8 @@ _SIGS = {
     "op2b_incidence_arrays": [u64, u64p, u64p, i32p],
     "op2b_incidence_free": [u64],
     "op2b_first_use_order": [u64, i32, i64, u64, i32, u64, u64],
+    "op2b_rows_gather": [u64, u64, u64, i64, i32, u64],
+    "op2b_map_renumber": [u64, u64, i64, u64, i32, u64],
     "op2b_mat_incidence_build": [u64, u64, u64, u64, i32, i32, i32, i32, u64, u64p],
     "op2b_lma_reduce": [u64, i32, u64, u64, i32, u64, i64, i32, u64, i32, u64],
     "op2b_mat_zero_rows": [u64, u64, u64, i32, i32p, i32, C.c_double, i32, u64],

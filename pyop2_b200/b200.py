@@ -214,6 +214,10 @@ class Dat(DeviceDataMixin, base.Dat):
         base.Dat.__init__(self, dataset, data, dtype, name, soa, uid)
         self._state = DEVICE_UNALLOCATED
         self._device = None
+        # write generation: bumped by every path that may change the values
+        # (host write access, par_loop writes, zero, device arithmetic); READ
+        # replicas compare it to know they are current
+        self._wgen = 0
 
     # host views ---------------------------------------------------------
     @property
@@ -224,6 +228,7 @@ class Dat(DeviceDataMixin, base.Dat):
         self._from_device()
         if self._state is not DEVICE_UNALLOCATED:
             self._state = HOST
+        self._wgen += 1
         self.needs_halo_update = True
         return self._data
 
@@ -233,6 +238,7 @@ class Dat(DeviceDataMixin, base.Dat):
         self._data = verify_reshape(value, self.dtype, self._data.shape)
         if self._state is not DEVICE_UNALLOCATED:
             self._state = HOST
+        self._wgen += 1
 
     @property
     def data_ro(self):
@@ -286,6 +292,7 @@ class Dat(DeviceDataMixin, base.Dat):
         self._allocate_device()
         self._device.memset(0)
         self._state = DEVICE
+        self._wgen += 1
 
     # ------------------------------------------------ arithmetic on the device
     # pyop2/base.py:749-797 computed these on the host copies; here float64 /
@@ -319,6 +326,7 @@ class Dat(DeviceDataMixin, base.Dat):
             out._allocate_device()
         call("op2b_vec_binop", out._device.ptr, self._device.ptr, yptr, ys, n, op, code, 0)
         out._state = DEVICE
+        out._wgen += 1
         maybe_setflags(out._data, write=False)
         return True
 
@@ -705,6 +713,7 @@ class Solver(base.Solver):
              float(p['divergence_tolerance']), max_it, C.byref(its), C.byref(reason),
              hist.ctypes.data_as(C.POINTER(C.c_double)), 0)
         x._state = DEVICE
+        x._wgen += 1
         maybe_setflags(x._data, write=False)
         x.needs_halo_update = True
         self.iterations, self.reason = its.value, reason.value
@@ -862,6 +871,77 @@ class RegionPlan(object):
                 _lib._lib.op2b_region_plan_free(h)
         except Exception:
             pass
+
+
+_REPLICAS = {}
+
+
+class ReadReplica(object):
+    """A device copy of a Dat in order of first use through a Map, with the
+    Map renumbered to match (op2b_first_use_order, op2b_rows_gather,
+    op2b_map_renumber).  A loop that only reads the Dat through that Map in
+    element order reads neighbouring rows for neighbouring elements.  The
+    copy is refreshed from the Dat whenever the Dat's write generation
+    changed since the last refresh; the renumbered Map is built once (Maps
+    do not change once on the device)."""
+
+    def __init__(self, dat, m):
+        import weakref
+        self.dat_ref, self.map_ref = weakref.ref(dat), weakref.ref(m)
+        n = m.dataset.total_size
+        self.rows = DeviceBuffer(max(dat._data.nbytes, 16))
+        self.order = DeviceBuffer(max(n, 1) * 4)
+        self.map = DeviceBuffer(max(m.values.size, 1) * 4)
+        call("op2b_first_use_order", m._to_device().ptr, m.dim, m.iterset.total_size, 0, n,
+             self.order.ptr, 0)
+        call("op2b_map_renumber", self.map.ptr, m._to_device().ptr, m.iterset.total_size * m.dim,
+             self.order.ptr, n, 0)
+        self.wgen = None
+
+    def ensure(self, dat):
+        """Refresh the copy if the Dat changed since the last refresh."""
+        if dat._state is HOST:
+            dat._to_device()
+        if self.wgen != dat._wgen:
+            call("op2b_rows_gather", self.rows.ptr, dat._device.ptr, self.order.ptr,
+                 dat.dataset.total_size, dat.dtype.itemsize * dat.cdim, 0)
+            self.wgen = dat._wgen
+
+
+def read_replica(dat, m):
+    key = (id(dat), id(m))
+    rep = _REPLICAS.get(key)
+    if rep is None or rep.dat_ref() is not dat or rep.map_ref() is not m:
+        rep = _REPLICAS[key] = ReadReplica(dat, m)
+    return rep
+
+
+def replica_candidates(spec, specs, dats, maps):
+    """(Dat slot, Map slot) pairs a loop can read through a READ replica:
+    the Dat is read-only in the loop and read only through that Map (no
+    direct access), and the Map serves no other Dat, Mat or INC arg; rows
+    of a size that is a multiple of 4 bytes.  Only loops that walk their
+    elements in set order (the atomic form) gain from it."""
+    if spec.mode != "atomic":
+        return []
+    out = []
+    for k in range(len(maps)):
+        users = [s for s in specs if s.kind in ("ind", "vec", "its", "mat") and
+                 (s.mslot == k or (s.kind == "mat" and s.cmslot == k))]
+        if not users or any(s.kind == "mat" or s.access != "READ" for s in users):
+            continue
+        slots = {s.slot for s in users}
+        if len(slots) != 1:
+            continue
+        j = slots.pop()
+        d_uses = [s for s in specs if s.kind in ("ind", "vec", "its", "direct") and s.slot == j]
+        if any(s.kind == "direct" or s.access != "READ" or s.mslot != k for s in d_uses):
+            continue
+        d = dats[j]
+        if d.soa or (d.dtype.itemsize * d.cdim) % 4:
+            continue
+        out.append((j, k))
+    return out
 
 
 _GATHER_ORDER_CACHE = {}
@@ -1432,6 +1512,14 @@ class _BoundLoop(object):
         if spec.mat_slots:
             vals.update(mat_slot_values(specs, maps, mats))
         vals["err"] = _state['err'].ptr
+        # READ replicas: (Dat slot, Dat, replica); the stub reads the copy
+        # through the renumbered Map
+        self.replicas = []
+        if cfg.cfg['read_replicas'] and iterset.size >= int(cfg.cfg['replica_min_size']):
+            for j, k in replica_candidates(spec, specs, dats, maps):
+                rep = read_replica(dats[j], maps[k])
+                vals["m%d" % k] = rep.map.ptr
+                self.replicas.append((j, dats[j], rep))
         self.vals = vals
         n = iterset.size
         self.range_end = n
@@ -1527,6 +1615,8 @@ class _BoundLoop(object):
             vals["d%d" % j] = d._device.ptr
             if d.soa:
                 vals["ds%d" % j] = d.dataset.total_size
+        for j, d, rep in self.replicas:
+            vals["d%d" % j] = rep.rows.ptr
         gargs = [k for k, a in enumerate(loop.args) if a._is_global]
         # (field offset of the Global's pointer, arg index, reducing?)
         self._gbl = []
@@ -1559,6 +1649,8 @@ class _BoundLoop(object):
                 d._to_device()
             elif st is DEVICE_UNALLOCATED:
                 raise DeviceError("Dat %s lost its device copy" % d.name)
+        for j, d, rep in self.replicas:
+            rep.ensure(d)
         buf = self._buf
         args = loop.args
         for k, (off, ai, red) in enumerate(self._gbl):
@@ -1598,6 +1690,7 @@ class _BoundLoop(object):
                      arity, mask, flags, 0)
         for d in self._written:
             d._state = DEVICE
+            d._wgen += 1
             maybe_setflags(d._data, write=False)
         for k in self._reducing:
             args[self._gbl[k][1]].data._state = DEVICE
@@ -1618,7 +1711,9 @@ def _env_key():
                        (cfg.cfg['block_size'], cfg.cfg['partition_size'], cfg.cfg['fmad'],
                         cfg.cfg['min_blocks_per_sm'], cfg.cfg['inc_mode'], cfg.cfg['owner_mode'],
                         cfg.cfg['kahan'], cfg.cfg['mat_slots'], cfg.cfg['region_size'],
-                        cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size']))
+                        cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size'],
+                        cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
+                        cfg.cfg['replica_min_size']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

@@ -235,6 +235,7 @@ class LoopInstance(object):
         """Record that the device copies of written data are now newer."""
         for d in self.written:
             d._state = b200.DEVICE
+            d._wgen += 1
         for g in self.reducing:
             g._state = b200.DEVICE
         for m in self.mats:

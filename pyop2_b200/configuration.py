@@ -63,6 +63,13 @@ keys of the B200 backend:
   the kernel call that computed it instead of after the whole local tensor
   (one entry live in registers instead of the tensor; Mats on one Sparsity
   through one Map pair share one slot load);
+* ``read_replicas``: a loop of the atomic form (no plan, elements in set
+  order) on a set of at least ``replica_min_size`` elements that only reads
+  a Dat through a Map reads a device copy of the Dat kept in order of first
+  use through that Map, through the Map renumbered to match: rows
+  neighbouring elements read lie next to each other.  The copy is refreshed
+  when the Dat was written since (host writes, loops, zero, arithmetic);
+  it costs one extra copy of the Dat and of the Map;
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;
 * ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
@@ -95,6 +102,8 @@ _defaults = {
     'kahan': False,
     'mat_slots': True,
     'mat_per_entry': True,
+    'read_replicas': True,
+    'replica_min_size': 262144,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

@@ -177,6 +177,32 @@ __global__ void fu_fill_kernel(int32_t *__restrict__ a, int64_t n, int32_t v) {
     a[i] = v;
 }
 
+// ---- row gather and Map renumbering (READ replicas in first-use order)
+__global__ void rows_gather_kernel(uint32_t *__restrict__ dst, const uint32_t *__restrict__ src,
+                                   const int32_t *__restrict__ index, int64_t n, int words) {
+  const int64_t tot = n * words;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = q / words;
+    const int w = (int)(q - i * words);
+    dst[q] = src[(int64_t)index[i] * words + w];
+  }
+}
+
+__global__ void inverse_kernel(const int32_t *__restrict__ order, int32_t n,
+                               int32_t *__restrict__ inv) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    inv[order[i]] = (int32_t)i;
+}
+
+__global__ void renumber_kernel(int32_t *__restrict__ dst, const int32_t *__restrict__ map,
+                                int64_t n, const int32_t *__restrict__ inv) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    dst[q] = inv[map[q]];
+}
+
 }  // namespace op2b
 
 using namespace op2b;
@@ -288,6 +314,44 @@ int op2b_first_use_order(uint64_t map, int32_t arity, int64_t nelem, uint64_t el
   if (rc) return done(rc);
   fu_unused_scatter_kernel<<<g2, 256, 0, s>>>(first, ntargets, tflag, scal, out);
   return done(check_cuda(cudaGetLastError(), "op2b_first_use_order"));
+}
+
+int op2b_rows_gather(uint64_t dst, uint64_t src, uint64_t index, int64_t n, int32_t row_bytes,
+                     uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (n < 0 || row_bytes <= 0 || row_bytes % 4 || (n > 0 && (!dst || !src || !index)))
+    return set_error(OP2B_ERR_ARG, "rows_gather: n %lld row_bytes %d", (long long)n, row_bytes);
+  if (n == 0) return OP2B_OK;
+  const int words = row_bytes / 4;
+  const int64_t tot = n * words;
+  const int grid = std::max(1, std::min<int>((int)std::min<int64_t>((tot + 255) / 256, INT_MAX),
+                                             sm_count() * 8));
+  rows_gather_kernel<<<grid, 256, 0, stream_of(stream)>>>(
+      reinterpret_cast<uint32_t *>(dst), reinterpret_cast<const uint32_t *>(src),
+      reinterpret_cast<const int32_t *>(index), n, words);
+  return check_cuda(cudaGetLastError(), "rows_gather_kernel");
+}
+
+int op2b_map_renumber(uint64_t dst_map, uint64_t map, int64_t n_entries, uint64_t order,
+                      int32_t ntargets, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (n_entries < 0 || ntargets < 0 || (n_entries > 0 && (!dst_map || !map || !order)))
+    return set_error(OP2B_ERR_ARG, "map_renumber: %lld entries, %d targets", (long long)n_entries,
+                     ntargets);
+  if (n_entries == 0 || ntargets == 0) return OP2B_OK;
+  cudaStream_t s = stream_of(stream);
+  int32_t *inv = nullptr;
+  int rc = dev_alloc((void **)&inv, sizeof(int32_t) * (size_t)ntargets, s);
+  if (rc) return rc;
+  const int g1 = std::max(1, std::min<int>((int)((ntargets + 255) / 256), sm_count() * 8));
+  const int g2 = std::max(1, std::min<int>((int)std::min<int64_t>((n_entries + 255) / 256, INT_MAX),
+                                           sm_count() * 8));
+  inverse_kernel<<<g1, 256, 0, s>>>(reinterpret_cast<const int32_t *>(order), ntargets, inv);
+  renumber_kernel<<<g2, 256, 0, s>>>(reinterpret_cast<int32_t *>(dst_map),
+                                     reinterpret_cast<const int32_t *>(map), n_entries, inv);
+  rc = check_cuda(cudaGetLastError(), "renumber_kernel");
+  dev_free(inv, s);
+  return rc;
 }
 
 int op2b_incidence_free(uint64_t inc) {

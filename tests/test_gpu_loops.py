@@ -648,3 +648,37 @@ class TestCapture:
             with b200.capture():
                 op2.par_loop(k, s, x(op2.IdentityMap, op2.RW), fresh(op2.INC))
         graph.close()
+
+
+def test_read_replica_follows_writes(backend):
+    """A loop that only reads a Dat through a Map reads a copy of it in
+    first-use order (READ replica); writes to the Dat from the host, from
+    another par_loop and by zero() are seen by the next run."""
+    from pyop2_b200 import b200, op2
+    from pyop2_b200 import configuration as cfg
+    cfg.configure(replica_min_size=0)
+    rng = np.random.default_rng(4)
+    nodes, cells = op2.Set(500, 2), op2.Set(300)
+    m = rng.integers(0, 500, size=(300, 3)).astype(np.int32)
+    cn = op2.Map(cells, nodes, 3, m, "cn")
+    x = op2.Dat(nodes, rng.standard_normal((500, 2)), np.float64, "x")
+    out = op2.Dat(cells, np.zeros(300), np.float64, "out")
+    k = op2.Kernel("void k(double *a, double *b, double *c, double *o) {"
+                   " o[0] = a[0] * 2.0 + b[1] - c[0] * c[1]; }", "k")
+
+    def run():
+        op2.par_loop(k, cells, x(cn[0], op2.READ), x(cn[1], op2.READ), x(cn[2], op2.READ),
+                     out(op2.IdentityMap, op2.WRITE))
+        xv = x.data_ro
+        want = xv[m[:, 0], 0] * 2.0 + xv[m[:, 1], 1] - xv[m[:, 2], 0] * xv[m[:, 2], 1]
+        np.testing.assert_array_equal(out.data_ro, want)
+    run()
+    bound = [bl for bl in b200.ParLoop._bound_cache.values() if bl.spec.kernel_name == "k"]
+    assert bound and bound[-1].replicas
+    x.data[:] = rng.standard_normal((500, 2))            # host write
+    run()
+    op2.par_loop(op2.Kernel("void w(double *a) { a[0] += 1.0; a[1] *= -3.0; }", "w"), nodes,
+                 x(op2.IdentityMap, op2.RW))             # device write
+    run()
+    x.zero()
+    run()
