@@ -249,6 +249,8 @@ class PatchedInstance(object):
     memory owned by the caller, so there is no host copy to synchronise."""
 
     __slots__ = ("spec", "key", "size", "params")
+    form = "atomic"     # patched instances run the atomic batched form
+    plan = None
 
     def __init__(self, template, params):
         self.spec, self.key, self.size = template.spec, template.key, template.size
