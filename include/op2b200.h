@@ -134,6 +134,14 @@ int op2b_function_occupancy(uint64_t fn, uint32_t block, uint32_t smem, int32_t 
  * The generated stubs all take a single struct argument. */
 int op2b_launch(uint64_t fn, uint32_t grid, uint32_t block, uint32_t smem,
                 uint64_t stream, const void *params, uint64_t nbytes);
+/* on != 0: op2b_launch and op2b_launch_colored launch with programmatic
+ * stream serialisation, so a stub's CTAs may be scheduled while the kernel
+ * before it on the stream finishes; the generated stubs wait for that
+ * kernel's completion (griddepcontrol.wait) before touching memory, so
+ * results are unchanged.  Only for functions of generated stubs.  No
+ * reference counterpart (the reference synchronised the host after every
+ * par_loop, pyop2/cuda.py:656-658). */
+int op2b_set_programmatic_launch(int32_t on);
 /* Colour-by-colour launch of an indirect stub: for colour c the int32 pair at
  * params+col_field_offset is set to (first block of c, blocks in c) and the
  * stub is launched on grid = blocks in c.  Replaces the per-colour host loop

@@ -62,6 +62,7 @@ _SIGS = {
     "op2b_function_set_smem": [u64, i32],
     "op2b_function_occupancy": [u64, u32, u32, i32p],
     "op2b_launch": [u64, u32, u32, u32, u64, P, u64],
+    "op2b_set_programmatic_launch": [i32],
     "op2b_launch_colored": [u64, i32, i32p, u32, u32, u64, P, u64, u64],
     "op2b_plan_build": [i32, i32, i32, u64p, i32p, i32p, i32p, i32p, i32p,
                         i32, i32p, i32p, u64p, i32p, i32p, i32, u64, u64p],

@@ -63,6 +63,7 @@ def _setup():
     fetch = int(cfg.cfg['l2_fetch_granularity'])
     if fetch:
         call("op2b_set_l2_fetch_granularity", fetch)
+    call("op2b_set_programmatic_launch", 1 if cfg.cfg['programmatic_launch'] else 0)
     reserve = int(float(cfg.cfg['pool_reserve_gb']) * (1 << 30))
     reserve = min(reserve, tot.value // 4)
     if reserve > 0:
@@ -1363,6 +1364,12 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
             # entries added one by one (scalar Mats only; the kernel of one
             # (i0, i1) writes its own entry)
             spec.mat_per_entry = bool(cfg.cfg['mat_per_entry'])
+    if (fmad is None and cfg.cfg['fmad_inc'] and not cfg.cfg['fmad']
+            and spec.mode in ("staged", "atomic", "gather", "plan")
+            and any(a.access == "INC" and a.kind != "gbl" for a in specs)):
+        # loops whose INC sums are reassociated anyway (colour, atomic or
+        # staged order): the element code may contract multiply-adds
+        spec.fmad = True
     gspecs = [s for s in specs if s.kind == "gbl"]
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
@@ -1713,7 +1720,7 @@ def _env_key():
                         cfg.cfg['kahan'], cfg.cfg['mat_slots'], cfg.cfg['region_size'],
                         cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size'],
                         cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
-                        cfg.cfg['replica_min_size']))
+                        cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

@@ -262,13 +262,24 @@ def generate(spec):
     w("}  // namespace op2b_user")
     w("#undef OP2_STRIDE")
     if spec.batch:
-        w(_batch_plan_body(spec) if spec.mode == "plan" else _batch_body(spec))
+        w(_enter(_batch_plan_body(spec) if spec.mode == "plan" else _batch_body(spec)))
         return "\n".join(out), layout, batch_stub_names(spec)[0]
     body = {"plan": _indirect_body, "atomic": _atomic_body, "lma": _atomic_body,
             "direct": _direct_body, "owner": _owner_body, "staged": _staged_body,
             "gather": _gather_body}[spec.mode](spec)
-    w(body)
+    w(_enter(body))
     return "\n".join(out), layout, stub_name(spec)
+
+
+def _enter(body):
+    """Every kernel of a stub begins with op2b_stub_enter() (wait for the
+    previous kernel on the stream, let the next one be scheduled)."""
+    out = []
+    for line in body.split("\n"):
+        out.append(line)
+        if line.startswith('extern "C" __global__') and line.rstrip().endswith("{"):
+            out.append("  op2b_stub_enter();")
+    return "\n".join(out)
 
 
 # ------------------------------------------------------------------ helpers

@@ -70,6 +70,14 @@ keys of the B200 backend:
   neighbouring elements read lie next to each other.  The copy is refreshed
   when the Dat was written since (host writes, loops, zero, arithmetic);
   it costs one extra copy of the Dat and of the Map;
+* ``fmad_inc``: compile the element code of loops with indirect INC in the
+  staged, atomic, gather and coloured forms with multiply-add contraction
+  (their sums are reassociated anyway, so they already differ from the
+  sequential order within rounding); other loops keep ``fmad``;
+* ``programmatic_launch``: launch the generated stubs with programmatic
+  stream serialisation, so a stub's CTAs are scheduled while the kernel
+  before it drains (each stub waits for that kernel's completion before it
+  touches memory);
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;
 * ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
@@ -104,6 +112,8 @@ _defaults = {
     'mat_per_entry': True,
     'read_replicas': True,
     'replica_min_size': 262144,
+    'fmad_inc': False,
+    'programmatic_launch': False,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

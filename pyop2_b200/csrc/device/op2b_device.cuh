@@ -20,6 +20,15 @@ typedef unsigned long long op2b_u64;
 
 #define OP2B_FULL_MASK 0xffffffffu
 
+// First statement of every generated stub: wait until the kernel before it
+// on the stream has completed and its writes are visible (a no-op when the
+// stub was launched without programmatic serialisation), then allow the
+// kernel after it to be scheduled.
+__device__ __forceinline__ void op2b_stub_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Asynchronous copy (cp.async) of one row of B bytes, B a multiple of 4,
 // from global to shared memory in 16-, 8- or 4-byte pieces as the size
 // allows; both addresses must be aligned to the piece size.

@@ -20,6 +20,11 @@ static int g_device = -1;
 static cudaStream_t g_stream = nullptr;
 static int g_sm_count = 0;
 static int g_smem_optin = 0;
+// Generated stubs launched through op2b_launch / op2b_launch_colored may
+// start while the previous kernel on the stream drains (programmatic
+// dependent launch); every stub waits for its predecessor's completion
+// (griddepcontrol.wait) before it touches memory.
+static bool g_programmatic = false;
 static std::mutex g_init_mutex;
 
 int set_error(int code, const char *fmt, ...) {
@@ -509,14 +514,39 @@ int op2b_function_occupancy(uint64_t fn, uint32_t block, uint32_t smem, int32_t 
   return OP2B_OK;
 }
 
+// One launch of a generated stub, with the programmatic-serialisation
+// attribute when that is on.
+static cudaError_t launch_stub(uint64_t fn, uint32_t grid, uint32_t block, uint32_t smem,
+                               cudaStream_t s, void **args) {
+  if (!g_programmatic)
+    return cudaLaunchKernel(reinterpret_cast<const void *>(fn), dim3(grid), dim3(block), args,
+                            smem, s);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, reinterpret_cast<const void *>(fn), args);
+}
+
+int op2b_set_programmatic_launch(int32_t on) {
+  OP2B_REQUIRE_INIT();
+  g_programmatic = on != 0;
+  return OP2B_OK;
+}
+
 int op2b_launch(uint64_t fn, uint32_t grid, uint32_t block, uint32_t smem, uint64_t stream,
                 const void *params, uint64_t nbytes) {
   OP2B_REQUIRE_INIT();
   (void)nbytes;
   if (grid == 0) return OP2B_OK;
   void *args[1] = {const_cast<void *>(params)};
-  OP2B_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(fn), dim3(grid), dim3(block), args,
-                             smem, stream_of(stream)));
+  OP2B_CUDA(launch_stub(fn, grid, block, smem, stream_of(stream), args));
   return OP2B_OK;
 }
 
@@ -536,8 +566,7 @@ int op2b_launch_colored(uint64_t fn, int32_t ncolors, const int32_t *ncolblk, ui
       fields[1] = nb;
       // The parameter block is copied at launch, so it may be patched for the
       // next colour straight away.
-      OP2B_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(fn), dim3(nb), dim3(block), args,
-                                 smem, stream_of(stream)));
+      OP2B_CUDA(launch_stub(fn, nb, block, smem, stream_of(stream), args));
     }
     first += nb;
   }
