@@ -1364,6 +1364,12 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
             # entries added one by one (scalar Mats only; the kernel of one
             # (i0, i1) writes its own entry)
             spec.mat_per_entry = bool(cfg.cfg['mat_per_entry'])
+            split = cfg.cfg['itspace_split']
+            if (split and spec.mat_per_entry and len(extents) == 2
+                    and all(s.kind == "mat" or s.access == "READ" for s in specs)):
+                nr, nc = (int(v) for v in str(split).lower().split("x"))
+                if 1 <= nr <= extents[0] and 1 <= nc <= extents[1] and nr * nc > 1:
+                    spec.itspace_split = (nr, nc)
     if (fmad is None and cfg.cfg['fmad_inc'] and not cfg.cfg['fmad']
             and spec.mode in ("staged", "atomic", "gather", "plan")
             and any(a.access == "INC" and a.kind != "gbl" for a in specs)):
@@ -1579,6 +1585,10 @@ class _BoundLoop(object):
             self.range_end = omap.dataset.size
             self.grid = self._wave_grid(self.range_end, bs)
             self.max_grid = self.grid
+        elif spec.mode == "atomic" and spec.itspace_split:
+            nr, nc = spec.itspace_split
+            self.grid = self._wave_grid(n * nr * nc, bs)
+            self.max_grid = self.grid
         elif spec.mode == "owner":
             # one warp per target of the owner Map
             omap = maps[spec.owner["mslot"]]
@@ -1720,7 +1730,8 @@ def _env_key():
                         cfg.cfg['kahan'], cfg.cfg['mat_slots'], cfg.cfg['region_size'],
                         cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size'],
                         cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
-                        cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc']))
+                        cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc'],
+                        cfg.cfg['itspace_split']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

@@ -86,6 +86,10 @@ class LoopSpec(object):
         # (i0, i1) instead of after the whole local tensor (atomic form with
         # slot tables): one entry live at a time instead of the whole tensor
         self.mat_per_entry = False
+        # (row blocks, column blocks) of a 2-d iteration space handed to
+        # different warps of the atomic form (each warp evaluates its block
+        # of local positions for 32 elements); None: one thread per element
+        self.itspace_split = None
         # staged form over a locality partition (mode 'staged'): map_stage
         # {map slot: staged Map}, stage_arity, row_base (first loc row of each
         # staged Map), read_pairs / inc_pairs [(Dat slot, staged Map, ctype,
@@ -113,7 +117,7 @@ class LoopSpec(object):
                 self.block_size, self.fmad, self.min_blocks, self.mode,
                 tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
                 self.mat_slots, _freeze(self.region), tuple(self.mat_alias),
-                self.mat_per_entry)
+                self.mat_per_entry, self.itspace_split)
 
     @property
     def needs_coloring(self):
@@ -370,12 +374,21 @@ def _direct_body(spec):
     return "\n".join(L)
 
 
-def _itspace_open(spec, indent):
+def _itspace_open(spec, indent, ranges=None):
     out = []
     for k, ext in enumerate(spec.extents):
+        lo, hi = ranges[k] if ranges else (0, ext)
         out.append("%s#pragma unroll" % (indent + "  " * k))
-        out.append("%sfor (int i%d = 0; i%d < %d; ++i%d) {" % (indent + "  " * k, k, k, ext, k))
+        out.append("%sfor (int i%d = %d; i%d < %d; ++i%d) {" % (indent + "  " * k, k, lo, k, hi, k))
     return out
+
+
+def _split_ranges(spec):
+    """The local-position blocks of an itspace split: [((r0, r1), (c0, c1))]."""
+    (nr, nc), (e0, e1) = spec.itspace_split, spec.extents
+    rb = [(e0 * i // nr, e0 * (i + 1) // nr) for i in range(nr)]
+    cb = [(e1 * j // nc, e1 * (j + 1) // nc) for j in range(nc)]
+    return [(r, c) for r in rb for c in cb]
 
 
 def _itspace_close(spec, indent):
@@ -561,6 +574,28 @@ def _atomic_body(spec):
     coloured form (OP2 leaves their conflicts to the user)."""
     bs = spec.block_size
     L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
+    if spec.itspace_split:
+        # warp w evaluates block (w mod Q) of the local positions of the 32
+        # elements 32 * (w div Q) + lane (the block is warp-uniform)
+        blocks = _split_ranges(spec)
+        Q = len(blocks)
+        L.append("  const int lane = threadIdx.x & 31;")
+        L.append("  const op2b_i64 nw = ((op2b_i64)gridDim.x * %d) >> 5;" % bs)
+        L.append("  const op2b_i64 nwork = ((p.end - p.start + 31) >> 5) * %d;" % Q)
+        L.append("  for (op2b_i64 w = ((op2b_i64)blockIdx.x * %d + threadIdx.x) >> 5; w < nwork; w += nw) {"
+                 % bs)
+        L.append("    const int q = (int)(w %% %d);" % Q)
+        L.append("    const op2b_i64 e = p.start + (w / %d) * 32 + lane;" % Q)
+        L.append("    if (e >= p.end) continue;")
+        L.append("    switch (q) {")
+        for k, rng in enumerate(blocks):
+            L.append("    case %d: {" % k)
+            L += _atomic_element(spec, "      ", ranges=rng)
+            L.append("      break; }")
+        L.append("    }")
+        L.append("  }")
+        L.append("}")
+        return "\n".join(L)
     _gbl_prologue(spec, L)
     L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
              " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
@@ -828,7 +863,7 @@ def _inc_sink(spec, a, n, k, src, val, ind):
     return "%sop2b_atomic_row(%s, %s);" % (ind, src, val)
 
 
-def _atomic_element(spec, ind):
+def _atomic_element(spec, ind, ranges=None):
     """Lines computing element ``e`` of an atomic-mode (or two-phase)
     indirect loop."""
     L = []
@@ -896,7 +931,7 @@ def _atomic_element(spec, ind):
             if not spec.mat_per_entry:
                 apply += _mat_addto(spec, n, a, ind, atomic=True, lma=spec.mode == "lma")
     L += pre
-    L += _itspace_open(spec, ind)
+    L += _itspace_open(spec, ind, ranges)
     deep = ind + "  " * len(spec.extents)
     for n, a in enumerate(spec.args):
         if a.kind == "mat":

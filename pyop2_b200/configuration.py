@@ -78,6 +78,12 @@ keys of the B200 backend:
   stream serialisation, so a stub's CTAs are scheduled while the kernel
   before it drains (each stub waits for that kernel's completion before it
   touches memory);
+* ``itspace_split``: ``'RxC'`` (e.g. ``'2x2'``) splits the 2-d iteration
+  space of an atomic-form Mat assembly (scalar Mats added entry by entry,
+  every other argument READ) into R x C blocks of local positions evaluated
+  by different warps for the same 32 elements: fewer values live per
+  thread, more warps resident; ``''`` (default) keeps one thread per
+  element;
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;
 * ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
@@ -114,6 +120,7 @@ _defaults = {
     'replica_min_size': 262144,
     'fmad_inc': False,
     'programmatic_launch': False,
+    'itspace_split': '',
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }
