@@ -945,7 +945,7 @@ def bench_assembly(op2, b200, reps=5, p2_ref=None):
                     "K_plus_M_ms": round(ms, 3), "nnz_per_s": round(2 * nz / (ms * 1e-3), 1),
                     "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "algorithmic_bytes": nbytes,
                     "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3),
-                    "kahan": kahan, "element_math": prec, "mode": mode or inc0,
+                    "kahan": kahan, "element_math": prec, "mode": _loop_mode(Q.k_km.name),
                     "max_rel_err_K_vs_oracle": errs[0], "max_rel_err_M_vs_oracle": errs[1]}
         del Q
     cfg.configure(kahan=False, inc_mode=inc0)
