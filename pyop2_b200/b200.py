@@ -84,6 +84,9 @@ def _teardown():
         pass
     ParLoop._bound_cache.clear()
     _PLAN_CACHE.clear()
+    _REGION_CACHE.clear()
+    _GATHER_ORDER_CACHE.clear()
+    _REPLICAS.clear()
     _state['init'] = False
 
 
@@ -913,6 +916,9 @@ def read_replica(dat, m):
     key = (id(dat), id(m))
     rep = _REPLICAS.get(key)
     if rep is None or rep.dat_ref() is not dat or rep.map_ref() is not m:
+        # replicas of Dats or Maps that no longer exist free their memory
+        for k in [k for k, r in _REPLICAS.items() if r.dat_ref() is None or r.map_ref() is None]:
+            del _REPLICAS[k]
         rep = _REPLICAS[key] = ReadReplica(dat, m)
     return rep
 
@@ -1317,7 +1323,7 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
             if owner["kind"] == "dat" and w.kind != "its":
                 owner = None
     req = inc_mode or cfg.cfg['inc_mode']
-    gather = None
+    gather, gather_region = None, None
     if (owner is None and indirect and req == 'gather'
             and iterset.size >= int(cfg.cfg['staged_min_size'])):
         gather = codegen.owner_plan(spec, None)
@@ -1380,7 +1386,7 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
     return dict(spec=spec, specs=specs, dats=dats, maps=maps, mats=mats, gbls=gbls,
                 gbl_specs=gspecs, stages=stages, races=races, indirect=indirect,
                 iterset=iterset, block_size=bs,
-                gather_region=gather_region if spec.mode == "gather" else None)
+                gather_region=gather_region)
 
 
 def _same_values(m1, m2):
@@ -1466,6 +1472,12 @@ class _BoundLoop(object):
         iterset = info['iterset']
         args = loop.args
         self.spec = spec
+        if spec.mode == "staged" and cfg.cfg['staged_tl_regs']:
+            # target ids held in registers: as many per thread as the
+            # partition's largest block needs
+            rp0 = region_plan(iterset, maps, spec.region)
+            bs0 = spec.block_size
+            spec.region["tl_regs"] = [max(1, -(-int(c) // bs0)) for c in rp0.max_count]
         self.module = _get_module(spec)
         self.layout = self.module.layout
         self.indirect = indirect
@@ -1731,7 +1743,7 @@ def _env_key():
                         cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size'],
                         cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
                         cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc'],
-                        cfg.cfg['itspace_split']))
+                        cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

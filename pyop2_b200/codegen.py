@@ -687,6 +687,44 @@ def _staged_copy_rows(R, used, bs, ind, dst, n, tl):
     return L
 
 
+def _staged_copy_rows_regs(R, used, bs, ind, KR):
+    """Row copies of the staged READ rows with the target ids already in
+    registers (tg<stage>_<k> holds the id of row threadIdx.x + k * bs)."""
+    L = []
+    for st in used:
+        pairs = [(q, slot, t, c) for q, (slot, s_, t, c) in enumerate(R["read_pairs"]) if s_ == st]
+        if not pairs:
+            continue
+        for k in range(KR[st]):
+            L.append("%sif (threadIdx.x + %d < n_s%d) {" % (ind, k * bs, st))
+            L.append("%s  const int r = threadIdx.x + %d;" % (ind, k * bs))
+            L.append("%s  const op2b_i64 g = tg%d_%d;" % (ind, st, k))
+            for q, slot, t, c in pairs:
+                nb = c * _CSIZE[t]
+                if nb % 4 == 0:
+                    L.append("%s  op2b_cp_async_srow<%d>(rd%d, r, p.d%d + g * %d);" % (ind, nb, q, slot, c))
+                else:
+                    L.append("%s  for (int k = 0; k < %d; ++k) rd%d[r * %d + k] = p.d%d[g * %d + k];"
+                             % (ind, c, q, c, slot, c))
+            L.append("%s}" % ind)
+    return L
+
+
+def _staged_flush_regs(R, bs, ind, KR):
+    """Flush of the accumulated INC rows, one row per thread: the row read
+    from shared memory with vector loads, added to its target with the id
+    already in a register."""
+    L = []
+    for q, (slot, st, ctype, cdim) in enumerate(R["inc_pairs"]):
+        for k in range(KR[st]):
+            L.append("%sif (threadIdx.x + %d < n_s%d) {" % (ind, k * bs, st))
+            L.append("%s  __align__(16) %s cur[%d]; op2b_srow_load(cur, acc%d, threadIdx.x + %d);"
+                     % (ind, ctype, cdim, q, k * bs))
+            L.append("%s  op2b_atomic_row(p.d%d + (op2b_i64)tg%d_%d * %d, cur);" % (ind, slot, st, k, cdim))
+            L.append("%s}" % ind)
+    return L
+
+
 def _staged_element(spec, R, ind):
     """(decl, pre, post, exprs, adds) of one element of a staged stub."""
     read_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["read_pairs"])}
@@ -830,11 +868,23 @@ def _staged_body(spec):
     for st in used:
         L.append("  const int n_s%d = p.rg_tcnt[blk * %d + %d];" % (st, ns, st))
         L.append("  const int *tl_s%d = p.rg_tlist + p.rg_toff[blk * %d + %d];" % (st, ns, st))
+    KR = R.get("tl_regs")
+    if KR:
+        # the block's target ids, row r = threadIdx.x + k * bs in register
+        # k: one load each, issued with the loc rows below, reused by the
+        # row copies and by the flush
+        for st in used:
+            for k in range(KR[st]):
+                L.append("  const int tg%d_%d = threadIdx.x + %d < n_s%d ? tl_s%d[threadIdx.x + %d] : 0;"
+                         % (st, k, k * bs, st, st, k * bs))
     L += _staged_prefetch(spec, R, used, bs, "  ")
     for q, (slot, st, t, c) in enumerate(R["read_pairs"]):
         L.append("  %s *rd%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
         L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
-    L += _staged_copy_rows(R, used, bs, "  ", "rd%d", "n_s%d", "tl_s%d")
+    if KR:
+        L += _staged_copy_rows_regs(R, used, bs, "  ", KR)
+    else:
+        L += _staged_copy_rows(R, used, bs, "  ", "rd%d", "n_s%d", "tl_s%d")
     for q, (slot, st, t, c) in enumerate(R["inc_pairs"]):
         L.append("  %s *acc%d = (%s *)(op2b_smem + smem_off);" % (t, q, t))
         L.append("  smem_off += (n_s%d * %d * (int)sizeof(%s) + 15) & ~15;" % (st, c, t))
@@ -845,7 +895,10 @@ def _staged_body(spec):
     L.append("  __syncthreads();")
     _gbl_prologue(spec, L)
     L += _staged_passes(spec, R, used, bs, "  ")
-    L += _staged_flush(R, bs, "  ")
+    if KR:
+        L += _staged_flush_regs(R, bs, "  ", KR)
+    else:
+        L += _staged_flush(R, bs, "  ")
     _gbl_epilogue(spec, L)
     L.append("}")
     return "\n".join(L)

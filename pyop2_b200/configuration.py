@@ -41,6 +41,9 @@ keys of the B200 backend:
   size, whose default in the staged form is 384);
 * ``staged_block_size``: threads per CTA of the staged form's stubs (one
   CTA per block of the partition);
+* ``staged_tl_regs``: the staged stubs load their block's target ids into
+  registers once (with the element rows) and reuse them for the row copies
+  and the flush, which then adds one accumulated row per thread;
 * ``staged_min_size``: iteration sets smaller than this run the atomic form
   even when ``inc_mode`` is ``'staged'`` (a partition of them has too few
   blocks to fill the GPU);
@@ -121,6 +124,7 @@ _defaults = {
     'fmad_inc': False,
     'programmatic_launch': False,
     'itspace_split': '',
+    'staged_tl_regs': False,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

@@ -32,7 +32,7 @@ def _clear_consts(op2mod):
     seq._CONSTS.clear()
 
 
-@pytest.fixture(params=["atomic", "color", "lma", "staged"])
+@pytest.fixture(params=["atomic", "color", "lma", "staged", "gather"])
 def inc_mode(request):
     """Run a test under both INC conflict strategies of indirect loops."""
     from pyop2_b200 import configuration as cfg
@@ -438,3 +438,74 @@ def test_two_phase_kahan_precision_form(op2):
         assert rel_err(out[True][0], out[False][0]) < 1e-14
     finally:
         cfg.configure(inc_mode=old[0], kahan=old[1])
+
+
+@pytest.mark.parametrize("opts", [dict(programmatic_launch=True), dict(fmad_inc=True),
+                                  dict(staged_tl_regs=True), dict(read_replicas=True,
+                                                                  replica_min_size=0)])
+def test_airfoil_chain_launch_options_match_oracle(op2, opts):
+    """The launch-level options on the staged airfoil chain: programmatic
+    dependent launch (every stub waits for its predecessor), multiply-add
+    contraction in INC-form loops, target ids in registers, READ replicas on
+    small sets; q and rms within 1e-12 of the oracle after three
+    iterations."""
+    from pyop2_b200 import b200
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200._lib import call
+    _clear_consts(op2)
+    cfg.configure(staged_min_size=0, **opts)
+    if opts.get("programmatic_launch"):
+        call("op2b_set_programmatic_launch", 1)
+    try:
+        grid = meshes.airfoil_grid(60, 30, 4)
+        G = airfoil.build(op2, 60, 30, 4, grid=grid)
+        O = airfoil.build(seq, 60, 30, 4, grid=grid)
+        for _ in range(3):
+            gr = airfoil.iteration(op2, G)
+            orr = airfoil.iteration(seq, O)
+        assert rel_err(G.p_q.data_ro, O.p_q.data) < TOL
+        assert rel_err(gr.data, orr.data) < TOL
+        if opts.get("read_replicas"):
+            assert any(bl.replicas for bl in b200.ParLoop._bound_cache.values()
+                       if bl.spec.kernel_name == "adt_calc")
+    finally:
+        call("op2b_set_programmatic_launch", 0)
+        _clear_consts(op2)
+
+
+@pytest.mark.parametrize("split", ["3x2", "2x2", "6x1"])
+def test_p2_itspace_split_matches_oracle(op2, split):
+    """Mat assembly with the 6x6 local positions split across warps: both
+    Mats of the fused P2 loop within 1e-12 of the oracle."""
+    from pyop2_b200 import configuration as cfg
+    from pyop2_b200.workloads import fem
+    cfg.configure(itspace_split=split)
+    G, O = fem.build_p2(op2, 12, seed=3), fem.build_p2(seq, 12, seed=3)
+    fem.assemble_p2(op2, G)
+    fem.assemble_p2(seq, O)
+    assert rel_err(G.K.array, O.K.array) < TOL
+    assert rel_err(G.M.array, O.M.array) < TOL
+
+
+def test_gather_form_is_bit_exact(op2):
+    """The gather form adds each target's contributions in the sequential
+    backend's order (element order, then map index) with the same
+    arithmetic, so res_calc and bres_calc equal the oracle bit for bit."""
+    from pyop2_b200 import b200
+    from pyop2_b200 import configuration as cfg
+    _clear_consts(op2)
+    cfg.configure(inc_mode="gather", staged_min_size=0)
+    try:
+        grid = meshes.airfoil_grid(60, 30, 6)
+        G = airfoil.build(op2, 60, 30, 6, grid=grid)
+        O = airfoil.build(seq, 60, 30, 6, grid=grid)
+        for api, A in ((op2, G), (seq, O)):
+            airfoil.save_soln(api, A)
+            airfoil.adt_calc(api, A)
+            airfoil.res_calc(api, A)
+            airfoil.bres_calc(api, A)
+        assert {bl.spec.mode for bl in b200.ParLoop._bound_cache.values()
+                if bl.spec.kernel_name in ("res_calc", "bres_calc")} == {"gather"}
+        np.testing.assert_array_equal(G.p_res.data_ro, O.p_res.data)
+    finally:
+        _clear_consts(op2)
