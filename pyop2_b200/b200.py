@@ -1376,6 +1376,8 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
                 nr, nc = (int(v) for v in str(split).lower().split("x"))
                 if 1 <= nr <= extents[0] and 1 <= nc <= extents[1] and nr * nc > 1:
                     spec.itspace_split = (nr, nc)
+    if spec.mode == "direct":
+        spec.direct_unroll = max(1, int(cfg.cfg['direct_unroll']))
     if (fmad is None and cfg.cfg['fmad_inc'] and not cfg.cfg['fmad']
             and spec.mode in ("staged", "atomic", "gather", "plan")
             and any(a.access == "INC" and a.kind != "gbl" for a in specs)):
@@ -1743,7 +1745,8 @@ def _env_key():
                         cfg.cfg['staged_min_size'], cfg.cfg['staged_block_size'],
                         cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
                         cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc'],
-                        cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs']))
+                        cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs'],
+                        cfg.cfg['direct_unroll']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

@@ -26,6 +26,7 @@ synchronise per colour).  Per element the stub:
 """
 
 import os
+import re
 import struct
 
 _DEVICE_HEADER = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "device",
@@ -90,6 +91,9 @@ class LoopSpec(object):
         # different warps of the atomic form (each warp evaluates its block
         # of local positions for 32 elements); None: one thread per element
         self.itspace_split = None
+        # elements per thread per round of a direct stub (their loads issued
+        # together before the kernel calls)
+        self.direct_unroll = 1
         # staged form over a locality partition (mode 'staged'): map_stage
         # {map slot: staged Map}, stage_arity, row_base (first loc row of each
         # staged Map), read_pairs / inc_pairs [(Dat slot, staged Map, ctype,
@@ -117,7 +121,7 @@ class LoopSpec(object):
                 self.block_size, self.fmad, self.min_blocks, self.mode,
                 tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
                 self.mat_slots, _freeze(self.region), tuple(self.mat_alias),
-                self.mat_per_entry, self.itspace_split)
+                self.mat_per_entry, self.itspace_split, self.direct_unroll)
 
     @property
     def needs_coloring(self):
@@ -345,6 +349,26 @@ def _kernel_call(spec, argexprs, indent):
     return "%sop2b_user::%s(%s);" % (indent, spec.kernel_name, ", ".join(argexprs + itargs))
 
 
+def _direct_element_parts(spec, ind, e, sfx):
+    """(row declarations and loads, kernel call, stores) of element ``e``
+    of a direct loop, its row variables suffixed ``sfx``."""
+    pre, post, exprs = [], [], []
+    for n, a in enumerate(spec.args):
+        if a.kind == "gbl":
+            exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
+        else:
+            p0, q0 = [], []
+            x = _direct_row(a, n, e, p0, q0, ind)
+            ren = lambda t, n=n: re.sub(r"\ba%d\b" % n, "a%d%s" % (n, sfx), t)  # noqa: E731
+            pre += [ren(t) for t in p0]
+            post += [ren(t) for t in q0]
+            exprs.append(ren(x))
+    call = _itspace_open(spec, ind)
+    call.append(_kernel_call(spec, exprs, ind + "  " * len(spec.extents)))
+    call += _itspace_close(spec, ind)
+    return pre, call, post
+
+
 def _direct_element(spec, ind):
     """Lines computing element ``e`` of a direct loop."""
     pre, post, exprs = [], [], []
@@ -363,8 +387,50 @@ def _direct_element(spec, ind):
 
 def _direct_body(spec):
     bs = spec.block_size
+    U = spec.direct_unroll
     L = ["extern \"C\" __global__ void %s %s(const op2b_params p) {" % (_bounds(spec), stub_name(spec))]
     _gbl_prologue(spec, L)
+    if U > 1:
+        # U elements per thread per round, one grid stride apart: all their
+        # rows are loaded before any kernel call and stored after all of
+        # them, so the loads of the U elements are in flight together
+        # (elements of a direct loop touch only their own rows)
+        L.append("  const op2b_i64 stride = (op2b_i64)gridDim.x * %d;" % bs)
+        L.append("  for (op2b_i64 e0 = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e0 < p.end;"
+                 " e0 += stride * %d) {" % (bs, U))
+        parts = []
+        for u in range(U):
+            L.append("    const op2b_i64 e_%d = e0 + %d * stride;" % (u, u))
+            L.append("    const bool ok_%d = e_%d < p.end;" % (u, u))
+            parts.append(_direct_element_parts(spec, "      ", "e_%d" % u, "_%d" % u))
+        for u, (pre, call, post) in enumerate(parts):
+            decls, loads = [], []
+            for x in pre:
+                x = x.strip()
+                if x.startswith("__align__"):
+                    cut = x.index(";") + 1
+                    decls.append("    " + x[:cut])
+                    x = x[cut:].strip()
+                if x:
+                    loads.append("      " + x)
+            L += decls
+            if loads:
+                L.append("    if (ok_%d) {" % u)
+                L += loads
+                L.append("    }")
+        for u, (pre, call, post) in enumerate(parts):
+            L.append("    if (ok_%d) {" % u)
+            L += call
+            L.append("    }")
+        for u, (pre, call, post) in enumerate(parts):
+            if post:
+                L.append("    if (ok_%d) {" % u)
+                L += post
+                L.append("    }")
+        L.append("  }")
+        _gbl_epilogue(spec, L)
+        L.append("}")
+        return "\n".join(L)
     L.append("  for (op2b_i64 e = p.start + (op2b_i64)blockIdx.x * %d + threadIdx.x; e < p.end;"
              " e += (op2b_i64)gridDim.x * %d) {" % (bs, bs))
     L += _direct_element(spec, "    ")

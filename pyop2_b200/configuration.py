@@ -44,6 +44,8 @@ keys of the B200 backend:
 * ``staged_tl_regs``: the staged stubs load their block's target ids into
   registers once (with the element rows) and reuse them for the row copies
   and the flush, which then adds one accumulated row per thread;
+* ``direct_unroll``: elements each thread of a direct stub takes per round
+  (their rows all loaded before the kernel calls, so the loads overlap);
 * ``staged_min_size``: iteration sets smaller than this run the atomic form
   even when ``inc_mode`` is ``'staged'`` (a partition of them has too few
   blocks to fill the GPU);
@@ -125,6 +127,7 @@ _defaults = {
     'programmatic_launch': False,
     'itspace_split': '',
     'staged_tl_regs': False,
+    'direct_unroll': 1,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

@@ -505,7 +505,7 @@ def test_gather_form_is_bit_exact(op2):
             airfoil.res_calc(api, A)
             airfoil.bres_calc(api, A)
         assert {bl.spec.mode for bl in b200.ParLoop._bound_cache.values()
-                if bl.spec.kernel_name in ("res_calc", "bres_calc")} == {"gather"}
+                if bl.iterset is G.edges or bl.iterset is G.bedges} == {"gather"}
         np.testing.assert_array_equal(G.p_res.data_ro, O.p_res.data)
     finally:
         _clear_consts(op2)
