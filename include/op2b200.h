@@ -369,6 +369,15 @@ int op2b_mat_zero_rows(uint64_t vals, uint64_t rowptr, uint64_t colidx, int32_t 
  * (assets/cuda_matrix_support.jinja2:27-81) and PETSc's MatSetValues lookup. */
 int op2b_mat_slots_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64_t cmap,
                          int64_t nelem, int32_t ra, int32_t ca, uint64_t slots, uint64_t stream);
+/* Compact form of the same table: slots[r*nelem + e] (uint64) holds in byte
+ * c the position of (rmap[e][r], cmap[e][c]) counted from rowptr[rmap[e][r]]
+ * (255 where the Sparsity has no such entry); ca <= 8, and rows of at most
+ * 254 stored entries.  8 bytes per (element, local row) instead of 4 per
+ * local entry; the stubs add the row start they read through the Map.  No
+ * direct reference counterpart (see op2b_mat_slots_build). */
+int op2b_mat_slots_rel_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64_t cmap,
+                             int64_t nelem, int32_t ra, int32_t ca, uint64_t slots,
+                             uint64_t stream);
 /* op2b_mat_zero_rows for callers that must not allocate device memory.
  * No counterpart in the reference.
  *

@@ -92,6 +92,7 @@ _SIGS = {
     "op2b_vec_dot": [u64, u64, i64, C.POINTER(C.c_double), u64],
     "op2b_cg_solve": [u64, u64, u64, i32, i64, u64, u64, i32, C.c_double, C.c_double, C.c_double,
                       i32, i32p, i32p, C.POINTER(C.c_double), u64],
+    "op2b_mat_slots_rel_build": [u64, u64, u64, u64, i64, i32, i32, u64, u64],
     "op2b_mat_slots_build": [u64, u64, u64, u64, i64, i32, i32, u64, u64],
     "op2b_mat_zero_rows_static": [u64, u64, u64, i32, i32p, i32, C.c_double, i32, u64],
 }

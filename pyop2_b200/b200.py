@@ -535,6 +535,22 @@ class Sparsity(base.Sparsity):
         tables[key] = (buf, rmap, cmap)
         return buf
 
+    def _slot_table_rel(self, rmap, cmap):
+        """Compact scatter-slot table (op2b_mat_slots_rel_build): per element
+        and local row one 64-bit word of in-row positions, kept with the
+        Sparsity."""
+        tables = self.__dict__.setdefault("_slot_tables_rel", {})
+        key = (id(rmap), id(cmap))
+        hit = tables.get(key)
+        if hit is not None:
+            return hit[0]
+        n = rmap.iterset.size
+        buf = DeviceBuffer(max(1, n * rmap.dim) * 8)
+        call("op2b_mat_slots_rel_build", self._d_rowptr, self._d_colidx, rmap._to_device().ptr,
+             cmap._to_device().ptr, n, rmap.dim, cmap.dim, buf.ptr, 0)
+        tables[key] = (buf, rmap, cmap)
+        return buf
+
     def _mat_incidence(self, rmap, cmap):
         """CSR position -> the (element, r, c) local entries that add to it,
         in element order (op2b_mat_incidence_build), kept with the
@@ -1172,13 +1188,15 @@ def mat_alias(specs, mats):
     return tuple(alias)
 
 
-def mat_slot_values(specs, maps, mats):
-    """Parameter values ms<j>: the scatter-slot table of each Mat slot."""
+def mat_slot_values(specs, maps, mats, rel=False):
+    """Parameter values ms<j>: the scatter-slot table of each Mat slot (the
+    compact in-row table with ``rel``)."""
     vals = {}
     for s in specs:
         if s.kind == "mat" and "ms%d" % s.slot not in vals:
             m = mats[s.slot]
-            vals["ms%d" % s.slot] = m.sparsity._slot_table(maps[s.mslot], maps[s.cmslot]).ptr
+            get = m.sparsity._slot_table_rel if rel else m.sparsity._slot_table
+            vals["ms%d" % s.slot] = get(maps[s.mslot], maps[s.cmslot]).ptr
     return vals
 
 
@@ -1370,6 +1388,12 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
             # entries added one by one (scalar Mats only; the kernel of one
             # (i0, i1) writes its own entry)
             spec.mat_per_entry = bool(cfg.cfg['mat_per_entry'])
+            # compact in-row slot tables: per-entry adds, at most 8 columns
+            # per element and rows of at most 254 entries
+            if (spec.mat_per_entry and cfg.cfg['mat_slots_rel'] and _state['init']
+                    and all(s.carity <= 8 for s in specs if s.kind == "mat")
+                    and all(m.sparsity._max_row_nnz() <= 254 for m in mats)):
+                spec.mat_slots_rel = True
             split = cfg.cfg['itspace_split']
             if (split and spec.mat_per_entry and len(extents) == 2
                     and all(s.kind == "mat" or s.access == "READ" for s in specs)):
@@ -1537,7 +1561,7 @@ class _BoundLoop(object):
             vals["mr%d" % j] = m.sparsity._d_rowptr
             vals["mc%d" % j] = m.sparsity._d_colidx
         if spec.mat_slots:
-            vals.update(mat_slot_values(specs, maps, mats))
+            vals.update(mat_slot_values(specs, maps, mats, rel=spec.mat_slots_rel))
         vals["err"] = _state['err'].ptr
         # READ replicas: (Dat slot, Dat, replica); the stub reads the copy
         # through the renumbered Map
@@ -1746,7 +1770,7 @@ def _env_key():
                         cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
                         cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc'],
                         cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs'],
-                        cfg.cfg['direct_unroll']))
+                        cfg.cfg['direct_unroll'], cfg.cfg['mat_slots_rel']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

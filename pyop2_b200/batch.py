@@ -73,7 +73,7 @@ def _fields(info):
         for s in info['specs']:
             if s.kind == "mat" and s.slot not in seen:
                 seen.add(s.slot)
-                f.append(("ms%d" % s.slot, "slots",
+                f.append(("ms%d" % s.slot, "slotsrel" if spec.mat_slots_rel else "slots",
                           (info['mats'][s.slot], info['maps'][s.mslot], info['maps'][s.cmslot])))
     for j, d in enumerate(info['dats']):
         f.append(("d%d" % j, "dat", d))
@@ -96,6 +96,9 @@ def _bind(fields):
         elif kind == "slots":
             m, rmap, cmap = o
             vals[name] = m.sparsity._slot_table(rmap, cmap).ptr
+        elif kind == "slotsrel":
+            m, rmap, cmap = o
+            vals[name] = m.sparsity._slot_table_rel(rmap, cmap).ptr
         elif kind == "dat":
             o._to_device()
             vals[name] = o._device.ptr
@@ -190,7 +193,7 @@ class LoopInstance(object):
         new.mats = [r(m) for m in self.mats]
         new.written = [r(d) for d in self.written]
         new.reducing = [r(g) for g in self.reducing]
-        new.fields = [(n, k, tuple(r(x) for x in o) if k == "slots" else r(o))
+        new.fields = [(n, k, tuple(r(x) for x in o) if k in ("slots", "slotsrel") else r(o))
                       for n, k, o in self.fields]
         for (n, k, o), (_, _, o2) in zip(self.fields, new.fields):
             if k in ("dat", "gbl") and (o.dtype != o2.dtype or o.cdim != o2.cdim):

@@ -87,6 +87,8 @@ class LoopSpec(object):
         # (i0, i1) instead of after the whole local tensor (atomic form with
         # slot tables): one entry live at a time instead of the whole tensor
         self.mat_per_entry = False
+        # per-entry adds read the compact in-row table (op2b_mat_slots_rel_build)
+        self.mat_slots_rel = False
         # (row blocks, column blocks) of a 2-d iteration space handed to
         # different warps of the atomic form (each warp evaluates its block
         # of local positions for 32 elements); None: one thread per element
@@ -121,7 +123,8 @@ class LoopSpec(object):
                 self.block_size, self.fmad, self.min_blocks, self.mode,
                 tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
                 self.mat_slots, _freeze(self.region), tuple(self.mat_alias),
-                self.mat_per_entry, self.itspace_split, self.direct_unroll)
+                self.mat_per_entry, self.itspace_split, self.direct_unroll,
+                self.mat_slots_rel)
 
     @property
     def needs_coloring(self):
@@ -1084,8 +1087,16 @@ def _mat_add_entry(spec, ind):
         ri, ci = "i%d" % a.idx, "i%d" % a.cidx
         if tab not in loaded:
             loaded.add(tab)
-            L.append("%sconst int pos%d = __ldg(p.ms%d + (op2b_i64)(%s * %d + %s) * p.set_size + e);"
-                     % (ind, tab, tab, ri, a.carity, ci))
+            if spec.mat_slots_rel:
+                # the local row's word of in-row positions and the row start
+                L.append("%sconst unsigned long long w%d = __ldg((const unsigned long long *)p.ms%d"
+                         " + (op2b_i64)%s * p.set_size + e);" % (ind, tab, tab, ri))
+                L.append("%sconst int off%d = (int)((w%d >> (8 * %s)) & 0xffull);" % (ind, tab, tab, ci))
+                L.append("%sconst int pos%d = off%d == 255 ? -1 : __ldg(p.mr%d + mr%d[%s]) + off%d;"
+                         % (ind, tab, tab, tab, a.mslot, ri, tab))
+            else:
+                L.append("%sconst int pos%d = __ldg(p.ms%d + (op2b_i64)(%s * %d + %s) * p.set_size + e);"
+                         % (ind, tab, tab, ri, a.carity, ci))
             L.append("%sif (pos%d < 0) op2b_flag_missing(p.err, mr%d[%s], mr%d[%s]);"
                      % (ind, tab, a.mslot, ri, a.cmslot, ci))
         if a.access == "WRITE":

@@ -89,6 +89,10 @@ keys of the B200 backend:
   by different warps for the same 32 elements: fewer values live per
   thread, more warps resident; ``''`` (default) keeps one thread per
   element;
+* ``mat_slots_rel``: with per-entry adds, read each local row's columns
+  from a compact slot table (one 64-bit word of in-row positions per element
+  and local row, added to the row start read through the Map) instead of one
+  32-bit position per local entry;
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;
 * ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
@@ -128,6 +132,7 @@ _defaults = {
     'itspace_split': '',
     'staged_tl_regs': False,
     'direct_unroll': 1,
+    'mat_slots_rel': False,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

@@ -180,6 +180,60 @@ __global__ void mat_slots_kernel(const int32_t *__restrict__ rowptr,
 }
 }  // namespace op2b
 
+// ---- compact scatter-slot table: for element e and local row r, one 64-bit
+// word whose byte c is the position of (rmap[e][r], cmap[e][c]) within the
+// CSR row, counted from rowptr[row] (255: the Sparsity lacks the entry).
+// Rows of up to 254 stored entries and up to 8 columns per element.
+namespace op2b {
+__global__ void mat_slots_rel_kernel(const int32_t *__restrict__ rowptr,
+                                     const int32_t *__restrict__ colidx,
+                                     const int32_t *__restrict__ rmap,
+                                     const int32_t *__restrict__ cmap, int64_t nelem, int ra,
+                                     int ca, unsigned long long *__restrict__ out) {
+  const int64_t total = nelem * ra;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int r = static_cast<int>(t / nelem);
+    const int64_t e = t - (int64_t)r * nelem;
+    const int row = rmap[e * ra + r];
+    const int lo0 = rowptr[row], hi0 = rowptr[row + 1];
+    unsigned long long w = ~0ull;
+    for (int c = 0; c < ca; ++c) {
+      const int col = cmap[e * ca + c];
+      int lo = lo0, hi = hi0;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (colidx[mid] < col)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      const unsigned long long off =
+          (lo < hi0 && colidx[lo] == col && lo - lo0 < 255) ? (unsigned long long)(lo - lo0) : 255ull;
+      w = (w & ~(0xffull << (8 * c))) | (off << (8 * c));
+    }
+    out[(int64_t)r * nelem + e] = w;
+  }
+}
+}  // namespace op2b
+
+extern "C" int op2b_mat_slots_rel_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap,
+                                        uint64_t cmap, int64_t nelem, int32_t ra, int32_t ca,
+                                        uint64_t slots, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  if (nelem < 0 || ra <= 0 || ca <= 0 || ca > 8 ||
+      (nelem > 0 && (!rowptr || !colidx || !rmap || !cmap || !slots)))
+    return set_error(OP2B_ERR_ARG, "op2b_mat_slots_rel_build: bad arguments (ca %d)", ca);
+  if (nelem == 0) return OP2B_OK;
+  const int64_t work = nelem * ra;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256,
+                                                                           (int64_t)sm_count() * 16)));
+  mat_slots_rel_kernel<<<grid, 256, 0, stream_of(stream)>>>(
+      (const int32_t *)rowptr, (const int32_t *)colidx, (const int32_t *)rmap, (const int32_t *)cmap,
+      nelem, ra, ca, (unsigned long long *)slots);
+  return check_cuda(cudaGetLastError(), "mat_slots_rel_kernel");
+}
+
 extern "C" int op2b_mat_slots_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, uint64_t cmap,
                                     int64_t nelem, int32_t ra, int32_t ca, uint64_t slots,
                                     uint64_t stream) {
