@@ -510,7 +510,7 @@ def run_gpu(args, ws, rank, local):
         cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
                "sample": "OpenMP port, %d iters" % iters,
                "sequential": {"value": round(s_gbs, 3), "cores": 1, "iters": seq_iters,
-                              "p2_nnz_per_s": float("%.3g" % p2_nnz_s)}}
+                              "p2_Mnnz_s": round(p2_nnz_s / 1e6, 1)}}
         if q_out is not None:
             rel = np.abs(np.array(rms_hist) - s_rms) / np.maximum(np.abs(s_rms), 1e-300)
             parity = {"iters": seq_iters,
@@ -809,7 +809,7 @@ def bench_serving(op2, b200, nreq, rate, seed=0, n_p1=16, n_quad=16):
     ratio = round(s_eng["req_per_s"] / s_plain["req_per_s"], 2)
     summary = {"req_per_s_ratio": ratio, "req_per_s": s_eng["req_per_s"],
                "p50_ms": s_eng["p50_ms"], "p99_ms": s_eng["p99_ms"],
-               "plain_p99_ms": s_plain["p99_ms"],
+               "plain_p99_ms": round(s_plain["p99_ms"], 1),
                "err_vs_plain": float("%.3g" % max(err.values()))}
     return {"summary": summary,
             "trace": {"requests": nreq, "rate_per_s": rate, "p1_meshes": n_p1,
@@ -970,9 +970,9 @@ def bench_assembly(op2, b200, reps=5, p2_ref=None):
     def e(v):
         return None if v is None else float("%.3g" % v)
     out["summary"] = {
-        "p1_nnz_per_s": float("%.3g" % p1["mass_nnz_per_s"]),
+        "p1_Gnnz_s": round(p1["mass_nnz_per_s"] / 1e9, 2),
         "p1_frac": round(p1["mass_rhs_GBps"] / peak, 3),
-        "p2_nnz_per_s": float("%.3g" % f64["nnz_per_s"]), "p2_frac": f64["frac"],
+        "p2_Gnnz_s": round(f64["nnz_per_s"] / 1e9, 2), "p2_frac": f64["frac"],
         "p2_err": e(max(f64["max_rel_err_K_vs_oracle"] or 0, f64["max_rel_err_M_vs_oracle"] or 0)
                     if p2_ref is not None else None),
         "prec_frac": prec["frac"],
