@@ -109,6 +109,26 @@ int op2b_graph_begin(uint64_t stream);
 int op2b_graph_end(uint64_t stream, uint64_t *graph_exec);
 int op2b_graph_launch(uint64_t graph_exec, uint64_t stream);
 int op2b_graph_destroy(uint64_t graph_exec);
+/* Overlapped capture (no direct reference counterpart: the reference ran
+ * every par_loop in program order on one stream).  A capture on one stream
+ * records a linear chain of nodes.  op2b_graph_capture_tail returns the
+ * chain's last node so far (0 before the first); op2b_graph_end_capture ends
+ * the capture and returns the un-instantiated graph; op2b_graph_chain_positions
+ * gives each marked node's position on the chain (-1 for a 0 mark) and the
+ * chain length; op2b_graph_relax takes segments [seg_first[s], seg_last[s]]
+ * that tile the chain in order and, for each segment s > 0, replaces the chain
+ * edge into its first node by edges from the last nodes of the earlier
+ * segments dep_idx[dep_ptr[s] .. dep_ptr[s+1]), then instantiates the graph
+ * (nseg == 0: instantiate unchanged).  The graph stays owned by the caller:
+ * free it with op2b_graph_free. */
+int op2b_graph_capture_tail(uint64_t stream, uint64_t *node);
+int op2b_graph_end_capture(uint64_t stream, uint64_t *graph);
+int op2b_graph_chain_positions(uint64_t graph, const uint64_t *marks, int32_t nmarks,
+                               int64_t *pos, int64_t *nnodes);
+int op2b_graph_relax(uint64_t graph, const int64_t *seg_first, const int64_t *seg_last,
+                     int32_t nseg, const int32_t *dep_ptr, const int32_t *dep_idx,
+                     uint64_t *graph_exec);
+int op2b_graph_free(uint64_t graph);
 
 /* ------------------------------------------------------------------------
  * JIT modules.  Replaces cuda.JITModule.compile (pyop2/cuda.py:610-651):

@@ -53,6 +53,11 @@ _SIGS = {
     "op2b_graph_end": [u64, u64p],
     "op2b_graph_launch": [u64, u64],
     "op2b_graph_destroy": [u64],
+    "op2b_graph_capture_tail": [u64, u64p],
+    "op2b_graph_end_capture": [u64, u64p],
+    "op2b_graph_chain_positions": [u64, u64p, i32, i64p, i64p],
+    "op2b_graph_relax": [u64, i64p, i64p, i32, i32p, i32p, u64p],
+    "op2b_graph_free": [u64],
     "op2b_nvrtc_compile": [charp, charp, C.POINTER(charp), i32, C.POINTER(P), u64p, charp, u64],
     "op2b_cubin_free": [P],
     "op2b_module_load": [P, u64p],

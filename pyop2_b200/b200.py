@@ -25,7 +25,7 @@ import weakref
 
 import numpy as np
 
-from . import base, codegen
+from . import base, codegen, overlap
 from . import configuration as cfg
 from . import _lib
 from ._lib import call
@@ -41,7 +41,7 @@ DEVICE = 'DEVICE'
 BOTH = 'BOTH'
 
 _state = {'init': False, 'sm_count': 148, 'smem_optin': 232448, 'stream': 0, 'err': None,
-          'l2_bytes': 0}
+          'l2_bytes': 0, 'trace': None}
 
 
 def _setup():
@@ -1374,6 +1374,8 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
         ps = int(cfg.cfg['partition_size']) or 384
         R["part_size"] = ps = max(1, min(ps, 16384 // max(R["stage_arity"])))
         R["ept"] = (ps + bs - 1) // bs
+        if int(cfg.cfg['staged_pair']) == 2:
+            R["pair"] = 2
         indirect = False   # one launch over the locality partition's blocks
     elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'lma' and codegen.lma_capable(spec):
         spec.mode = "lma"
@@ -1521,6 +1523,21 @@ class _BoundLoop(object):
         # Dats the loop only writes, row by row over the whole set: a fresh
         # device copy needs no upload of the host values first
         self.write_only = {k for k, v in direct_write.items() if v}
+        # accesses of the bound Dats and Mats (Globals vary per call) for
+        # overlapped capture: atomic adds commute, other writes do not
+        atomic = spec.mode in ("staged", "atomic")
+        pairs = []
+        for a, s in zip(args, specs):
+            if s.kind == "gbl":
+                continue
+            if s.access == "READ":
+                kind = "R"
+            elif s.access == "INC" and atomic and s.kind != "direct":
+                kind = "I"
+            else:
+                kind = "W"
+            pairs.append((id(a.data), kind))
+        self.accesses = overlap.loop_accesses(pairs)
         self.refs = [weakref.ref(o) for o in dats + maps + mats]
         self.consts = base.Const._definitions()
         self.block_size = info['block_size']
@@ -1696,6 +1713,19 @@ class _BoundLoop(object):
                                            self.layout.nbytes)
 
     def run(self, loop):
+        trace = _state['trace']
+        if trace is None:
+            self._run(loop)
+            return
+        # overlapped capture: the chain's tail before and after this loop's
+        # nodes, and what the loop reads and writes
+        pre = _capture_tail()
+        self._run(loop)
+        args = loop.args
+        gbl = tuple((id(args[ai].data), "W" if red else "R") for _, ai, red in self._gbl)
+        trace.append((pre, _capture_tail(), self.accesses + gbl))
+
+    def _run(self, loop):
         if getattr(self, "_buf", None) is None:
             self._prepare(loop)
         for d in self.dats:
@@ -1770,7 +1800,8 @@ def _env_key():
                         cfg.cfg['mat_per_entry'], cfg.cfg['read_replicas'],
                         cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc'],
                         cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs'],
-                        cfg.cfg['direct_unroll'], cfg.cfg['mat_slots_rel']))
+                        cfg.cfg['direct_unroll'], cfg.cfg['mat_slots_rel'],
+                        cfg.cfg['staged_pair']))
         _ENV["gen"] = gen
     return _ENV["key"]
 
@@ -1903,6 +1934,7 @@ class Graph(object):
 
     def __init__(self):
         self.handle = 0
+        self.segments = None
 
     def launch(self):
         call("op2b_graph_launch", self.handle, 0)
@@ -1921,6 +1953,50 @@ class Graph(object):
             pass
 
 
+def _capture_tail():
+    node = C.c_uint64()
+    call("op2b_graph_capture_tail", 0, C.byref(node))
+    return node.value
+
+
+def _relaxed_exec(graph, trace):
+    """Instantiate the captured chain ``graph`` with the edges between
+    independent par_loops dropped (:mod:`pyop2_b200.overlap`); ``trace``
+    holds per loop the chain's tail before and after its nodes and its
+    accesses.  A loop of more than one node, and any node between loops,
+    is a barrier."""
+    marks = [m for pre, post, _ in trace for m in (pre, post)]
+    nm = len(marks)
+    pos = (C.c_int64 * max(nm, 1))()
+    nnodes = C.c_int64()
+    call("op2b_graph_chain_positions", graph, (C.c_uint64 * max(nm, 1))(*marks), nm, pos,
+         C.byref(nnodes))
+    segs, cursor = [], 0
+    for k, (_, _, acc) in enumerate(trace):
+        first, last = pos[2 * k] + 1, pos[2 * k + 1]
+        if last < first:
+            continue                      # the loop added no node
+        if first < cursor:
+            raise DeviceError("overlapped capture: loop %d's nodes are out of order" % k)
+        if first > cursor:
+            segs.append((cursor, first - 1, None))
+        segs.append((first, last, acc if last == first else None))
+        cursor = last + 1
+    if cursor < nnodes.value:
+        segs.append((cursor, nnodes.value - 1, None))
+    deps = overlap.dependencies([acc for _, _, acc in segs])
+    ptr, idx = [0], []
+    for d in deps:
+        idx.extend(d)
+        ptr.append(len(idx))
+    ns = len(segs)
+    h = C.c_uint64()
+    call("op2b_graph_relax", graph, (C.c_int64 * max(ns, 1))(*[a for a, _, _ in segs]),
+         (C.c_int64 * max(ns, 1))(*[b for _, b, _ in segs]), ns,
+         (C.c_int32 * (ns + 1))(*ptr), (C.c_int32 * max(len(idx), 1))(*idx), C.byref(h))
+    return h.value, [(acc is not None, d) for (_, _, acc), d in zip(segs, deps)]
+
+
 class capture(object):
     """Record the par_loops issued inside the block into a CUDA graph instead
     of running them::
@@ -1930,21 +2006,45 @@ class capture(object):
         g.launch()
 
     Every loop must have run once before (its stub, plan and device data
-    exist), and the block must not read results on the host."""
+    exist), and the block must not read results on the host.
+
+    ``overlap`` (default: the ``graph_overlap`` configuration key) lets
+    loops that touch no common data in a conflicting way run side by side
+    in the graph (:mod:`pyop2_b200.overlap`); other device work recorded in
+    the block stays in program order with everything around it."""
+
+    def __init__(self, overlap=None):
+        self.overlap = bool(cfg.cfg['graph_overlap']) if overlap is None else bool(overlap)
 
     def __enter__(self):
         self.graph = Graph()
         call("op2b_graph_begin", 0)
         _state['capturing'] = True
+        _state['trace'] = [] if self.overlap else None
         return self.graph
 
     def __exit__(self, exc_type, exc, tb):
         _state['capturing'] = False
-        h = C.c_uint64()
-        rc = _lib._lib.op2b_graph_end(0, C.byref(h))
-        if exc_type is None:
-            _lib.check(rc, "op2b_graph_end")
-            self.graph.handle = h.value
+        trace, _state['trace'] = _state['trace'], None
+        if trace is None:
+            h = C.c_uint64()
+            rc = _lib._lib.op2b_graph_end(0, C.byref(h))
+            if exc_type is None:
+                _lib.check(rc, "op2b_graph_end")
+                self.graph.handle = h.value
+            return False
+        g = C.c_uint64()
+        rc = _lib._lib.op2b_graph_end_capture(0, C.byref(g))
+        if exc_type is not None:
+            if rc == 0:
+                _lib._lib.op2b_graph_free(g.value)
+            return False
+        _lib.check(rc, "op2b_graph_end_capture")
+        try:
+            # segments (par_loop or barrier) and the earlier segments each follows
+            self.graph.handle, self.graph.segments = _relaxed_exec(g.value, trace)
+        finally:
+            call("op2b_graph_free", g.value)
         return False
 
 

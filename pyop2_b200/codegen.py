@@ -794,8 +794,23 @@ def _staged_flush_regs(R, bs, ind, KR):
     return L
 
 
-def _staged_element(spec, R, ind):
-    """(decl, pre, post, exprs, adds) of one element of a staged stub."""
+def _staged_element(spec, R, ind, sfx=""):
+    """(decl, pre, post, exprs, adds) of one element of a staged stub; with
+    ``sfx`` its row variables (a<n>, a<n>_v, sl<stage>) and element id (e)
+    carry that suffix, so several elements' code can share one scope."""
+    parts = _staged_element_parts(spec, R, ind, "e" + sfx)
+    if not sfx:
+        return parts
+    pat = re.compile(r"\b(a\d+|sl\d+)(_v)?\b")
+
+    def ren(t):
+        return pat.sub(lambda m: m.group(1) + sfx + (m.group(2) or ""), t)
+    decl, pre, post, exprs, adds = parts
+    return ([ren(t) for t in decl], [ren(t) for t in pre], [ren(t) for t in post],
+            [ren(t) for t in exprs], [(ren(v), ren(r), q, c) for v, r, q, c in adds])
+
+
+def _staged_element_parts(spec, R, ind, evar):
     read_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["read_pairs"])}
     inc_of = {(sl, st): q for q, (sl, st, _, _) in enumerate(R["inc_pairs"])}
     decl, pre, post, exprs, adds = [], [], [], [], []
@@ -805,7 +820,7 @@ def _staged_element(spec, R, ind):
             exprs.append("g%d_l" % n if a.access == "READ" else "r%d" % n)
             continue
         if a.kind == "direct":
-            exprs.append(_direct_row(a, n, "e", pre, post, ind + "  "))
+            exprs.append(_direct_row(a, n, evar, pre, post, ind + "  "))
             continue
         st = R["map_stage"][a.mslot]
         cnt = a.arity if a.kind == "vec" else a.ext
@@ -861,9 +876,63 @@ def _staged_element(spec, R, ind):
     return decl, pre, post, exprs, adds
 
 
+def _staged_pair_passes(spec, R, used, bs, ind):
+    """Passes of two elements per thread (element j * bs + threadIdx.x of
+    passes j = 2m and 2m + 1): both elements' rows loaded and kernels
+    evaluated before one run of colour rounds over the colours the two
+    groups span (elements of one colour share no target, whichever thread
+    adds them), so the two kernel bodies are independent work for the
+    scheduler and the rounds and barriers are shared."""
+    has_direct = any(a.kind == "direct" for a in spec.args)
+    inner = ind + "  "
+    L = []
+    ept = R["ept"]
+    for j0 in range(0, ept, 2):
+        js = [j for j in (j0, j0 + 1) if j < ept]
+        L.append("%sif (%d < nelem) {" % (ind, j0 * bs))
+        elems = []
+        for j in js:
+            sfx = "_e%d" % j
+            decl, pre, post, exprs, adds = _staged_element(spec, R, ind + "  ", sfx)
+            elems.append((j, sfx, pre, post, exprs, adds))
+            L.append("%sconst bool active%s = active_%d;" % (inner, sfx, j))
+            if has_direct:
+                L.append("%sconst op2b_i64 e%s = e_%d;" % (inner, sfx, j))
+            for st in used:
+                ar = R["stage_arity"][st]
+                L.append("%sconst int sl%d%s[%d] = {%s};" % (inner, st, sfx, ar, ", ".join(
+                    "sl%d_%d[%d]" % (st, j, r) for r in range(ar))))
+            L += decl
+        for j, sfx, pre, post, exprs, adds in elems:
+            L.append("%sif (active%s) {" % (inner, sfx))
+            L += pre
+            L += _itspace_open(spec, inner + "  ")
+            L.append(_kernel_call(spec, exprs, inner + "  " + "  " * len(spec.extents)))
+            L += _itspace_close(spec, inner + "  ")
+            L += post
+            L.append("%s}" % inner)
+        hi = "chi_%d" % js[0] if len(js) == 1 else "max(chi_%d, chi_%d)" % tuple(js)
+        L.append("%sfor (int c = clo_%d; c <= %s; ++c) {" % (inner, js[0], hi))
+        for j, sfx, pre, post, exprs, adds in elems:
+            L.append("%s  if (col_%d == c) {" % (inner, j))
+            for var, lrow, q, c in adds:
+                t = R["inc_pairs"][q][2]
+                L.append("%s    { const int r = %s;" % (inner, lrow))
+                L.append("%s      __align__(16) %s cur[%d]; op2b_srow_load(cur, acc%d, r);" % (inner, t, c, q))
+                L.append("%s      for (int k = 0; k < %d; ++k) cur[k] += %s[k];" % (inner, c, var))
+                L.append("%s      op2b_srow_store(acc%d, r, cur); }" % (inner, q))
+            L.append("%s  }" % inner)
+        L.append("%s  __syncthreads();" % inner)
+        L.append("%s}" % inner)
+        L.append("%s}" % ind)
+    return L
+
+
 def _staged_passes(spec, R, used, bs, ind):
     """The ept passes over the block's elements: compute, then add the INC
     rows into the shared accumulators colour by colour."""
+    if R.get("pair", 1) == 2:
+        return _staged_pair_passes(spec, R, used, bs, ind)
     decl, pre, post, exprs, adds = _staged_element(spec, R, ind + "  ")
     has_direct = any(a.kind == "direct" for a in spec.args)
     inner = ind + "  "

@@ -44,6 +44,9 @@ keys of the B200 backend:
 * ``staged_tl_regs``: the staged stubs load their block's target ids into
   registers once (with the element rows) and reuse them for the row copies
   and the flush, which then adds one accumulated row per thread;
+* ``staged_pair``: 2 makes each thread of a staged stub evaluate two
+  elements (of two consecutive passes) before one shared run of colour
+  rounds; 1 (default) one element per pass;
 * ``direct_unroll``: elements each thread of a direct stub takes per round
   (their rows all loaded before the kernel calls, so the loads overlap);
 * ``staged_min_size``: iteration sets smaller than this run the atomic form
@@ -93,6 +96,10 @@ keys of the B200 backend:
   from a compact slot table (one 64-bit word of in-row positions per element
   and local row, added to the row start read through the Map) instead of one
   32-bit position per local entry;
+* ``graph_overlap``: a CUDA graph recorded with ``b200.capture`` lets
+  par_loops that touch no common data in a conflicting way run side by side
+  (reads of one object, atomic increments of one object); other device work
+  recorded in the graph stays in program order with everything around it;
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;
 * ``pool_reserve_gb``: device memory (GB, at most a quarter of the device)
@@ -133,6 +140,8 @@ _defaults = {
     'staged_tl_regs': False,
     'direct_unroll': 1,
     'mat_slots_rel': False,
+    'graph_overlap': False,
+    'staged_pair': 1,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

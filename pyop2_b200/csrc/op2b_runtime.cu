@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "op2b_internal.h"
@@ -94,6 +95,34 @@ __global__ void map_validate_kernel(const int32_t *__restrict__ map, int64_t n, 
     int32_t v = map[i];
     if (v < 0 || v >= to_size) atomicMin(bad, (unsigned long long)i);
   }
+}
+
+// The graph's nodes in chain order; fails unless every node has at most one
+// dependency and one dependent and there is one root.
+int graph_chain(cudaGraph_t g, std::vector<cudaGraphNode_t> &chain) {
+  size_t n = 0;
+  OP2B_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+  chain.clear();
+  if (!n) return OP2B_OK;
+  size_t nr = 0;
+  OP2B_CUDA(cudaGraphGetRootNodes(g, nullptr, &nr));
+  if (nr != 1) return set_error(OP2B_ERR_STATE, "graph: %zu roots, not a chain", nr);
+  cudaGraphNode_t cur = nullptr;
+  OP2B_CUDA(cudaGraphGetRootNodes(g, &cur, &nr));
+  chain.reserve(n);
+  while (cur) {
+    chain.push_back(cur);
+    if (chain.size() > n) return set_error(OP2B_ERR_STATE, "graph: cycle");
+    size_t nd = 0;
+    OP2B_CUDA(cudaGraphNodeGetDependentNodes(cur, nullptr, &nd));
+    if (nd > 1) return set_error(OP2B_ERR_STATE, "graph: node with %zu dependents", nd);
+    cudaGraphNode_t next = nullptr;
+    if (nd) OP2B_CUDA(cudaGraphNodeGetDependentNodes(cur, &next, &nd));
+    cur = nd ? next : nullptr;
+  }
+  if (chain.size() != n) return set_error(OP2B_ERR_STATE, "graph: %zu of %zu nodes on the chain",
+                                          chain.size(), n);
+  return OP2B_OK;
 }
 
 }  // namespace op2b
@@ -401,6 +430,110 @@ int op2b_graph_end(uint64_t stream, uint64_t *graph_exec) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
   *graph_exec = reinterpret_cast<uint64_t>(ge);
+  return OP2B_OK;
+}
+
+// ---- overlapped capture: a capture on one stream records a linear chain of
+// nodes; the host marks the chain's tail around each par_loop, computes which
+// loops must follow which from their accesses, and the chain edges between
+// independent loops are replaced by those dependencies before instantiation.
+int op2b_graph_capture_tail(uint64_t stream, uint64_t *node) {
+  OP2B_REQUIRE_INIT();
+  if (!node) return set_error(OP2B_ERR_ARG, "op2b_graph_capture_tail: null");
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  OP2B_CUDA(cudaStreamGetCaptureInfo(stream_of(stream), &st, nullptr, nullptr, &deps, &nd));
+  if (st != cudaStreamCaptureStatusActive)
+    return set_error(OP2B_ERR_STATE, "op2b_graph_capture_tail: the stream is not capturing");
+  if (nd > 1)
+    return set_error(OP2B_ERR_STATE, "op2b_graph_capture_tail: the capture has %zu tails", nd);
+  *node = nd ? reinterpret_cast<uint64_t>(deps[0]) : 0;
+  return OP2B_OK;
+}
+
+int op2b_graph_end_capture(uint64_t stream, uint64_t *graph) {
+  OP2B_REQUIRE_INIT();
+  if (!graph) return set_error(OP2B_ERR_ARG, "op2b_graph_end_capture: null");
+  cudaGraph_t g = nullptr;
+  OP2B_CUDA(cudaStreamEndCapture(stream_of(stream), &g));
+  *graph = reinterpret_cast<uint64_t>(g);
+  return OP2B_OK;
+}
+
+
+int op2b_graph_chain_positions(uint64_t graph, const uint64_t *marks, int32_t nmarks,
+                               int64_t *pos, int64_t *nnodes) {
+  OP2B_REQUIRE_INIT();
+  if (!graph || nmarks < 0 || (nmarks && (!marks || !pos)) || !nnodes)
+    return set_error(OP2B_ERR_ARG, "op2b_graph_chain_positions: bad arguments");
+  std::vector<cudaGraphNode_t> chain;
+  int rc = graph_chain(reinterpret_cast<cudaGraph_t>(graph), chain);
+  if (rc) return rc;
+  *nnodes = (int64_t)chain.size();
+  std::unordered_map<uint64_t, int64_t> at;
+  for (size_t k = 0; k < chain.size(); ++k) at[reinterpret_cast<uint64_t>(chain[k])] = (int64_t)k;
+  for (int32_t m = 0; m < nmarks; ++m) {
+    if (!marks[m]) {
+      pos[m] = -1;
+      continue;
+    }
+    auto it = at.find(marks[m]);
+    if (it == at.end()) return set_error(OP2B_ERR_STATE, "graph: mark %d is not a node", m);
+    pos[m] = it->second;
+  }
+  return OP2B_OK;
+}
+
+int op2b_graph_relax(uint64_t graph, const int64_t *seg_first, const int64_t *seg_last,
+                     int32_t nseg, const int32_t *dep_ptr, const int32_t *dep_idx,
+                     uint64_t *graph_exec) {
+  OP2B_REQUIRE_INIT();
+  if (!graph || !graph_exec || nseg < 0 || (nseg && (!seg_first || !seg_last || !dep_ptr)))
+    return set_error(OP2B_ERR_ARG, "op2b_graph_relax: bad arguments");
+  cudaGraph_t g = reinterpret_cast<cudaGraph_t>(graph);
+  if (nseg) {
+    std::vector<cudaGraphNode_t> chain;
+    int rc = graph_chain(g, chain);
+    if (rc) return rc;
+    const int64_t n = (int64_t)chain.size();
+    // the segments tile the chain in order
+    int64_t expect = 0;
+    for (int32_t s = 0; s < nseg; ++s) {
+      if (seg_first[s] != expect || seg_last[s] < seg_first[s] || seg_last[s] >= n)
+        return set_error(OP2B_ERR_ARG, "op2b_graph_relax: segment %d [%lld, %lld] does not tile "
+                         "the chain of %lld nodes", s, (long long)seg_first[s],
+                         (long long)seg_last[s], (long long)n);
+      expect = seg_last[s] + 1;
+      for (int32_t k = dep_ptr[s]; k < dep_ptr[s + 1]; ++k)
+        if (dep_idx[k] < 0 || dep_idx[k] >= s)
+          return set_error(OP2B_ERR_ARG, "op2b_graph_relax: segment %d depends on %d", s,
+                           dep_idx[k]);
+    }
+    if (expect != n)
+      return set_error(OP2B_ERR_ARG, "op2b_graph_relax: segments cover %lld of %lld nodes",
+                       (long long)expect, (long long)n);
+    std::vector<cudaGraphNode_t> from, to;
+    for (int32_t s = 1; s < nseg; ++s) {
+      cudaGraphNode_t first = chain[seg_first[s]], prev = chain[seg_first[s] - 1];
+      OP2B_CUDA(cudaGraphRemoveDependencies(g, &prev, &first, 1));
+      for (int32_t k = dep_ptr[s]; k < dep_ptr[s + 1]; ++k) {
+        from.push_back(chain[seg_last[dep_idx[k]]]);
+        to.push_back(first);
+      }
+    }
+    if (!from.empty()) OP2B_CUDA(cudaGraphAddDependencies(g, from.data(), to.data(), from.size()));
+  }
+  cudaGraphExec_t ge = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+  if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
+  *graph_exec = reinterpret_cast<uint64_t>(ge);
+  return OP2B_OK;
+}
+
+int op2b_graph_free(uint64_t graph) {
+  OP2B_REQUIRE_INIT();
+  if (graph) OP2B_CUDA(cudaGraphDestroy(reinterpret_cast<cudaGraph_t>(graph)));
   return OP2B_OK;
 }
 

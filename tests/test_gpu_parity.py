@@ -442,12 +442,14 @@ def test_two_phase_kahan_precision_form(op2):
 
 @pytest.mark.parametrize("opts", [dict(programmatic_launch=True), dict(fmad_inc=True),
                                   dict(staged_tl_regs=True), dict(read_replicas=True,
-                                                                  replica_min_size=0)])
+                                                                  replica_min_size=0),
+                                  dict(staged_pair=2), dict(staged_pair=2, partition_size=512)])
 def test_airfoil_chain_launch_options_match_oracle(op2, opts):
     """The launch-level options on the staged airfoil chain: programmatic
     dependent launch (every stub waits for its predecessor), multiply-add
     contraction in INC-form loops, target ids in registers, READ replicas on
-    small sets; q and rms within 1e-12 of the oracle after three
+    small sets, two elements per thread in the staged passes (odd and even
+    pass counts); q and rms within 1e-12 of the oracle after three
     iterations."""
     from pyop2_b200 import b200
     from pyop2_b200 import configuration as cfg
