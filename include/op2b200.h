@@ -302,6 +302,18 @@ int op2b_map_renumber(uint64_t dst_map, uint64_t map, int64_t n_entries, uint64_
                       int32_t ntargets, uint64_t stream);
 
 /* ------------------------------------------------------------------------
+ * Halo rows of partitioned sets.  Replaces the host-side packing of
+ * Dat.halo_exchange_begin / _end (pyop2/base.py:797-835:
+ * send_buf = data[sends[dest]]; data[receives[source]] = recv_buf).
+ * op2b_halo_pack: buf[i] = rows[index[i]]; op2b_halo_unpack:
+ * rows[index[i]] = buf[i]; n rows of row_bytes bytes each, index int32.
+ * ---------------------------------------------------------------------- */
+int op2b_halo_pack(uint64_t buf, uint64_t rows, uint64_t index, int64_t n, int32_t row_bytes,
+                   uint64_t stream);
+int op2b_halo_unpack(uint64_t rows, uint64_t buf, uint64_t index, int64_t n, int32_t row_bytes,
+                     uint64_t stream);
+
+/* ------------------------------------------------------------------------
  * Two-phase deterministic INC.  A generated stub writes every element's INC
  * contribution to a tiled contribution array: element e, position k (of K)
  * at row ((e / 32) * K + k) * 32 + e % 32, cdim values per row (k: map

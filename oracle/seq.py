@@ -492,10 +492,13 @@ def _marshal(args):
     return (C.c_void_p * max(len(ptrs), 1))(*ptrs), keep
 
 
-def par_loop(kernel, itspace, *args, openmp=False, part_size=1024, timer=None):
+def par_loop(kernel, itspace, *args, openmp=False, part_size=1024, timer=None, span=None):
     """Run the loop with sequential (or restated OpenMP) semantics.
     ``timer``, if given, is called with the wall seconds of the element loop
-    alone (code generation, compilation and planning excluded)."""
+    alone (code generation, compilation and planning excluded).  ``span`` =
+    (start, end) runs elements [start, end) only, as the sequential backend's
+    wrapper does for the core / owned / execute-halo ranges of a
+    partitioned set (sequential.py:96-117; sequential only)."""
     import time
     if isinstance(itspace, Set):
         itspace = IterationSpace(itspace, ())
@@ -506,9 +509,12 @@ def par_loop(kernel, itspace, *args, openmp=False, part_size=1024, timer=None):
     cvals = [np.ascontiguousarray(c.data) for c in consts]
     cptr = (C.c_void_p * max(len(cvals), 1))(*[c.ctypes.data for c in cvals])
     n = itspace.iterset.size
+    start, end = (0, n) if span is None else (int(span[0]), int(span[1]))
+    if not 0 <= start <= end <= n or (openmp and span is not None):
+        raise ValueError("span %s of a set of %d elements" % (span, n))
     if not openmp:
         t0 = time.perf_counter()
-        err = lib.wrap(0, n, cargs, cptr)
+        err = lib.wrap(start, end, cargs, cptr)
         dt = time.perf_counter() - t0
     else:
         from .plan import plan as make_plan

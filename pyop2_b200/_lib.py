@@ -58,6 +58,8 @@ _SIGS = {
     "op2b_graph_chain_positions": [u64, u64p, i32, i64p, i64p],
     "op2b_graph_relax": [u64, i64p, i64p, i32, i32p, i32p, u64p],
     "op2b_graph_free": [u64],
+    "op2b_halo_pack": [u64, u64, u64, i64, i32, u64],
+    "op2b_halo_unpack": [u64, u64, u64, i64, i32, u64],
     "op2b_nvrtc_compile": [charp, charp, C.POINTER(charp), i32, C.POINTER(P), u64p, charp, u64],
     "op2b_cubin_free": [P],
     "op2b_module_load": [P, u64p],

@@ -26,6 +26,7 @@ import weakref
 import numpy as np
 
 from . import base, codegen, overlap
+from . import halo as halo_mod
 from . import configuration as cfg
 from . import _lib
 from ._lib import call
@@ -1491,8 +1492,8 @@ class _BoundLoop(object):
     """Everything about a par_loop that does not change between calls with
     the same objects: generated stub, plan, parameter block."""
 
-    def __init__(self, loop, inc_mode=None):
-        info = loop_spec(loop, inc_mode=inc_mode)
+    def __init__(self, loop, inc_mode=None, owner_mode=None):
+        info = loop_spec(loop, inc_mode=inc_mode, owner_mode=owner_mode)
         spec = info['spec']
         specs = info['specs']
         dats, maps, mats, gbls = info['dats'], info['maps'], info['mats'], info['gbls']
@@ -1510,6 +1511,7 @@ class _BoundLoop(object):
         self.layout = self.module.layout
         self.indirect = indirect
         self.iterset = iterset
+        self.partitioned = _partitioned(iterset)
         self.dats, self.maps, self.mats = dats, maps, mats
         self.gbl_specs = [s for s in specs if s.kind == "gbl"]
         self.dat_access = {}
@@ -1712,20 +1714,23 @@ class _BoundLoop(object):
         self._buf = C.create_string_buffer(self.layout.pack(n, 0, self.range_end, vals),
                                            self.layout.nbytes)
 
-    def run(self, loop):
+    def run(self, loop, rng=None):
+        """Run the loop over its whole set, or over elements [start, end)
+        with ``rng`` (the direct and atomic forms, whose stubs walk the
+        parameter block's element range)."""
         trace = _state['trace']
         if trace is None:
-            self._run(loop)
+            self._run(loop, rng)
             return
         # overlapped capture: the chain's tail before and after this loop's
         # nodes, and what the loop reads and writes
         pre = _capture_tail()
-        self._run(loop)
+        self._run(loop, rng)
         args = loop.args
         gbl = tuple((id(args[ai].data), "W" if red else "R") for _, ai, red in self._gbl)
         trace.append((pre, _capture_tail(), self.accesses + gbl))
 
-    def _run(self, loop):
+    def _run(self, loop, rng=None):
         if getattr(self, "_buf", None) is None:
             self._prepare(loop)
         for d in self.dats:
@@ -1749,6 +1754,11 @@ class _BoundLoop(object):
         if self.consts:
             _sync_consts(mod, self.consts)
         n = self.iterset.size
+        if rng is not None:
+            if self.spec.mode not in ("direct", "atomic") or rng[0] < 0 or rng[1] > \
+                    self.iterset.total_size:
+                raise DeviceError("element range %s of a %s-form loop" % (rng, self.spec.mode))
+            n = rng[1] - rng[0]
         if n == 0:
             return
         params = buf
@@ -1756,6 +1766,15 @@ class _BoundLoop(object):
             plan = self.plan
             call("op2b_launch_colored", mod.fn, plan.ncolors, plan.ncolblk_host, self.block_size,
                  self.smem, 0, params, self.layout.nbytes, codegen.ParamLayout.COL_OFFSET)
+        elif rng is not None:
+            # the header's (start, end) for this launch only: the launch
+            # copies the parameter block when it is issued
+            struct.pack_into("<qq", buf, 16, rng[0], rng[1])
+            try:
+                call("op2b_launch", mod.fn, self.grid, self.block_size, self.launch_smem, 0,
+                     params, self.layout.nbytes)
+            finally:
+                struct.pack_into("<qq", buf, 16, 0, self.range_end)
         else:
             call("op2b_launch", mod.fn, self.grid, self.block_size, self.launch_smem, 0, params,
                  self.layout.nbytes)
@@ -1835,6 +1854,195 @@ class _Args(object):
         self.args = args
 
 
+# ------------------------------------------------ partitioned sets (halos)
+class _DeviceHaloBuffer(object):
+    """A device buffer in the protocol of :mod:`pyop2_b200.halo` (copy,
+    assign, host round trips, torch tensor view).  ``owner`` keeps the
+    memory alive; a view of a Global's value passes the Global."""
+
+    def __init__(self, ptr, nbytes, dtype, shape, owner=None):
+        self.ptr, self.nbytes, self.dtype, self.shape = ptr, int(nbytes), np.dtype(dtype), shape
+        self.owner = owner
+
+    @classmethod
+    def alloc(cls, nbytes, dtype, shape):
+        buf = DeviceBuffer(max(int(nbytes), 16))
+        return cls(buf.ptr, nbytes, dtype, shape, buf)
+
+    def copy(self):
+        out = _DeviceHaloBuffer.alloc(self.nbytes, self.dtype, self.shape)
+        out.assign(self)
+        return out
+
+    def assign(self, other):
+        if other.nbytes != self.nbytes:
+            raise DeviceError("halo buffer of %d bytes assigned %d" % (self.nbytes, other.nbytes))
+        if self.nbytes:
+            call("op2b_memcpy_d2d", self.ptr, other.ptr, self.nbytes, 0)
+
+    def to_host(self):
+        out = np.empty(self.shape, self.dtype)
+        if self.nbytes:
+            call("op2b_memcpy_d2h", out.ctypes.data, self.ptr, self.nbytes, 0)
+        return out
+
+    def from_host(self, a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=self.dtype).reshape(self.shape))
+        if self.nbytes:
+            call("op2b_memcpy_h2d", self.ptr, a.ctypes.data, self.nbytes, 0)
+
+    def tensor(self):
+        """A torch CUDA tensor over the same memory (no copy)."""
+        import torch
+        n = self.nbytes // self.dtype.itemsize
+
+        class _View(object):
+            __cuda_array_interface__ = {"shape": (n,), "typestr": self.dtype.str,
+                                        "data": (self.ptr, False), "version": 3,
+                                        "strides": None, "stream": None}
+        return torch.as_tensor(_View(), device="cuda")
+
+
+class _DatRows(object):
+    """Row store of a Dat on the device for halo exchanges: rows packed with
+    op2b_halo_pack and unpacked with op2b_halo_unpack (an SoA Dat one
+    component at a time, its buffers component-major)."""
+
+    def __init__(self, dat):
+        dat._to_device()
+        self.dat = dat
+        self.elem = np.dtype(dat.dtype).itemsize
+        self.cdim = dat.cdim
+
+    def _index(self, idx):
+        # device copies of the Set's halo index lists, made once
+        cache = self.dat.dataset.__dict__.setdefault("_halo_device_index", {})
+        ent = cache.get(id(idx))
+        if ent is None or ent[0] is not idx:
+            a = np.ascontiguousarray(idx, dtype=np.int32)
+            buf = DeviceBuffer(max(a.nbytes, 16))
+            if a.nbytes:
+                call("op2b_memcpy_h2d", buf.ptr, a.ctypes.data, a.nbytes, 0)
+            ent = cache[id(idx)] = (idx, buf)
+        return ent[1].ptr
+
+    def _rows(self, n):
+        return (n, self.cdim) if self.cdim > 1 else (n,)
+
+    def new_buffer(self, n):
+        return _DeviceHaloBuffer.alloc(n * self.cdim * self.elem, self.dat.dtype, self._rows(n))
+
+    def _move(self, name, idx, buf):
+        n = len(idx)
+        d = self.dat
+        if not n:
+            return
+        ix = self._index(idx)
+        if d.soa:
+            total = d.dataset.total_size
+            for k in range(self.cdim):
+                rows = d._device.ptr + k * total * self.elem
+                part = buf.ptr + k * n * self.elem
+                if name == "op2b_halo_pack":
+                    call(name, part, rows, ix, n, self.elem, 0)
+                else:
+                    call(name, rows, part, ix, n, self.elem, 0)
+        elif name == "op2b_halo_pack":
+            call(name, buf.ptr, d._device.ptr, ix, n, self.cdim * self.elem, 0)
+        else:
+            call(name, d._device.ptr, buf.ptr, ix, n, self.cdim * self.elem, 0)
+
+    def pack(self, idx):
+        buf = self.new_buffer(len(idx))
+        self._move("op2b_halo_pack", idx, buf)
+        return buf
+
+    def unpack(self, idx, buf):
+        self._move("op2b_halo_unpack", idx, buf)
+        d = self.dat
+        d._state = DEVICE
+        d._wgen += 1
+
+
+def _global_value(g):
+    """A Global's device value as a halo-protocol buffer."""
+    g._to_device()
+    return _DeviceHaloBuffer(g._device.ptr, g._data.nbytes, g.dtype, g._data.shape, g)
+
+
+def _partitioned(iterset):
+    """The set has halo elements (sizes core < owned < exec < total, as the
+    reference runs over distributed meshes)."""
+    return not (iterset.core_size == iterset.size == iterset.exec_size == iterset.total_size)
+
+
+def _set_comm(iterset):
+    h = iterset.halo
+    return h.comm if h is not None else MPI.comm
+
+
+_RED_OPS = {"INC": "sum", "MIN": "min", "MAX": "max"}
+
+
+def _loop_phases(bl, loop, args):
+    """One par_loop over a partitioned set in the reference's order
+    (pyop2/sequential.py:96-117): halo exchanges of the stale Dats an
+    indirect loop reads, core elements, the exchanges' completion, the other
+    owned elements, the Global all-reduces, the execute halo for loops that
+    write through a Map.  A generator that yields where the rank waits for
+    its peers (:func:`pyop2_b200.halo.run_lockstep` drives in-process ranks)."""
+    it = bl.iterset
+    direct = all(a._map is None or a._map is IdentityMap for a in args)
+    exchanges = []
+    if not direct:
+        # pyop2/base.py:197-206 and 1492-1499: every Dat arg read by an
+        # indirect loop, once per Dat (the first arg clears the flag)
+        for a in args:
+            d = a._dat
+            if (isinstance(d, base.Dat) and a._access in (READ, RW) and d.needs_halo_update
+                    and d.dataset.halo is not None):
+                d.needs_halo_update = False
+                exchanges.append(halo_mod.DatExchange(_DatRows(d), d.dataset.halo,
+                                                      d.dataset.halo.comm))
+    comm = _set_comm(it)
+    reductions, seen = [], set()
+    for a in args:
+        g = a._dat
+        if isinstance(g, base.Global) and a._access in (INC, MIN, MAX) and id(g) not in seen:
+            seen.add(id(g))
+            reductions.append(halo_mod.GlobalReduction(_global_value(g), comm,
+                                                       _RED_OPS[a._access._mode]))
+    exec_halo = any(a._is_indirect_and_not_read or a._is_mat for a in args)
+
+    def launch(start, end):
+        if end > start:
+            bl.run(loop, (start, end))
+    yield from halo_mod.loop_phases(it.sizes, launch, exchanges, reductions, direct, exec_halo)
+    for a in args:
+        if a._access is not READ and isinstance(a._dat, base.Dat):
+            a._dat.needs_halo_update = True
+
+
+def _bind(loop, iterset):
+    """A new bound loop; loops over partitioned sets run element ranges, so
+    they take the one-launch atomic form (no partition, plan or owner
+    ordering over the whole set)."""
+    if _partitioned(iterset):
+        if any(isinstance(a._dat, base.Mat) for a in loop.args):
+            raise NotImplementedError("Mat assembly over a partitioned set needs a distributed "
+                                      "matrix; the B200 backend assembles Mats on one rank")
+        bl = _BoundLoop(loop, inc_mode='atomic', owner_mode='never')
+        if bl.spec.mode not in ("direct", "atomic"):
+            raise NotImplementedError("par_loop %s over a partitioned set needs the %s form, "
+                                      "which runs whole sets only" % (bl.spec.kernel_name,
+                                                                      bl.spec.mode))
+        return bl
+    try:
+        return _BoundLoop(loop)
+    except _StagedTooLarge:
+        return _BoundLoop(loop, inc_mode='atomic')
+
+
 class ParLoop(base.ParLoop):
 
     _bound_cache = {}
@@ -1842,15 +2050,29 @@ class ParLoop(base.ParLoop):
     def _bound_key(self):
         return _loop_key(self.kernel, self.it_space.iterset, self.it_space.extents, self.args)
 
-    def compute(self):
+    def _bound(self):
         key = self._bound_key()
         bl = ParLoop._bound_cache.get(key)
         if bl is None or not bl.matches(self):
-            try:
-                bl = _BoundLoop(self)
-            except _StagedTooLarge:
-                bl = _BoundLoop(self, inc_mode='atomic')
+            bl = _bind(self, self.it_space.iterset)
             ParLoop._bound_cache[key] = bl
+        return bl
+
+    def compute(self):
+        bl = self._bound()
+        if _partitioned(bl.iterset):
+            halo_mod.run(_loop_phases(bl, self, self.args))
+            return
+        bl.run(self)
+        self.maybe_set_halo_update_needed()
+
+    def phases(self):
+        """The loop as a generator of phases (see :func:`_loop_phases`); a
+        set without halo elements runs in one phase."""
+        bl = self._bound()
+        if _partitioned(bl.iterset):
+            yield from _loop_phases(bl, self, self.args)
+            return
         bl.run(self)
         self.maybe_set_halo_update_needed()
 
@@ -1873,6 +2095,9 @@ def par_loop(kernel, it_space, *args):
         key = None   # not well-formed: the full path raises the reference's error
     bl = ParLoop._bound_cache.get(key) if key is not None else None
     if bl is not None and bl.matches(None):
+        if bl.partitioned:
+            halo_mod.run(_loop_phases(bl, _Args(args), args))
+            return
         bl.run(_Args(args))
         for a in args:
             if a._access is not READ and isinstance(a._dat, base.Dat):
@@ -1881,14 +2106,25 @@ def par_loop(kernel, it_space, *args):
     ParLoop(kernel, it_space, *args).compute()
 
 
-class _SingleRank(object):
-    rank = 0
-    size = 1
+def par_loop_phases(kernel, it_space, *args):
+    """:func:`par_loop` as a generator that yields where a rank of a
+    partitioned run waits for its peers, so that several ranks held by one
+    process (:class:`pyop2_b200.halo.LocalComm`) can be stepped together with
+    :func:`pyop2_b200.halo.run_lockstep`."""
+    return ParLoop(kernel, it_space, *args).phases()
 
 
 class _MPIConfig(object):
-    comm = _SingleRank()
-    parallel = False
+    """The communicator of partitioned runs (pyop2/mpi.py:46-73): a
+    :mod:`pyop2_b200.halo` communicator, set by ``op2.init(comm=...)``;
+    one rank alone by default."""
+
+    def __init__(self):
+        self.comm = halo_mod.SelfComm()
+
+    @property
+    def parallel(self):
+        return self.comm.size > 1
 
 
 MPI = _MPIConfig()

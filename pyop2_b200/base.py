@@ -18,7 +18,7 @@ from hashlib import md5
 import numpy as np
 
 from . import configuration as cfg
-from .backends import _make_object
+from .backends import _BackendSelector, _make_object
 from .caching import Cached
 from .exceptions import (DataTypeError, DataValueError, DimTypeError, IndexTypeError,
                          IndexValueError, MapTypeError, MapValueError, ModeValueError,
@@ -256,18 +256,30 @@ class Set(object):
 
 
 class Halo(object):
-    """Halo description (pyop2/base.py:402-505).  Only the single-process form
-    (no sends, no receives) is meaningful on one GPU; it is kept for API
-    compatibility and verified like the reference's."""
+    """Halo description (pyop2/base.py:402-505): per peer rank, the owned
+    elements sent to it and the halo elements received from it.  ``comm`` is
+    any communicator of :mod:`pyop2_b200.halo` (a ``torch.distributed`` group,
+    in-process ranks) and defaults to the backend's ``MPI.comm``."""
 
     def __init__(self, sends, receives, comm=None, gnn2unn=None):
         self._sends = tuple(np.asarray(x, dtype=np.int32) for x in sends)
         self._receives = tuple(np.asarray(x, dtype=np.int32) for x in receives)
         self._global_to_petsc_numbering = gnn2unn
-        assert len(self._sends) == 1 and len(self._receives) == 1, \
-            "Only single-process halos are supported by the B200 backend"
-        assert self._sends[0].size == 0, "Halo was specified with self-sends on rank 0"
-        assert self._receives[0].size == 0, "Halo was specified with self-receives on rank 0"
+        if comm is None:
+            comm = _default_comm()
+        self._comm = comm
+        rank, size = comm.rank, comm.size
+        assert len(self._sends) == size, \
+            "Invalid number of sends for Halo, got %d, wanted %d" % (len(self._sends), size)
+        assert len(self._receives) == size, \
+            "Invalid number of receives for Halo, got %d, wanted %d" % (len(self._receives), size)
+        assert self._sends[rank].size == 0, "Halo was specified with self-sends on rank %d" % rank
+        assert self._receives[rank].size == 0, \
+            "Halo was specified with self-receives on rank %d" % rank
+
+    @property
+    def comm(self):
+        return self._comm
 
     @property
     def sends(self):
@@ -288,6 +300,16 @@ class Halo(object):
         for source, receives in enumerate(self.receives):
             assert (receives >= s.size).all() and (receives < s.total_size).all(), \
                 "Halo receive from %d is invalid (not in halo elements)" % source
+
+
+def _default_comm():
+    """The selected backend's communicator, else a single rank."""
+    mpi = getattr(_BackendSelector._backend, "MPI", None)
+    comm = getattr(mpi, "comm", None)
+    if comm is None:
+        from .halo import SelfComm
+        comm = SelfComm()
+    return comm
 
 
 class IterationSpace(object):

@@ -22,6 +22,7 @@ def init(**kwargs):
     Calling ``init`` again with another backend, or after ``exit``, raises
     RuntimeError; calling it again with the same backend updates the
     configuration."""
+    comm = kwargs.pop('comm', None)
     backend = backends.get_backend()
     if backend == 'pyop2_b200.finalised':
         raise RuntimeError("Calling init() after exit() is illegal.")
@@ -40,6 +41,9 @@ def init(**kwargs):
         # the backend may have been selected without a device (host-only
         # use of the data classes); setting up is idempotent
         backends._BackendSelector._backend._setup()
+    if comm is not None:
+        # pyop2/op2.py:78-79: the communicator of partitioned runs
+        backends._BackendSelector._backend.MPI.comm = comm
     global MPI
     MPI = backends._BackendSelector._backend.MPI
 

@@ -232,6 +232,82 @@ def build_from_hdf5(op2, f):
     return A
 
 
+def partition_grid(g, nranks):
+    """Owner-computes partition of the airfoil mesh ``g`` over ``nranks``
+    ranks (:func:`pyop2_b200.partition.partition`): cells in bands of their
+    centroid's x coordinate, each edge and boundary edge with the owner of
+    its first cell, each node with the owner of the lowest-numbered cell
+    that holds it."""
+    from ..partition import partition
+    pcell = np.asarray(g.pcell, np.int64).reshape(-1, 4)
+    pecell = np.asarray(g.pecell, np.int64).reshape(-1, 2)
+    pbecell = np.asarray(g.pbecell, np.int64).reshape(-1, 1)
+    cx = np.asarray(g.x, np.float64).reshape(-1, 2)[pcell, 0].mean(axis=1)
+    cuts = np.quantile(cx, np.arange(1, nranks) / nranks) if nranks > 1 else np.zeros(0)
+    cell_owner = np.searchsorted(cuts, cx, side="right").astype(np.int64)
+    first = np.full(g.nnodes, g.ncells, np.int64)
+    np.minimum.at(first, pcell.ravel(), np.repeat(np.arange(g.ncells), 4))
+    node_owner = cell_owner[np.minimum(first, g.ncells - 1)]
+    sets = {"nodes": g.nnodes, "edges": g.nedges, "bedges": g.nbedges, "cells": g.ncells}
+    maps = {"pedge": ("edges", "nodes", g.pedge), "pecell": ("edges", "cells", pecell),
+            "pbedge": ("bedges", "nodes", g.pbedge), "pbecell": ("bedges", "cells", pbecell),
+            "pcell": ("cells", "nodes", pcell)}
+    owner = {"cells": cell_owner, "nodes": node_owner, "edges": cell_owner[pecell[:, 0]],
+             "bedges": cell_owner[pbecell[:, 0]]}
+    return partition(sets, maps, owner, nranks)
+
+
+def build_partitioned(op2, g, local, comm, seed=0, q0=None, consts=True):
+    """Declare one rank's part of the airfoil problem (``local``: that
+    rank's :class:`pyop2_b200.partition.LocalMesh` of :func:`partition_grid`)
+    with Sets of four sizes and Halos over ``comm``, as a distributed run of
+    the demo declares them; Dats hold the rank's rows of the global initial
+    state, halo rows included."""
+    A = Airfoil()
+    A.grid, A.local = g, local
+    S = local.sets
+
+    def mkset(name, dim):
+        ls = S[name]
+        return op2.Set(list(ls.sizes), dim, name,
+                       halo=op2.Halo(ls.sends, ls.receives, comm=comm))
+    A.nodes = mkset("nodes", 2)
+    A.edges = mkset("edges", 1)
+    A.bedges = mkset("bedges", 1)
+    A.cells = mkset("cells", 1)
+    A.vcells = mkset("cells", 4)
+    lm = local.maps
+    A.pedge = op2.Map(A.edges, A.nodes, 2, lm["pedge"][2], "pedge")
+    A.pecell = op2.Map(A.edges, A.cells, 2, lm["pecell"][2], "pecell")
+    A.pevcell = op2.Map(A.edges, A.vcells, 2, lm["pecell"][2], "pevcell")
+    A.pbedge = op2.Map(A.bedges, A.nodes, 2, lm["pbedge"][2], "pbedge")
+    A.pbecell = op2.Map(A.bedges, A.cells, 1, lm["pbecell"][2], "pbecell")
+    A.pbevcell = op2.Map(A.bedges, A.vcells, 1, lm["pbecell"][2], "pbevcell")
+    A.pcell = op2.Map(A.cells, A.nodes, 4, lm["pcell"][2], "pcell")
+    q = (initial_q(g.ncells, seed) if q0 is None else np.asarray(q0, np.float64)).reshape(-1, 4)
+    cells = S["cells"]
+    A.p_bound = op2.Dat(A.bedges, S["bedges"].local_rows(np.asarray(g.p_bound).reshape(-1, 1)),
+                        np.int32, "p_bound")
+    A.p_x = op2.Dat(A.nodes, S["nodes"].local_rows(np.asarray(g.x).reshape(-1, 2)), np.float64,
+                    "p_x")
+    A.p_q = op2.Dat(A.vcells, cells.local_rows(q), np.float64, "p_q")
+    A.p_qold = op2.Dat(A.vcells, cells.local_rows(q), np.float64, "p_qold")
+    A.p_adt = op2.Dat(A.cells, np.zeros(cells.sizes[3]), np.float64, "p_adt")
+    A.p_res = op2.Dat(A.vcells, np.zeros((cells.sizes[3], 4)), np.float64, "p_res")
+    for d in (A.p_bound, A.p_x, A.p_q, A.p_qold, A.p_adt, A.p_res):
+        d.needs_halo_update = False        # halo rows start as copies of the owners' rows
+    if consts:
+        A.consts = [op2.Const(1, GAM, "gam", np.float64), op2.Const(1, GM1, "gm1", np.float64),
+                    op2.Const(1, CFL, "cfl", np.float64), op2.Const(1, EPS, "eps", np.float64),
+                    op2.Const(4, freestream(), "qinf", np.float64)]
+    A.k_save = op2.Kernel(SAVE_SOLN, "save_soln")
+    A.k_adt = op2.Kernel(ADT_CALC, "adt_calc")
+    A.k_res = op2.Kernel(RES_CALC, "res_calc")
+    A.k_bres = op2.Kernel(BRES_CALC, "bres_calc")
+    A.k_update = op2.Kernel(UPDATE, "update")
+    return A
+
+
 def save_soln(op2, A):
     op2.par_loop(A.k_save, A.cells, A.p_q(op2.IdentityMap, op2.READ),
                  A.p_qold(op2.IdentityMap, op2.WRITE))

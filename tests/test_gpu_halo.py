@@ -1,0 +1,133 @@
+"""Partitioned execution on the device (b200 par_loop over Sets with four
+sizes and Halos; pyop2/sequential.py:96-117, pyop2/base.py:797-835): the
+halo pack / unpack kernels against numpy, element-range launches with the
+reference's Global semantics, and the airfoil problem split over two and
+three ranks held by one process (LocalComm, ranks stepped together; their
+kernels never wait on one another) against the sequential oracle on the
+undivided mesh."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+TOL = 1e-12
+
+
+@pytest.fixture
+def op2(backend):
+    from pyop2_b200 import op2 as _op2
+    return _op2
+
+
+def _clear_consts():
+    from pyop2_b200 import base
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+
+
+@pytest.mark.parametrize("dtype,dim,soa", [(np.float64, 4, False), (np.float64, 3, True),
+                                           (np.int8, 3, False), (np.int32, 1, False)])
+def test_halo_pack_unpack_match_numpy(op2, dtype, dim, soa):
+    from pyop2_b200 import b200
+    n = 1000
+    rng = np.random.default_rng(5)
+    s = op2.Set(n, dim, "s")
+    vals = rng.integers(0, 100, size=(n, dim)).astype(dtype)
+    d = op2.Dat(s, vals.copy(), dtype, "d", soa=soa)
+    rows = b200._DatRows(d)
+    idx = rng.choice(n, 300, replace=False).astype(np.int32)
+    buf = rows.pack(idx)
+    got = buf.to_host().reshape(dim, 300).T if soa else buf.to_host().reshape(300, dim)
+    np.testing.assert_array_equal(got, vals[idx])
+    dst = rng.choice(n, 300, replace=False).astype(np.int32)
+    rows.unpack(dst, buf)
+    want = vals.copy()
+    want[dst] = vals[idx]
+    np.testing.assert_array_equal(d.data_ro.reshape(n, dim), want)
+
+
+def test_partitioned_set_runs_core_owned_and_exec_ranges(op2):
+    """One rank, sizes (core, owned, exec, total) = (3, 6, 8, 10): an
+    indirect loop that increments through a Map runs the execute halo too,
+    while its Global reduction keeps the owned elements' sum only
+    (pyop2/base.py:216-249); a direct loop runs the owned elements."""
+    s = op2.Set([3, 6, 8, 10], 1, "parts")
+    t = op2.Set(10, 1, "targets")
+    m = op2.Map(s, t, 1, np.arange(10, dtype=np.int32), "ident")
+    out = op2.Dat(t, np.zeros(10), np.float64, "out")
+    g = op2.Global(1, 0.0, np.float64, "g")
+    k = op2.Kernel("void k(double *o, double *g, double *v) { o[0] += v[0]; g[0] += v[0]; }", "k")
+    v = op2.Dat(s, np.arange(1.0, 11.0), np.float64, "v")
+    op2.par_loop(k, s, out(m[0], op2.INC), g(op2.INC), v(op2.IdentityMap, op2.READ))
+    np.testing.assert_array_equal(out.data_ro.ravel(), [1, 2, 3, 4, 5, 6, 7, 8, 0, 0])
+    assert g.data[0] == 21.0
+    kd = op2.Kernel("void kd(double *v, double *g) { v[0] *= 2.0; g[0] += 1.0; }", "kd")
+    h = op2.Global(1, 0.0, np.float64, "h")
+    op2.par_loop(kd, s, v(op2.IdentityMap, op2.RW), h(op2.INC))
+    np.testing.assert_array_equal(v.data_ro.ravel(), [2, 4, 6, 8, 10, 12, 7, 8, 9, 10])
+    assert h.data[0] == 6.0
+
+
+class _Recorder(object):
+    """The op2 API with par_loop recorded instead of run."""
+
+    def __init__(self, op2):
+        self._op2, self.calls = op2, []
+
+    def __getattr__(self, name):
+        return getattr(self._op2, name)
+
+    def par_loop(self, kernel, iterset, *args):
+        self.calls.append((kernel, iterset, args))
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_partitioned_airfoil_matches_oracle(op2, nranks):
+    from pyop2_b200 import b200, halo
+    from pyop2_b200.workloads import airfoil, meshes
+    sys.path.insert(0, ROOT)
+    from oracle import seq
+    g = meshes.airfoil_grid(60, 30, 3)
+    q0 = airfoil.initial_q(g.ncells, 3).reshape(-1, 4)
+    for c in list(seq._CONSTS.values()):
+        c.remove_from_namespace()
+    O = airfoil.build(seq, 0, 0, grid=g, q0=q0.copy())
+    ref_rms = [float(airfoil.iteration(seq, O).data[0]) for _ in range(3)]
+    _clear_consts()
+    parts = airfoil.partition_grid(g, nranks)
+    comms = halo.LocalGroup(nranks).comms()
+    ranks = [airfoil.build_partitioned(op2, g, parts[r], comms[r], 3, q0, consts=(r == 0))
+             for r in range(nranks)]
+    for A in ranks:
+        assert A.edges.core_size < A.edges.size < A.edges.exec_size
+    rms = []
+    try:
+        for _ in range(3):
+            recs = [_Recorder(op2) for _ in ranks]
+            outs = [airfoil.iteration(rec, A) for rec, A in zip(recs, ranks)]
+            for k in range(len(recs[0].calls)):
+                halo.run_lockstep([b200.par_loop_phases(kern, it, *args)
+                                   for kern, it, args in (recs[r].calls[k] for r in range(nranks))])
+            vals = [float(x.data[0]) for x in outs]
+            assert max(vals) == min(vals)
+            rms.append(vals[0])
+        q = np.full((g.ncells, 4), np.nan)
+        for p, A in zip(parts, ranks):
+            ls = p.sets["cells"]
+            q[ls.l2g[:ls.sizes[1]]] = A.p_q.data_ro[:ls.sizes[1]]
+        assert rel_err(q, O.p_q.data) < TOL
+        for a, b in zip(rms, ref_rms):
+            assert abs(a - b) <= TOL * abs(b)
+        # the partitioned loops ran in the atomic form, in element ranges
+        assert all(bl.spec.mode in ("direct", "atomic") for bl in b200.ParLoop._bound_cache.values()
+                   if bl.partitioned)
+    finally:
+        _clear_consts()
