@@ -1970,6 +1970,17 @@ def _global_value(g):
     return _DeviceHaloBuffer(g._device.ptr, g._data.nbytes, g.dtype, g._data.shape, g)
 
 
+def torch_comm(group=None):
+    """A halo communicator over a ``torch.distributed`` group (NCCL between
+    GPUs, one process per GPU) whose transfers are ordered with the
+    library's stream: torch's current stream is that stream while they are
+    issued and waited for."""
+    import torch
+    s = C.c_uint64()
+    call("op2b_default_stream", C.byref(s))
+    return halo_mod.TorchComm(group, torch.cuda.ExternalStream(s.value))
+
+
 def _partitioned(iterset):
     """The set has halo elements (sizes core < owned < exec < total, as the
     reference runs over distributed meshes)."""
