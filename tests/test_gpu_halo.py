@@ -131,3 +131,48 @@ def test_partitioned_airfoil_matches_oracle(op2, nranks):
                    if bl.partitioned)
     finally:
         _clear_consts()
+
+
+def test_torch_comm_allreduce_on_device_values(op2):
+    """The NCCL communicator on one rank: the Global's device value is
+    reduced through a torch tensor over the library's own memory, with the
+    library's stream as torch's current stream (a one-rank group: the sum is
+    the value itself, and what the execute halo adds is dropped)."""
+    import socket
+    from datetime import timedelta
+    import torch
+    import torch.distributed as dist
+    from pyop2_b200 import b200, halo
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                            world_size=1, timeout=timedelta(seconds=60))
+    try:
+        comm = b200.torch_comm()
+        assert comm.size == 1
+        s = op2.Set([3, 6, 8, 8], 1, "tc_parts", halo=op2.Halo([[]], [[]], comm=comm))
+        t = op2.Set(8, 1, "tc_targets")
+        m = op2.Map(s, t, 1, np.arange(8, dtype=np.int32), "tc_ident")
+        out = op2.Dat(t, np.zeros(8), np.float64, "tc_out")
+        v = op2.Dat(s, np.arange(1.0, 9.0), np.float64, "tc_v")
+        g = op2.Global(1, 0.5, np.float64, "tc_g")
+        k = op2.Kernel("void k(double *o, double *g, double *v) { o[0] += v[0]; g[0] += v[0]; }",
+                       "k")
+        op2.par_loop(k, s, out(m[0], op2.INC), g(op2.INC), v(op2.IdentityMap, op2.READ))
+        assert g.data[0] == 21.5
+        np.testing.assert_array_equal(out.data_ro.ravel(), np.arange(1.0, 9.0))
+        # a device buffer seen as a torch tensor is the same memory
+        buf = b200._DeviceHaloBuffer.alloc(32, np.float64, (4,))
+        buf.from_host(np.arange(4.0))
+        t4 = buf.tensor()
+        b200.synchronize()
+        assert t4.device.type == "cuda" and t4.cpu().tolist() == [0.0, 1.0, 2.0, 3.0]
+        req = halo.GlobalReduction(buf, comm, "max").begin()
+        req.wait()
+        b200.synchronize()
+        np.testing.assert_array_equal(buf.to_host(), np.arange(4.0))
+    finally:
+        dist.destroy_process_group()
