@@ -1675,7 +1675,10 @@ class _BoundLoop(object):
     def matches(self, loop):
         """The Dats, Maps and Mats the loop was bound to are all alive (the
         key holds their ids, which a new object could reuse otherwise)."""
-        return all(r() is not None for r in self.refs)
+        for r in self.refs:
+            if r() is None:
+                return False
+        return True
 
     def _prepare(self, loop):
         """First run: device copies of the Dats, the full parameter block in a
@@ -1831,19 +1834,37 @@ def _loop_key(kernel, iterset, extents, args):
     the index and the access mode (a Global only by type, so a fresh Global
     per call reuses the loop), plus the Consts and configuration."""
     k = [kernel.cache_key, id(iterset), extents]
+    app = k.append
     for a in args:
         d = a._dat
-        if isinstance(d, base.Global):
-            k.append(("g", d.dtype.str, d.cdim, a._access._mode))
-        elif isinstance(d, base.Mat):
-            m, ix = a._map, a._idx
-            k.append(("m", id(d), id(m[0]), id(m[1]), ix[0].index, ix[1].index, a._access._mode))
-        else:
+        kind = _KEY_KIND.get(type(d))
+        if kind is None:
+            kind = _key_kind(type(d))
+        if kind == "d":
             ix = a._idx
-            its = isinstance(ix, IterationIndex)
-            k.append(("d", id(d), id(a._map), its, ix.index if its else ix, a._access._mode))
-    k.append(_env_key())
+            if type(ix) is int or ix is None:
+                app(("d", id(d), id(a._map), False, ix, a._access._mode))
+            else:
+                its = isinstance(ix, IterationIndex)
+                app(("d", id(d), id(a._map), its, ix.index if its else ix, a._access._mode))
+        elif kind == "g":
+            app(("g", d.dtype.str, d.cdim, a._access._mode))
+        else:
+            m, ix = a._map, a._idx
+            app(("m", id(d), id(m[0]), id(m[1]), ix[0].index, ix[1].index, a._access._mode))
+    app(_env_key())
     return tuple(k)
+
+
+_KEY_KIND = {}
+
+
+def _key_kind(t):
+    """'g' (Global), 'm' (Mat) or 'd' (anything else, a Dat) for an argument
+    data type, remembered per type."""
+    k = "g" if issubclass(t, base.Global) else "m" if issubclass(t, base.Mat) else "d"
+    _KEY_KIND[t] = k
+    return k
 
 
 class _Args(object):
@@ -2110,9 +2131,9 @@ def par_loop(kernel, it_space, *args):
             halo_mod.run(_loop_phases(bl, _Args(args), args))
             return
         bl.run(_Args(args))
-        for a in args:
-            if a._access is not READ and isinstance(a._dat, base.Dat):
-                a._dat.needs_halo_update = True
+        # the Dats the call writes are the bound ones (same objects)
+        for d in bl._written:
+            d._needs_halo_update = True
         return
     ParLoop(kernel, it_space, *args).compute()
 

@@ -52,6 +52,16 @@ MAX = Access("MAX")
 
 
 # ------------------------------------------------------------------------ Arg
+def _new_arg(data, map, idx, access):
+    """The selected backend's Arg (as ``_make_object('Arg', ...)``), built
+    with positional arguments: this runs for every argument of every
+    par_loop call."""
+    cls = _BackendSelector._backend.__dict__.get('Arg')
+    if cls is None:
+        return _make_object('Arg', data=data, map=map, idx=idx, access=access)
+    return cls(data, map, idx, access)
+
+
 class Arg(object):
     """An argument to a :func:`par_loop`; build it by calling a Dat/Mat/Global."""
 
@@ -438,7 +448,7 @@ class Dat(DataCarrier):
         if isinstance(path, Map):
             if path._dataset != self._dataset and path is not IdentityMap:
                 raise MapValueError("Dataset of Map does not match Dataset of Dat.")
-            return _make_object('Arg', data=self, map=path, access=access)
+            return _new_arg(self, path, None, access)
         path._dat = self
         path._access = access
         return path
@@ -638,8 +648,12 @@ class Global(DataCarrier):
 
     @validate_type(('name', str, NameTypeError))
     def __init__(self, dim, data=None, dtype=None, name=None):
-        self._dim = as_tuple(dim, (int, np.integer))
-        self._dim = tuple(int(d) for d in self._dim)
+        if type(dim) is int:
+            # the usual scalar Global of a reduction (a fresh one per loop
+            # call in the demos): no tuple normalisation
+            self._dim = (dim,)
+        else:
+            self._dim = tuple(int(d) for d in as_tuple(dim, (int, np.integer)))
         self._cdim = math.prod(self._dim)
         self._data = verify_reshape(data, dtype, self._dim, allow_none=True)
         self._name = name or "global_%d" % Global._globalcount
@@ -647,7 +661,7 @@ class Global(DataCarrier):
 
     @validate_in(('access', _modes, ModeValueError))
     def __call__(self, access):
-        return _make_object('Arg', data=self, access=access)
+        return _new_arg(self, None, None, access)
 
     def __str__(self):
         return "OP2 Global Argument: %s with dim %s and value %s" % (self._name, self._dim, self._data)
@@ -730,7 +744,7 @@ class Map(object):
     def __getitem__(self, index):
         # the common case first: a Python int within the arity
         if type(index) is int and 0 <= index < self._dim:
-            return _make_object('Arg', map=self, idx=index)
+            return _new_arg(None, self, index, None)
         if isinstance(index, slice):
             # test/unit/test_api.py:655-660: slicing a Map is not supported
             raise NotImplementedError("Slicing maps is not allowed")
