@@ -929,6 +929,41 @@ class ReadReplica(object):
             self.wgen = dat._wgen
 
 
+class GatheredReplica(object):
+    """A device copy of the rows a Map names, element by element: row k of
+    element e at (e * arity + k).  A loop that only reads the Dat through
+    that Map streams its rows in element order with no Map read and no
+    dependent gather, at the price of arity copies of each row.  Refreshed
+    from the Dat (one row gather through the Map) whenever the Dat's write
+    generation changed since the last refresh."""
+
+    def __init__(self, dat, m):
+        import weakref
+        self.dat_ref, self.map_ref = weakref.ref(dat), weakref.ref(m)
+        self.n = m.iterset.total_size * m.dim
+        self.rows = DeviceBuffer(max(self.n * dat.dtype.itemsize * dat.cdim, 16))
+        self.wgen = None
+
+    def ensure(self, dat):
+        """Refresh the copy if the Dat changed since the last refresh."""
+        if dat._state is HOST:
+            dat._to_device()
+        if self.wgen != dat._wgen:
+            call("op2b_rows_gather", self.rows.ptr, dat._device.ptr, self.map_ref()._to_device().ptr,
+                 self.n, dat.dtype.itemsize * dat.cdim, 0)
+            self.wgen = dat._wgen
+
+
+def gathered_replica(dat, m):
+    key = ("gathered", id(dat), id(m))
+    rep = _REPLICAS.get(key)
+    if rep is None or rep.dat_ref() is not dat or rep.map_ref() is not m:
+        for k in [k for k, r in _REPLICAS.items() if r.dat_ref() is None or r.map_ref() is None]:
+            del _REPLICAS[k]
+        rep = _REPLICAS[key] = GatheredReplica(dat, m)
+    return rep
+
+
 def read_replica(dat, m):
     key = (id(dat), id(m))
     rep = _REPLICAS.get(key)
@@ -1405,6 +1440,14 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
                     spec.itspace_split = (nr, nc)
     if spec.mode == "direct":
         spec.direct_unroll = max(1, int(cfg.cfg['direct_unroll']))
+    if (spec.mode == "atomic" and cfg.cfg['read_replicas'] and cfg.cfg['gathered_replicas']
+            and iterset.size >= int(cfg.cfg['replica_min_size'])):
+        # READ-only Dats read through one Map: a copy gathered per element
+        # (no Map read, no dependent gather) while it fits the byte cap
+        cap = float(cfg.cfg['gathered_max_gb']) * 1e9
+        spec.gathered = tuple(
+            (j, k) for j, k in replica_candidates(spec, specs, dats, maps)
+            if iterset.total_size * maps[k].dim * dats[j].dtype.itemsize * dats[j].cdim <= cap)
     if (fmad is None and cfg.cfg['fmad_inc'] and not cfg.cfg['fmad']
             and spec.mode in ("staged", "atomic", "gather", "plan")
             and any(a.access == "INC" and a.kind != "gbl" for a in specs)):
@@ -1585,8 +1628,14 @@ class _BoundLoop(object):
         # READ replicas: (Dat slot, Dat, replica); the stub reads the copy
         # through the renumbered Map
         self.replicas = []
+        for j, k in spec.gathered:
+            rep = gathered_replica(dats[j], maps[k])
+            vals["d%d" % j] = rep.rows.ptr
+            self.replicas.append((j, dats[j], rep))
         if cfg.cfg['read_replicas'] and iterset.size >= int(cfg.cfg['replica_min_size']):
             for j, k in replica_candidates(spec, specs, dats, maps):
+                if (j, k) in spec.gathered:
+                    continue
                 rep = read_replica(dats[j], maps[k])
                 vals["m%d" % k] = rep.map.ptr
                 self.replicas.append((j, dats[j], rep))
@@ -1823,7 +1872,8 @@ def _env_key():
                         cfg.cfg['replica_min_size'], cfg.cfg['fmad_inc'],
                         cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs'],
                         cfg.cfg['direct_unroll'], cfg.cfg['mat_slots_rel'],
-                        cfg.cfg['staged_pair']))
+                        cfg.cfg['staged_pair'], cfg.cfg['gathered_replicas'],
+                        cfg.cfg['gathered_max_gb']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

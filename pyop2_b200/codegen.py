@@ -96,6 +96,9 @@ class LoopSpec(object):
         # elements per thread per round of a direct stub (their loads issued
         # together before the kernel calls)
         self.direct_unroll = 1
+        # (Dat slot, Map slot) pairs of the atomic form read from a gathered
+        # copy: row k of element e at (e * arity + k), no Map read
+        self.gathered = ()
         # staged form over a locality partition (mode 'staged'): map_stage
         # {map slot: staged Map}, stage_arity, row_base (first loc row of each
         # staged Map), read_pairs / inc_pairs [(Dat slot, staged Map, ctype,
@@ -124,7 +127,7 @@ class LoopSpec(object):
                 tuple(sorted(self.owner.items())) if self.owner else None, self.batch,
                 self.mat_slots, _freeze(self.region), tuple(self.mat_alias),
                 self.mat_per_entry, self.itspace_split, self.direct_unroll,
-                self.mat_slots_rel)
+                self.mat_slots_rel, tuple(self.gathered))
 
     @property
     def needs_coloring(self):
@@ -1054,11 +1057,23 @@ def _inc_sink(spec, a, n, k, src, val, ind):
     return "%sop2b_atomic_row(%s, %s);" % (ind, src, val)
 
 
+def _gathered_row(spec, a, r):
+    """Row ``r`` (an int or the iteration index variable) of element e of a
+    READ arg read from its gathered copy (element-major: the arity rows of
+    one element next to each other)."""
+    return "p.d%d + ((op2b_i64)e * %d + %s) * %d" % (a.slot, spec.maps[a.mslot], r, a.cdim)
+
+
 def _atomic_element(spec, ind, ranges=None):
     """Lines computing element ``e`` of an atomic-mode (or two-phase)
     indirect loop."""
     L = []
-    used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")} |
+    G = set(tuple(x) for x in spec.gathered)
+
+    def gathered(a):
+        return a.access == "READ" and (a.slot, a.mslot) in G
+    used_maps = sorted({a.mslot for a in spec.args if a.kind in ("ind", "vec", "its", "mat")
+                        and not gathered(a)} |
                        {a.cmslot for a in spec.args if a.kind == "mat"})
     for k in used_maps:
         ar = spec.maps[k]
@@ -1072,7 +1087,8 @@ def _atomic_element(spec, ind, ranges=None):
         elif a.kind == "direct":
             exprs.append(_direct_row(a, n, "e", pre, post, ind))
         elif a.kind == "ind":
-            row = "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, a.idx, c)
+            row = (_gathered_row(spec, a, a.idx) if gathered(a) else
+                   "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, a.idx, c))
             if a.access == "INC":
                 pre.append("%s__align__(16) %s a%d[%d]; op2b_zero(a%d);" % (ind, t, n, c, n))
                 apply.append(_inc_sink(spec, a, n, a.idx, row, "a%d" % n, ind))
@@ -1089,7 +1105,8 @@ def _atomic_element(spec, ind, ranges=None):
             if a.access in ("READ", "INC"):
                 pre.append("%s__align__(16) %s a%d[%d][%d];" % (ind, t, n, cnt, c))
                 for r in range(cnt):
-                    src = "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, r, c)
+                    src = (_gathered_row(spec, a, r) if gathered(a) else
+                           "p.d%d + (op2b_i64)mr%d[%d] * %d" % (a.slot, a.mslot, r, c))
                     if a.access == "READ":
                         pre.append("%sop2b_load<%s, %d, %s>(a%d[%d], %s);" % (ind, t, c, _ro(a), n, r, src))
                     else:

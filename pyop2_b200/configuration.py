@@ -78,6 +78,10 @@ keys of the B200 backend:
   neighbouring elements read lie next to each other.  The copy is refreshed
   when the Dat was written since (host writes, loops, zero, arithmetic);
   it costs one extra copy of the Dat and of the Map;
+* ``gathered_replicas``: with ``read_replicas``, such a loop reads the Dat
+  from a copy gathered element by element (row k of element e at
+  e * arity + k: no Map read, no dependent gather) when that copy takes at
+  most ``gathered_max_gb`` GB (arity copies of each row);
 * ``fmad_inc``: compile the element code of loops with indirect INC in the
   staged, atomic, gather and coloured forms with multiply-add contraction
   (their sums are reassociated anyway, so they already differ from the
@@ -134,6 +138,8 @@ _defaults = {
     'mat_per_entry': True,
     'read_replicas': True,
     'replica_min_size': 262144,
+    'gathered_replicas': False,
+    'gathered_max_gb': 2.0,
     'fmad_inc': False,
     'programmatic_launch': False,
     'itspace_split': '',

@@ -443,14 +443,16 @@ def test_two_phase_kahan_precision_form(op2):
 @pytest.mark.parametrize("opts", [dict(programmatic_launch=True), dict(fmad_inc=True),
                                   dict(staged_tl_regs=True), dict(read_replicas=True,
                                                                   replica_min_size=0),
-                                  dict(staged_pair=2), dict(staged_pair=2, partition_size=512)])
+                                  dict(staged_pair=2), dict(staged_pair=2, partition_size=512),
+                                  dict(read_replicas=True, replica_min_size=0,
+                                       gathered_replicas=True)])
 def test_airfoil_chain_launch_options_match_oracle(op2, opts):
     """The launch-level options on the staged airfoil chain: programmatic
     dependent launch (every stub waits for its predecessor), multiply-add
     contraction in INC-form loops, target ids in registers, READ replicas on
     small sets, two elements per thread in the staged passes (odd and even
-    pass counts); q and rms within 1e-12 of the oracle after three
-    iterations."""
+    pass counts), element-gathered READ copies; q and rms within 1e-12 of
+    the oracle after three iterations."""
     from pyop2_b200 import b200
     from pyop2_b200 import configuration as cfg
     from pyop2_b200._lib import call
@@ -469,6 +471,9 @@ def test_airfoil_chain_launch_options_match_oracle(op2, opts):
         assert rel_err(gr.data, orr.data) < TOL
         if opts.get("read_replicas"):
             assert any(bl.replicas for bl in b200.ParLoop._bound_cache.values()
+                       if bl.spec.kernel_name == "adt_calc")
+        if opts.get("gathered_replicas"):
+            assert any(bl.spec.gathered for bl in b200.ParLoop._bound_cache.values()
                        if bl.spec.kernel_name == "adt_calc")
     finally:
         call("op2b_set_programmatic_launch", 0)
