@@ -427,11 +427,12 @@ int op2b_mat_slots_rel_build(uint64_t rowptr, uint64_t colidx, uint64_t rmap, ui
  *    (split the list, or call op2b_mat_zero_rows); so are rows outside
  *    [0, mat_rows) and elem_bytes other than 4 or 8, before any copy or launch.
  *  - The first call on a device looks up the scratch array's device address
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    (cudaGetSymbolAddress).
  *  - All calls share the one scratch array, which keeps the last call's row
  *    list: calls that overlap on the GPU (other streams, other threads) race
  *    and must be serialised by the caller.  The call returns after its work
- *    has finished on the stream. */
+ *    has finished on the stream (it synchronises the stream), so it cannot
+ *    be recorded into a CUDA graph: call it outside any stream capture. */
 #define OP2B_ZERO_ROWS_STATIC_MAX 65536
 int op2b_mat_zero_rows_static(uint64_t vals, uint64_t rowptr, uint64_t colidx, int32_t mat_rows,
                               const int32_t *rows, int32_t nrows_zero, double diag,
