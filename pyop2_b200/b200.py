@@ -2074,6 +2074,9 @@ def _loop_phases(bl, loop, args):
     write through a Map.  A generator that yields where the rank waits for
     its peers (:func:`pyop2_b200.halo.run_lockstep` drives in-process ranks)."""
     it = bl.iterset
+    if _state.get('capturing') and _set_comm(it).size > 1:
+        raise DeviceError("a par_loop over a set shared with other ranks exchanges halos "
+                          "through the host or NCCL and cannot be recorded into a CUDA graph")
     direct = all(a._map is None or a._map is IdentityMap for a in args)
     exchanges = []
     if not direct:
