@@ -176,3 +176,58 @@ def test_torch_comm_allreduce_on_device_values(op2):
         np.testing.assert_array_equal(buf.to_host(), np.arange(4.0))
     finally:
         dist.destroy_process_group()
+
+
+def test_partitioned_p1_rhs_matches_oracle(op2):
+    """P1 RHS assembly (iteration-space INC through a Map, vector-map READ)
+    over a mesh split across two ranks on one GPU, then a reduction over the
+    owned nodes: owned rows of b and the all-reduced sum equal the oracle's
+    on the undivided mesh."""
+    from pyop2_b200 import b200, halo, partition
+    from pyop2_b200.workloads import fem
+    sys.path.insert(0, ROOT)
+    from oracle import seq
+    coords, elem = fem.square_p1(24)
+    O = fem.build_p1(seq, 24)
+    seq.par_loop(O.k_rhs, O.elements(3), O.b(O.elem_node[seq.i[0]], seq.INC),
+                 O.coords(O.elem_vnode, seq.READ), O.f(O.elem_node, seq.READ))
+    ne, nn = len(elem), len(coords)
+    cx = coords[elem, 0].mean(axis=1)
+    own_e = (cx > np.median(cx)).astype(np.int64)
+    first = np.full(nn, ne, np.int64)
+    np.minimum.at(first, elem.ravel(), np.repeat(np.arange(ne), 3))
+    parts = partition.partition({"nodes": nn, "elements": ne},
+                                {"elem_node": ("elements", "nodes", elem)},
+                                {"elements": own_e, "nodes": own_e[first]}, 2)
+    comms = halo.LocalGroup(2).comms()
+    f_all = np.sin(np.pi * coords[:, 0]) * np.sin(np.pi * coords[:, 1])
+    k_sum = op2.Kernel("void s(double *b, double *t) { t[0] += b[0]; }", "s")
+    ranks = []
+    for r, p in enumerate(parts):
+        S = p.sets
+
+        def mkset(name, dim):
+            ls = S[name]
+            return op2.Set(list(ls.sizes), dim, name, halo=op2.Halo(ls.sends, ls.receives, comm=comms[r]))
+        nodes, vnodes, elements = mkset("nodes", 1), mkset("nodes", 2), mkset("elements", 1)
+        lv = p.maps["elem_node"][2]
+        en = op2.Map(elements, nodes, 3, lv, "en")
+        evn = op2.Map(elements, vnodes, 3, lv, "evn")
+        c = op2.Dat(vnodes, S["nodes"].local_rows(coords), np.float64, "c")
+        f = op2.Dat(nodes, S["nodes"].local_rows(f_all), np.float64, "f")
+        b = op2.Dat(nodes, np.zeros(S["nodes"].sizes[3]), np.float64, "b")
+        for d in (c, f, b):
+            d.needs_halo_update = False
+        ranks.append((nodes, elements, en, evn, c, f, b, op2.Global(1, 0.0, np.float64, "t")))
+    k_rhs = op2.Kernel(fem.P1_RHS, "p1_rhs")
+    halo.run_lockstep([b200.par_loop_phases(k_rhs, el(3), b(en[op2.i[0]], op2.INC),
+                                            c(evn, op2.READ), f(en, op2.READ))
+                       for nodes, el, en, evn, c, f, b, t in ranks])
+    halo.run_lockstep([b200.par_loop_phases(k_sum, nodes, b(op2.IdentityMap, op2.READ), t(op2.INC))
+                       for nodes, el, en, evn, c, f, b, t in ranks])
+    got = np.full(nn, np.nan)
+    for p, (nodes, el, en, evn, c, f, b, t) in zip(parts, ranks):
+        ls = p.sets["nodes"]
+        got[ls.l2g[:ls.sizes[1]]] = b.data_ro.ravel()[:ls.sizes[1]]
+        assert abs(t.data[0] - O.b.data.sum()) <= TOL * abs(O.b.data).sum()
+    assert rel_err(got, O.b.data) < TOL
