@@ -34,7 +34,7 @@ from .base import (INC, MAX, MIN, READ, RW, WRITE, IdentityMap, IterationIndex, 
                    i)
 from .exceptions import DeviceError, MapValueError
 from .logger import debug
-from .utils import as_tuple, maybe_setflags, verify_reshape
+from .utils import maybe_setflags, verify_reshape
 
 DEVICE_UNALLOCATED = 'DEVICE_UNALLOCATED'
 HOST = 'HOST'

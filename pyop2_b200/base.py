@@ -17,10 +17,9 @@ from hashlib import md5
 
 import numpy as np
 
-from . import configuration as cfg
 from .backends import _BackendSelector, _make_object
 from .caching import Cached
-from .exceptions import (DataTypeError, DataValueError, DimTypeError, IndexTypeError,
+from .exceptions import (DataTypeError, DimTypeError, IndexTypeError,
                          IndexValueError, MapTypeError, MapValueError, ModeValueError,
                          NameTypeError, SetTypeError, SizeTypeError, SparsityTypeError)
 from .utils import as_tuple, as_type, maybe_setflags, validate_in, validate_type, verify_reshape
