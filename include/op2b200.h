@@ -243,6 +243,17 @@ int op2b_region_plan_info(uint64_t plan, int32_t *nblocks, int32_t *nregions, in
  * element at position pos is tlist[toff[b*nstage+s] + loc[(row0(s)+r)*set_size+pos]],
  * 6 thrcol [set_size] (thread colour per position), 7 nthrcol [nblocks]. */
 int op2b_region_plan_array(uint64_t plan, int32_t which, uint64_t *dptr, int64_t *count);
+/* Renumber a built plan's staged slots so that the rows eight consecutive
+ * positions of a block read (one quarter-warp of a staged stub, for any CTA
+ * size) lie in distinct 16-byte shared-memory bank groups where the targets
+ * allow: per (block, staged Map) a greedy choice of slot residue mod 8 over
+ * the groups of 8 positions, row by row, then slots grouped by residue.  A
+ * block's slot count becomes 8 x its largest residue class; padding slots
+ * have target -1 in tlist (stubs skip them).  tcnt, toff, tlist, loc and the
+ * max counts of op2b_region_plan_info change; order, boff and the colours
+ * do not.  Idempotent.  No reference counterpart (the reference staged rows
+ * in sorted target order, pyop2/plan.pyx:112-212). */
+int op2b_region_plan_bank_slots(uint64_t plan, uint64_t stream);
 int op2b_region_plan_free(uint64_t plan);
 
 /* ------------------------------------------------------------------------

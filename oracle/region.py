@@ -169,3 +169,84 @@ def region_plan(grow_values, ntargets, stage_values, part_size, region_size, sta
         nthrcol[b] = col.max() + 1 if col.size else 0
     return dict(order=order, boff=boff, tlist=tlist, toff=toff, tcnt=tcnt, loc=loc,
                 thrcol=thrcol, nthrcol=nthrcol, nregions=nregions, levels=levels + 1)
+
+
+def bank_slots(plan, arities):
+    """The plan with its staged slots renumbered for shared-memory bank
+    groups, as op2b_region_plan_bank_slots does: per (block, staged Map),
+    over groups of 8 consecutive positions and row by row, every target not
+    yet placed takes the residue mod 8 unused in its group with the fewest
+    targets so far (ties: the lowest residue; any residue when all 8 are
+    used); slots are residue + 8 * rank in the residue class (first-use
+    order); padding slots hold target -1."""
+    boff, tcnt, toff, tlist, loc = (plan[k] for k in ("boff", "tcnt", "toff", "tlist", "loc"))
+    ns, nb = len(arities), len(boff) - 1
+    row0 = np.concatenate([[0], np.cumsum(arities)]).astype(np.int64)
+    new_loc = loc.copy()
+    ncnt = np.zeros(nb * ns, dtype=np.int32)
+    lists = []
+    for b in range(nb):
+        start, nelem = int(boff[b]), int(boff[b + 1] - boff[b])
+        for s in range(ns):
+            nu = int(tcnt[b * ns + s])
+            res = [-1] * nu
+            cls = [0] * 8
+            for g in range(0, nelem, 8):
+                m = min(8, nelem - g)
+                for r in range(arities[s]):
+                    ts = [int(loc[row0[s] + r, start + g + i]) for i in range(m)]
+                    used = 0
+                    for t in ts:
+                        if res[t] >= 0:
+                            used |= 1 << res[t]
+                    for t in ts:
+                        if res[t] >= 0:
+                            continue
+                        free = 0xFF if used == 0xFF else (~used & 0xFF)
+                        best = -1
+                        for c in range(8):
+                            if (free >> c) & 1 and (best < 0 or cls[c] < cls[best]):
+                                best = c
+                        res[t] = best
+                        cls[best] += 1
+                        used |= 1 << best
+            nxt = [0] * 8
+            perm = np.zeros(nu, dtype=np.int64)
+            for k in range(nu):
+                c = max(res[k], 0)
+                perm[k] = c + 8 * nxt[c]
+                nxt[c] += 1
+            top = int(perm.max()) + 1 if nu else 0
+            ncnt[b * ns + s] = top
+            lst = np.full(top, -1, dtype=np.int32)
+            lst[perm] = tlist[toff[b * ns + s]:toff[b * ns + s] + nu]
+            lists.append(lst)
+            for r in range(arities[s]):
+                seg = new_loc[row0[s] + r, start:start + nelem]
+                new_loc[row0[s] + r, start:start + nelem] = perm[seg.astype(np.int64)]
+    out = dict(plan)
+    out.update(tcnt=ncnt, toff=np.concatenate([[0], np.cumsum(ncnt)]).astype(np.int32),
+               tlist=np.concatenate(lists).astype(np.int32) if lists else np.zeros(0, np.int32),
+               loc=new_loc)
+    return out
+
+
+def bank_conflicts(plan, arities, chunks):
+    """Extra 16-byte bank-group wavefronts of the staged-row reads of a
+    plan: per group of 8 consecutive positions of a block and per row, the
+    largest number of distinct slots sharing a residue mod 8, minus one,
+    summed; ``chunks`` is the row size in 16-byte chunks (informative
+    metric for tests)."""
+    boff, loc = plan["boff"], plan["loc"]
+    row0 = np.concatenate([[0], np.cumsum(arities)]).astype(np.int64)
+    total = 0
+    for b in range(len(boff) - 1):
+        start, nelem = int(boff[b]), int(boff[b + 1] - boff[b])
+        for s in range(len(arities)):
+            for g in range(0, nelem, 8):
+                m = min(8, nelem - g)
+                for r in range(arities[s]):
+                    slots = set(int(x) for x in loc[row0[s] + r, start + g:start + g + m])
+                    counts = np.bincount([x % 8 for x in slots], minlength=8)
+                    total += (int(counts.max()) - 1) * chunks
+    return total

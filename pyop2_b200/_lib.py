@@ -81,6 +81,7 @@ _SIGS = {
     "op2b_region_plan_info": [u64, i32p, i32p, i32p, i32p, i64p, i32p],
     "op2b_region_plan_array": [u64, i32, u64p, i64p],
     "op2b_region_plan_free": [u64],
+    "op2b_region_plan_bank_slots": [u64, u64],
     "op2b_sparsity_build": [i32, i32, i32, i32, i32, u64p, i32p, u64p, i32p, i32p, u64, u64p],
     "op2b_sparsity_info": [u64, i32p, i64p],
     "op2b_sparsity_arrays": [u64, u64p, u64p, u64p],

@@ -847,7 +847,8 @@ class RegionPlan(object):
     thread colours over the targets of the staged Maps flagged in
     ``stage_inc``."""
 
-    def __init__(self, set_size, part_size, region_size, grow_map, stage_maps, stage_inc=None):
+    def __init__(self, set_size, part_size, region_size, grow_map, stage_maps, stage_inc=None,
+                 bank_slots=False):
         ns = len(stage_maps)
         smap = (C.c_uint64 * max(ns, 1))(*[m._to_device().ptr for m in stage_maps])
         sar = (C.c_int32 * max(ns, 1))(*[m.dim for m in stage_maps])
@@ -857,6 +858,9 @@ class RegionPlan(object):
         call("op2b_region_plan_build", set_size, part_size, region_size, grow_map._to_device().ptr,
              grow_map.dim, grow_map.dataset.total_size, ns, smap, sar, sinc, 0, C.byref(h))
         self._handle = h.value
+        if bank_slots:
+            call("op2b_region_plan_bank_slots", self._handle, 0)
+        self.bank_slots = bool(bank_slots)
         nb, nr, lv, tl, mt = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32()
         mc = (C.c_int32 * max(ns, 1))()
         call("op2b_region_plan_info", self._handle, C.byref(nb), C.byref(nr), C.byref(lv), mc,
@@ -1030,10 +1034,11 @@ def region_plan(iterset, maps, region):
     reps = [maps[k] for k in region["stage_maps"]]
     grow = reps[region["grow"]]
     inc = [st in region["inc_stages"] for st in range(len(reps))]
-    key = (iterset.size, ps, rs, id(grow), tuple(id(m) for m in reps), tuple(inc))
+    banks = bool(cfg.cfg['staged_bank_slots'])
+    key = (iterset.size, ps, rs, id(grow), tuple(id(m) for m in reps), tuple(inc), banks)
     plan = _REGION_CACHE.get(key)
     if plan is None:
-        plan = _REGION_CACHE[key] = RegionPlan(iterset.size, ps, rs, grow, reps, inc)
+        plan = _REGION_CACHE[key] = RegionPlan(iterset.size, ps, rs, grow, reps, inc, banks)
     return plan
 
 
@@ -1873,7 +1878,7 @@ def _env_key():
                         cfg.cfg['itspace_split'], cfg.cfg['staged_tl_regs'],
                         cfg.cfg['direct_unroll'], cfg.cfg['mat_slots_rel'],
                         cfg.cfg['staged_pair'], cfg.cfg['gathered_replicas'],
-                        cfg.cfg['gathered_max_gb']))
+                        cfg.cfg['gathered_max_gb'], cfg.cfg['staged_bank_slots']))
         _ENV["gen"] = gen
     return _ENV["key"]
 

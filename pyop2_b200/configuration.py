@@ -44,6 +44,9 @@ keys of the B200 backend:
 * ``staged_tl_regs``: the staged stubs load their block's target ids into
   registers once (with the element rows) and reuse them for the row copies
   and the flush, which then adds one accumulated row per thread;
+* ``staged_bank_slots``: renumber the staged rows of each block of the
+  locality partition so that the rows eight neighbouring threads read lie in
+  distinct shared-memory bank groups (``op2b_region_plan_bank_slots``);
 * ``staged_pair``: 2 makes each thread of a staged stub evaluate two
   elements (of two consecutive passes) before one shared run of colour
   rounds; 1 (default) one element per pass;
@@ -148,6 +151,7 @@ _defaults = {
     'mat_slots_rel': False,
     'graph_overlap': False,
     'staged_pair': 1,
+    'staged_bank_slots': False,
     'hbm_budget_gb': 120.0,
     'pool_reserve_gb': 4.0,
 }

@@ -54,6 +54,8 @@ struct RegionPlan {
   int16_t *loc = nullptr;
   int32_t max_nthrcol = 0;
   std::vector<int32_t> max_count;   // per staged Map: largest tcnt over blocks
+  std::vector<int32_t> arity;       // per staged Map: rows per element (loc rows from row_base)
+  bool bank_slots = false;          // op2b_region_plan_bank_slots applied
 };
 
 constexpr int kRgThreads = 256;
@@ -302,6 +304,100 @@ __global__ void rg_compact_kernel(const RgStage *__restrict__ stages, int nstage
   for (int i = threadIdx.x; i < nu; i += blockDim.x) tlist[dst + i] = st.tmp[(int64_t)blk * st.cap + i];
 }
 
+// Bank-aware slot numbering (op2b_region_plan_bank_slots).  A staged stub's
+// lanes 8k..8k+7 of a warp (positions start+8g .. start+8g+7 of a block,
+// whatever the CTA size) read one staged row each with one 16-byte shared
+// access per chunk; the access is conflict-free when their rows lie in
+// distinct 16-byte bank groups, which with the rows' chunk permutation
+// (op2b_srow_layout) means distinct slot numbers mod 8.  Thread 0 of a
+// (block, staged Map) CTA walks the groups of 8 positions, row by row, and
+// gives every target not yet placed the residue mod 8 unused in its group
+// with the fewest targets so far (any residue when all 8 are taken); slots
+// are then residue + 8 * (rank in its residue class, in first-use order), so
+// a block's slot count becomes 8 x its largest class (unused slots are
+// padding, tlist -1).  perm[b][s][old slot] = new slot, ncnt[b][s] = count.
+__global__ void rg_slot_kernel(int nstage, int set_size, const int32_t *__restrict__ boff,
+                               const int32_t *__restrict__ tcnt, const int16_t *__restrict__ loc,
+                               const int32_t *__restrict__ arity, const int32_t *__restrict__ row0,
+                               int maxc, int16_t *__restrict__ perm, int32_t *__restrict__ ncnt) {
+  extern __shared__ int8_t rg_res[];      // [maxc] residue per old slot
+  const int blk = blockIdx.x, s = blockIdx.y;
+  const int start = boff[blk], nelem = boff[blk + 1] - start;
+  const int nu = tcnt[blk * nstage + s];
+  const int A = arity[s], rb = row0[s];
+  int16_t *pm = perm + ((int64_t)blk * nstage + s) * maxc;
+  for (int k = threadIdx.x; k < nu; k += blockDim.x) rg_res[k] = -1;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  int cls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int g = 0; g < nelem; g += 8) {
+    const int m = min(8, nelem - g);
+    for (int r = 0; r < A; ++r) {
+      const int16_t *row = loc + (int64_t)(rb + r) * set_size + start + g;
+      unsigned used = 0u;
+      for (int i = 0; i < m; ++i) {
+        const int t = row[i];
+        if (rg_res[t] >= 0) used |= 1u << rg_res[t];
+      }
+      for (int i = 0; i < m; ++i) {
+        const int t = row[i];
+        if (rg_res[t] >= 0) continue;
+        const unsigned freec = used == 0xffu ? 0xffu : (~used & 0xffu);
+        int best = -1;
+        for (int c = 0; c < 8; ++c)
+          if (((freec >> c) & 1u) && (best < 0 || cls[c] < cls[best])) best = c;
+        rg_res[t] = (int8_t)best;
+        ++cls[best];
+        used |= 1u << best;
+      }
+    }
+  }
+  int next[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int top = 0;
+  for (int k = 0; k < nu; ++k) {
+    const int c = rg_res[k] < 0 ? 0 : rg_res[k];   // every slot is used, so c >= 0
+    const int v = c + 8 * next[c]++;
+    top = max(top, v + 1);
+    pm[k] = (int16_t)(v <= 32767 ? v : -1);          // loc rows are int16
+  }
+  ncnt[blk * nstage + s] = top <= 32768 ? top : -1;
+}
+
+// New target lists (padding -1) and loc rows in the new numbering; bad[0] is
+// set if any renumbered slot falls outside its block's new count.
+__global__ void rg_slot_apply_kernel(int nstage, int set_size, const int32_t *__restrict__ boff,
+                                     const int32_t *__restrict__ tcnt, const int32_t *__restrict__ toff,
+                                     const int32_t *__restrict__ tlist, const int32_t *__restrict__ ncnt,
+                                     const int32_t *__restrict__ ntoff, int32_t *__restrict__ ntlist,
+                                     const int16_t *__restrict__ loc, int16_t *__restrict__ nloc,
+                                     const int32_t *__restrict__ arity, const int32_t *__restrict__ row0,
+                                     int maxc, const int16_t *__restrict__ perm, int32_t *bad) {
+  const int blk = blockIdx.x, s = blockIdx.y;
+  const int start = boff[blk], nelem = boff[blk + 1] - start;
+  const int bs = blk * nstage + s;
+  const int nu = tcnt[bs], nn = ncnt[bs];
+  const int16_t *pm = perm + (int64_t)bs * maxc;
+  for (int k = threadIdx.x; k < nu; k += blockDim.x) {
+    const int v = pm[k];
+    if (v < 0 || v >= nn) {
+      atomicExch(bad, 1);
+      continue;
+    }
+    ntlist[ntoff[bs] + v] = tlist[toff[bs] + k];
+  }
+  const int A = arity[s], rb = row0[s];
+  for (int q = threadIdx.x; q < nelem * A; q += blockDim.x) {
+    const int i = q / A, r = q - i * A;
+    const int64_t at = (int64_t)(rb + r) * set_size + start + i;
+    const int o = loc[at];
+    if (o < 0 || o >= nu) {
+      atomicExch(bad, 1);
+      continue;
+    }
+    nloc[at] = pm[o];
+  }
+}
+
 static int rg_grid(int64_t n) {
   return std::max(1, std::min(op2b_div_up(std::max<int64_t>(n, 1), kRgThreads), sm_count() * 8));
 }
@@ -347,6 +443,7 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
   P->nstage = nstage;
   P->loc_rows = loc_rows;
   P->max_count.assign(nstage, 0);
+  P->arity.assign(stage_arity, stage_arity + nstage);
   std::vector<void *> temps;
   uint64_t inc = 0;
   auto fail = [&](int rc) {
@@ -584,6 +681,108 @@ int op2b_region_plan_array(uint64_t plan, int32_t which, uint64_t *dptr, int64_t
   *dptr = reinterpret_cast<uint64_t>(ptrs[which]);
   if (count) *count = counts[which];
   return OP2B_OK;
+}
+
+int op2b_region_plan_bank_slots(uint64_t plan, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  RegionPlan *P = reinterpret_cast<RegionPlan *>(plan);
+  if (!P) return set_error(OP2B_ERR_ARG, "null region plan");
+  if (P->bank_slots || P->nblocks == 0 || P->nstage == 0) {
+    P->bank_slots = true;
+    return OP2B_OK;
+  }
+  cudaStream_t s = stream_of(stream);
+  const int nb = P->nblocks, ns = P->nstage, n = P->set_size;
+  const int64_t nbs = (int64_t)nb * ns;
+  int maxc = 1;
+  for (int q = 0; q < ns; ++q) maxc = std::max(maxc, P->max_count[q]);
+  std::vector<int32_t> h_row0(ns);
+  for (int q = 0, r = 0; q < ns; ++q) {
+    h_row0[q] = r;
+    r += P->arity[q];
+  }
+  std::vector<void *> temps;
+  auto alloc = [&](void **ptr, size_t bytes, bool temp) -> int {
+    int rc = dev_alloc(ptr, bytes, s);
+    if (rc == OP2B_OK && temp) temps.push_back(*ptr);
+    return rc;
+  };
+  auto done = [&](int rc) {
+    for (void *t : temps) dev_free(t, s);
+    return rc;
+  };
+#define BS_TRY(x) do { int _rc = (x); if (_rc) return done(_rc); } while (0)
+#define BS_CUDA(x) BS_TRY(check_cuda((x), #x))
+  int32_t *d_ar = nullptr, *d_row0 = nullptr, *ncnt = nullptr, *ntoff = nullptr, *ntlist = nullptr,
+          *bad = nullptr;
+  int16_t *perm = nullptr, *nloc = nullptr;
+  BS_TRY(alloc((void **)&d_ar, sizeof(int32_t) * ns, true));
+  BS_TRY(alloc((void **)&d_row0, sizeof(int32_t) * ns, true));
+  BS_CUDA(cudaMemcpyAsync(d_ar, P->arity.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, s));
+  BS_CUDA(cudaMemcpyAsync(d_row0, h_row0.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, s));
+  BS_TRY(alloc((void **)&perm, sizeof(int16_t) * (size_t)nbs * maxc, true));
+  BS_TRY(alloc((void **)&ncnt, sizeof(int32_t) * (size_t)nbs, false));
+  BS_CUDA(cudaFuncSetAttribute(rg_slot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, maxc));
+  rg_slot_kernel<<<dim3(nb, ns), 32, maxc, s>>>(ns, n, P->boff, P->tcnt, P->loc, d_ar, d_row0, maxc,
+                                                perm, ncnt);
+  BS_CUDA(cudaGetLastError());
+  std::vector<int32_t> h_cnt((size_t)nbs);
+  BS_CUDA(cudaMemcpyAsync(h_cnt.data(), ncnt, sizeof(int32_t) * h_cnt.size(), cudaMemcpyDeviceToHost, s));
+  BS_CUDA(cudaStreamSynchronize(s));
+  std::vector<int32_t> h_off(h_cnt.size() + 1);
+  std::vector<int32_t> mc(ns, 0);
+  int64_t tot = 0;
+  for (size_t i = 0; i < h_cnt.size(); ++i) {
+    h_off[i] = (int32_t)tot;
+    tot += h_cnt[i];
+    mc[i % ns] = std::max(mc[i % ns], h_cnt[i]);
+  }
+  if (tot > INT_MAX) {
+    dev_free(ncnt, s);
+    return done(set_error(OP2B_ERR_ARG, "region plan: %lld staged slots", (long long)tot));
+  }
+  for (size_t i = 0; i < h_cnt.size(); ++i)
+    if (h_cnt[i] < 0) {
+      dev_free(ncnt, s);
+      return done(set_error(OP2B_ERR_ARG, "region plan: block %zu needs more than 32768 slots",
+                            i / ns));
+    }
+  h_off[h_cnt.size()] = (int32_t)tot;
+  BS_TRY(alloc((void **)&ntoff, sizeof(int32_t) * h_off.size(), false));
+  BS_CUDA(cudaMemcpyAsync(ntoff, h_off.data(), sizeof(int32_t) * h_off.size(), cudaMemcpyHostToDevice, s));
+  BS_TRY(alloc((void **)&ntlist, sizeof(int32_t) * (size_t)std::max<int64_t>(tot, 1), false));
+  BS_CUDA(cudaMemsetAsync(ntlist, 0xff, sizeof(int32_t) * (size_t)std::max<int64_t>(tot, 1), s));
+  BS_TRY(alloc((void **)&nloc, sizeof(int16_t) * (size_t)P->loc_rows * std::max(n, 1), false));
+  BS_TRY(alloc((void **)&bad, sizeof(int32_t), true));
+  BS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
+  rg_slot_apply_kernel<<<dim3(nb, ns), kRgThreads, 0, s>>>(ns, n, P->boff, P->tcnt, P->toff, P->tlist,
+                                                          ncnt, ntoff, ntlist, P->loc, nloc, d_ar,
+                                                          d_row0, maxc, perm, bad);
+  BS_CUDA(cudaGetLastError());
+  int32_t h_bad = 0;
+  BS_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  BS_CUDA(cudaStreamSynchronize(s));
+  if (h_bad) {
+    dev_free(ncnt, s);
+    dev_free(ntoff, s);
+    dev_free(ntlist, s);
+    dev_free(nloc, s);
+    return done(set_error(OP2B_ERR_STATE, "region plan: slot renumbering out of range"));
+  }
+  temps.push_back(P->tcnt);
+  temps.push_back(P->toff);
+  temps.push_back(P->tlist);
+  temps.push_back(P->loc);
+  P->tcnt = ncnt;
+  P->toff = ntoff;
+  P->tlist = ntlist;
+  P->loc = nloc;
+  P->tlist_len = tot;
+  P->max_count = mc;
+  P->bank_slots = true;
+#undef BS_TRY
+#undef BS_CUDA
+  return done(OP2B_OK);
 }
 
 int op2b_region_plan_free(uint64_t plan) {

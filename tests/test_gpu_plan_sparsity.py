@@ -214,11 +214,12 @@ def test_sparsity_empty_rows(op2):
 
 
 # ------------------------------------------------- locality partition
-def _region_check(op2, n, grow, stages, part, rs, inc=None):
+def _region_check(op2, n, grow, stages, part, rs, inc=None, banks=False):
     """Device locality partition (op2b_region_plan_build) equals the numpy
     restatement (oracle/region.py) array for array; grow / stages are
     (values [n][arity], target size); inc flags the staged Maps the thread
-    colours separate."""
+    colours separate; banks applies the bank-aware slot numbering
+    (op2b_region_plan_bank_slots) on both sides."""
     from oracle import region
     from pyop2_b200 import b200
     it = op2.Set(n)
@@ -229,8 +230,11 @@ def _region_check(op2, n, grow, stages, part, rs, inc=None):
         if key not in mk:
             mk[key] = op2.Map(it, op2.Set(ntg), vals.shape[1], vals)
         return mk[key]
-    rp = b200.RegionPlan(n, part, rs, dmap(*grow), [dmap(v, t) for v, t in stages], inc)
+    rp = b200.RegionPlan(n, part, rs, dmap(*grow), [dmap(v, t) for v, t in stages], inc,
+                         bank_slots=banks)
     want = region.region_plan(grow[0], grow[1], [v for v, _ in stages], part, rs, inc)
+    if banks:
+        want = region.bank_slots(want, [v.shape[1] for v, _ in stages])
     for name in ("order", "boff", "tlist", "toff", "tcnt", "thrcol", "nthrcol"):
         np.testing.assert_array_equal(rp.host_array(name), want[name], err_msg=name)
     np.testing.assert_array_equal(rp.host_array("loc"), want["loc"].ravel())
@@ -245,15 +249,19 @@ def _region_check(op2, n, grow, stages, part, rs, inc=None):
     return rp, want
 
 
-@pytest.mark.parametrize("nx,ny,seed,part,rs", [(60, 30, 0, 1024, 512), (40, 17, 3, 256, 64),
-                                                (7, 5, 1, 32, 1000)])
-def test_region_plan_airfoil_matches_oracle(op2, nx, ny, seed, part, rs):
+@pytest.mark.parametrize("nx,ny,seed,part,rs,banks", [(60, 30, 0, 1024, 512, False),
+                                                      (40, 17, 3, 256, 64, False),
+                                                      (7, 5, 1, 32, 1000, False),
+                                                      (60, 30, 0, 384, 192, True),
+                                                      (7, 5, 1, 32, 1000, True)])
+def test_region_plan_airfoil_matches_oracle(op2, nx, ny, seed, part, rs, banks):
     from pyop2_b200.workloads import meshes
     g = meshes.airfoil_grid(nx, ny, seed)
     pecell = np.asarray(g.pecell, np.int32).reshape(-1, 2)
     pedge = np.asarray(g.pedge, np.int32).reshape(-1, 2)
     rp, want = _region_check(op2, g.nedges, (pecell, g.ncells),
-                             [(pecell, g.ncells), (pedge, g.nnodes)], part, rs, [True, False])
+                             [(pecell, g.ncells), (pedge, g.nnodes)], part, rs, [True, False],
+                             banks)
     assert rp.max_nthrcol == want["nthrcol"].max()
     if nx == 60:
         # compact regions: far fewer distinct cells per block than elements

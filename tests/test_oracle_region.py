@@ -89,3 +89,34 @@ def test_single_seed_and_empty():
     e = np.zeros((0, 2), np.int32)
     R = region.region_plan(e, 4, [e], 64, 64)
     assert len(R["boff"]) == 1 and R["order"].size == 0
+
+
+def test_bank_slots_keep_targets_and_cut_conflicts():
+    """The bank-aware slot numbering (restated in oracle/region.py, the
+    checker of op2b_region_plan_bank_slots) keeps every (position, row)'s
+    target, marks padding slots -1, and removes a part of the bank-group conflicts of
+    the staged-row reads on the airfoil edges."""
+    g = meshes.airfoil_grid(60, 30, 0)
+    pecell = np.asarray(g.pecell, np.int64).reshape(-1, 2)
+    pedge = np.asarray(g.pedge, np.int64).reshape(-1, 2)
+    stages = [pecell, pedge]
+    R = region.region_plan(pecell, g.ncells, stages, 384, 192, [True, False])
+    B = region.bank_slots(R, [2, 2])
+    ns, n = 2, g.nedges
+    for k in ("order", "boff", "thrcol", "nthrcol"):
+        np.testing.assert_array_equal(B[k], R[k])
+    for b in range(len(R["boff"]) - 1):
+        seg = slice(R["boff"][b], R["boff"][b + 1])
+        for s, v in enumerate(stages):
+            lo, cnt = B["toff"][b * ns + s], B["tcnt"][b * ns + s]
+            tl = B["tlist"][lo:lo + cnt]
+            real = tl[tl >= 0]
+            assert sorted(real.tolist()) == sorted(set(v[R["order"][seg]].ravel().tolist()))
+            for r in range(2):
+                np.testing.assert_array_equal(tl[B["loc"][2 * s + r, seg]], v[R["order"][seg], r])
+            # at most one residue class longer than the others by the balance rule
+            assert cnt <= 8 * (-(-R["tcnt"][b * ns + s] // 8)) + 8 * 4
+    before = region.bank_conflicts(R, [2, 2], 2)
+    after = region.bank_conflicts(B, [2, 2], 2)
+    assert after < 0.8 * before, (before, after)
+    assert n == R["loc"].shape[1]
