@@ -274,6 +274,11 @@ def loop_phases(sizes, launch, exchanges=(), reductions=(), direct=False, exec_h
     yield
     for p in pending:
         p.wait()
+    if not reductions:
+        # nothing is reduced between the owned elements and the execute
+        # halo: one launch covers both
+        launch(core, exec_size if exec_halo else size)
+        return
     launch(core, size)
     red = [r.begin() for r in reductions]
     yield

@@ -90,6 +90,10 @@ def test_loop_phase_order():
     halo.run(halo.loop_phases((2, 5, 7, 9), launch, [X("x")], [X("g")], exec_halo=True))
     assert seen == ["x begin", "run 0-2", "x end", "run 2-5", "g begin", "run 5-7", "g end"]
     seen.clear()
+    # without a reduction the owned rest and the execute halo are one launch
+    halo.run(halo.loop_phases((2, 5, 7, 9), launch, [X("x")], [], exec_halo=True))
+    assert seen == ["x begin", "run 0-2", "x end", "run 2-7"]
+    seen.clear()
     halo.run(halo.loop_phases((2, 5, 7, 9), launch, [X("x")], [X("g")], direct=True))
     assert seen == ["run 0-5", "g begin", "g end"]
 
