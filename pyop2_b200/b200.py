@@ -1027,18 +1027,20 @@ def gather_order(iterset, maps, region, omap):
     return order
 
 
-def region_plan(iterset, maps, region):
-    """The cached locality partition of a staged loop."""
+def region_plan(iterset, maps, region, size=None):
+    """The cached locality partition of a staged loop (over the set's first
+    ``size`` elements, default all)."""
+    n = iterset.size if size is None else int(size)
     ps = region["part_size"]
     rs = int(cfg.cfg['region_size']) or max(1, ps // 2)
     reps = [maps[k] for k in region["stage_maps"]]
     grow = reps[region["grow"]]
     inc = [st in region["inc_stages"] for st in range(len(reps))]
     banks = bool(cfg.cfg['staged_bank_slots'])
-    key = (iterset.size, ps, rs, id(grow), tuple(id(m) for m in reps), tuple(inc), banks)
+    key = (n, ps, rs, id(grow), tuple(id(m) for m in reps), tuple(inc), banks)
     plan = _REGION_CACHE.get(key)
     if plan is None:
-        plan = _REGION_CACHE[key] = RegionPlan(iterset.size, ps, rs, grow, reps, inc, banks)
+        plan = _REGION_CACHE[key] = RegionPlan(n, ps, rs, grow, reps, inc, banks)
     return plan
 
 
@@ -1242,12 +1244,13 @@ def mat_slot_values(specs, maps, mats, rel=False):
 
 
 def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=None,
-              inc_mode=None, min_blocks=None):
+              inc_mode=None, min_blocks=None, size=None):
     """Static description of a par_loop: the LoopSpec of its stub plus the
     unique Dats/Maps/Mats/Globals, the INC staging pairs and the plan race
     groups.  Touches no device memory (used to generate and test stubs)."""
     it = loop.it_space
     iterset = it.iterset
+    nsz = iterset.size if size is None else int(size)
     extents = it.extents
     args = loop.args
     dats, dat_slot = [], {}
@@ -1384,7 +1387,7 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
     req = inc_mode or cfg.cfg['inc_mode']
     gather, gather_region = None, None
     if (owner is None and indirect and req == 'gather'
-            and iterset.size >= int(cfg.cfg['staged_min_size'])):
+            and nsz >= int(cfg.cfg['staged_min_size'])):
         gather = codegen.owner_plan(spec, None)
         if gather is not None and gather["kind"] != "dat":
             gather = None
@@ -1406,7 +1409,7 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
         gather_region = R
         indirect = False
     elif (indirect and req in ('staged', 'gather') and codegen.staged_capable(spec)
-          and iterset.size >= int(cfg.cfg['staged_min_size'])):
+          and nsz >= int(cfg.cfg['staged_min_size'])):
         spec.mode = "staged"
         spec.region = R = _region_layout(specs, maps)
         if block_size is None:
@@ -1446,7 +1449,7 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
     if spec.mode == "direct":
         spec.direct_unroll = max(1, int(cfg.cfg['direct_unroll']))
     if (spec.mode == "atomic" and cfg.cfg['read_replicas'] and cfg.cfg['gathered_replicas']
-            and iterset.size >= int(cfg.cfg['replica_min_size'])):
+            and nsz >= int(cfg.cfg['replica_min_size'])):
         # READ-only Dats read through one Map: a copy gathered per element
         # (no Map read, no dependent gather) while it fits the byte cap
         cap = float(cfg.cfg['gathered_max_gb']) * 1e9
@@ -1540,8 +1543,10 @@ class _BoundLoop(object):
     """Everything about a par_loop that does not change between calls with
     the same objects: generated stub, plan, parameter block."""
 
-    def __init__(self, loop, inc_mode=None, owner_mode=None):
-        info = loop_spec(loop, inc_mode=inc_mode, owner_mode=owner_mode)
+    def __init__(self, loop, inc_mode=None, owner_mode=None, nelem=None):
+        # nelem: bind to the set's first nelem elements only (the core of a
+        # partitioned set, run in the staged form)
+        info = loop_spec(loop, inc_mode=inc_mode, owner_mode=owner_mode, size=nelem)
         spec = info['spec']
         specs = info['specs']
         dats, maps, mats, gbls = info['dats'], info['maps'], info['mats'], info['gbls']
@@ -1549,10 +1554,12 @@ class _BoundLoop(object):
         iterset = info['iterset']
         args = loop.args
         self.spec = spec
+        self.nelem = iterset.size if nelem is None else int(nelem)
+        self.core_loop = None
         if spec.mode == "staged" and cfg.cfg['staged_tl_regs']:
             # target ids held in registers: as many per thread as the
             # partition's largest block needs
-            rp0 = region_plan(iterset, maps, spec.region)
+            rp0 = region_plan(iterset, maps, spec.region, self.nelem)
             bs0 = spec.block_size
             spec.region["tl_regs"] = [max(1, -(-int(c) // bs0)) for c in rp0.max_count]
         self.module = _get_module(spec)
@@ -1568,7 +1575,7 @@ class _BoundLoop(object):
             if a._is_dat:
                 self.dat_access.setdefault(id(a.data), []).append(s.access)
                 ok = (s.kind == "direct" and s.access == "WRITE"
-                      and a.data.dataset.total_size == iterset.size)
+                      and a.data.dataset.total_size == self.nelem)
                 direct_write[id(a.data)] = direct_write.get(id(a.data), True) and ok
         # Dats the loop only writes, row by row over the whole set: a fresh
         # device copy needs no upload of the host values first
@@ -1637,7 +1644,7 @@ class _BoundLoop(object):
             rep = gathered_replica(dats[j], maps[k])
             vals["d%d" % j] = rep.rows.ptr
             self.replicas.append((j, dats[j], rep))
-        if cfg.cfg['read_replicas'] and iterset.size >= int(cfg.cfg['replica_min_size']):
+        if cfg.cfg['read_replicas'] and self.nelem >= int(cfg.cfg['replica_min_size']):
             for j, k in replica_candidates(spec, specs, dats, maps):
                 if (j, k) in spec.gathered:
                     continue
@@ -1645,14 +1652,14 @@ class _BoundLoop(object):
                 vals["m%d" % k] = rep.map.ptr
                 self.replicas.append((j, dats[j], rep))
         self.vals = vals
-        n = iterset.size
+        n = self.nelem
         self.range_end = n
         self.launch_smem = 0
         if indirect:
             self.grid = 0
             self.max_grid = self.plan.max_blocks_per_color
         elif spec.mode == "staged":
-            rp = region_plan(iterset, maps, spec.region)
+            rp = region_plan(iterset, maps, spec.region, self.nelem)
             self.region_plan = rp
             for name in _REGION_ARRAYS:
                 vals["rg_" + name] = rp.dptr[name]
@@ -1767,7 +1774,7 @@ class _BoundLoop(object):
         self._gptr = [None] * len(self._gbl)
         self._written = [d for d in self.dats if any(m != "READ" for m in self.dat_access[id(d)])]
         self._reducing = [k for k, (_, _, red) in enumerate(self._gbl) if red]
-        n = self.iterset.size
+        n = self.nelem
         self._buf = C.create_string_buffer(self.layout.pack(n, 0, self.range_end, vals),
                                            self.layout.nbytes)
 
@@ -1810,7 +1817,7 @@ class _BoundLoop(object):
         mod = self.module
         if self.consts:
             _sync_consts(mod, self.consts)
-        n = self.iterset.size
+        n = self.nelem
         if rng is not None:
             if self.spec.mode not in ("direct", "atomic") or rng[0] < 0 or rng[1] > \
                     self.iterset.total_size:
@@ -2105,7 +2112,11 @@ def _loop_phases(bl, loop, args):
     exec_halo = any(a._is_indirect_and_not_read or a._is_mat for a in args)
 
     def launch(start, end):
-        if end > start:
+        if end <= start:
+            return
+        if start == 0 and end == it.core_size and bl.core_loop is not None:
+            bl.core_loop.run(loop)
+        else:
             bl.run(loop, (start, end))
     yield from halo_mod.loop_phases(it.sizes, launch, exchanges, reductions, direct, exec_halo)
     for a in args:
@@ -2126,6 +2137,16 @@ def _bind(loop, iterset):
             raise NotImplementedError("par_loop %s over a partitioned set needs the %s form, "
                                       "which runs whole sets only" % (bl.spec.kernel_name,
                                                                       bl.spec.mode))
+        core = iterset.core_size
+        if bl.spec.mode == "atomic" and core > 0 and cfg.cfg['inc_mode'] in ('staged', 'gather'):
+            # the core (most of a rank's elements) in the staged form over a
+            # locality partition of its own; the other ranges stay atomic
+            try:
+                cb = _BoundLoop(loop, nelem=core)
+            except _StagedTooLarge:
+                cb = None
+            if cb is not None and cb.spec.mode == "staged":
+                bl.core_loop = cb
         return bl
     try:
         return _BoundLoop(loop)

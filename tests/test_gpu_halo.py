@@ -89,10 +89,15 @@ class _Recorder(object):
         self.calls.append((kernel, iterset, args))
 
 
-@pytest.mark.parametrize("nranks", [2, 3])
-def test_partitioned_airfoil_matches_oracle(op2, nranks):
+@pytest.mark.parametrize("nranks,staged_core", [(2, False), (3, False), (2, True)])
+def test_partitioned_airfoil_matches_oracle(op2, nranks, staged_core):
+    """staged_core: the core ranges of the INC loops in the staged form (a
+    locality partition of each rank's core), the rest atomic."""
     from pyop2_b200 import b200, halo
+    from pyop2_b200 import configuration as cfg
     from pyop2_b200.workloads import airfoil, meshes
+    if staged_core:
+        cfg.configure(staged_min_size=0)
     sys.path.insert(0, ROOT)
     from oracle import seq
     g = meshes.airfoil_grid(60, 30, 3)
@@ -126,9 +131,15 @@ def test_partitioned_airfoil_matches_oracle(op2, nranks):
         assert rel_err(q, O.p_q.data) < TOL
         for a, b in zip(rms, ref_rms):
             assert abs(a - b) <= TOL * abs(b)
-        # the partitioned loops ran in the atomic form, in element ranges
-        assert all(bl.spec.mode in ("direct", "atomic") for bl in b200.ParLoop._bound_cache.values()
-                   if bl.partitioned)
+        # the partitioned loops ran in the atomic form, in element ranges,
+        # with the core in the staged form where asked
+        part = [bl for bl in b200.ParLoop._bound_cache.values() if bl.partitioned]
+        assert all(bl.spec.mode in ("direct", "atomic") for bl in part)
+        cores = [bl.core_loop for bl in part if bl.core_loop is not None]
+        if staged_core:
+            assert any(c.spec.kernel_name == "res_calc" and c.spec.mode == "staged" for c in cores)
+        else:
+            assert not cores
     finally:
         _clear_consts()
 
