@@ -242,3 +242,39 @@ def test_partitioned_p1_rhs_matches_oracle(op2):
         got[ls.l2g[:ls.sizes[1]]] = b.data_ro.ravel()[:ls.sizes[1]]
         assert abs(t.data[0] - O.b.data.sum()) <= TOL * abs(O.b.data).sum()
     assert rel_err(got, O.b.data) < TOL
+
+
+@pytest.mark.parametrize("mode,want", [("MIN", 1.0), ("MAX", 8.0), ("INC", 36.0)])
+def test_partitioned_global_reductions_across_ranks(op2, mode, want):
+    """Global MIN / MAX / INC over the owned elements of a set split across
+    two ranks on one GPU: every rank holds the reduction over both ranks'
+    owned elements (pyop2/base.py:216-249), and the execute halo's values
+    (here the largest and smallest of all) never reach it."""
+    from pyop2_b200 import b200, halo
+    comms = halo.LocalGroup(2).comms()
+    # rank 0 owns values 1..4, rank 1 owns 5..8; each holds an execute-halo
+    # copy of one peer element with a value outside [1, 8]
+    k = op2.Kernel("void r(double *o, double *g, double *v) { o[0] += 0.0; %s }" % {
+        "MIN": "if (v[0] < g[0]) g[0] = v[0];", "MAX": "if (v[0] > g[0]) g[0] = v[0];",
+        "INC": "g[0] += v[0];"}[mode], "r")
+    ranks = []
+    for r in range(2):
+        own = np.arange(1.0, 5.0) + 4 * r
+        vals = np.concatenate([own, [100.0 if mode != "MIN" else -100.0]])
+        sends = [np.zeros(0, np.int32), np.array([3], np.int32)] if r == 0 else \
+            [np.array([0], np.int32), np.zeros(0, np.int32)]
+        recvs = [np.zeros(0, np.int32), np.array([4], np.int32)] if r == 0 else \
+            [np.array([4], np.int32), np.zeros(0, np.int32)]
+        s = op2.Set([2, 4, 5, 5], 1, "gr%d" % r, halo=op2.Halo(sends, recvs, comm=comms[r]))
+        t = op2.Set(5, 1, "gt%d" % r)
+        m = op2.Map(s, t, 1, np.arange(5, dtype=np.int32), "gm%d" % r)
+        out = op2.Dat(t, np.zeros(5), np.float64, "go%d" % r)
+        v = op2.Dat(s, vals, np.float64, "gv%d" % r)
+        v.needs_halo_update = False
+        init = {"MIN": 1e30, "MAX": -1e30, "INC": 0.0}[mode]
+        ranks.append((s, m, out, v, op2.Global(1, init, np.float64, "g%d" % r)))
+    acc = {"MIN": op2.MIN, "MAX": op2.MAX, "INC": op2.INC}[mode]
+    halo.run_lockstep([b200.par_loop_phases(k, s, out(m[0], op2.INC), g(acc), v(op2.IdentityMap, op2.READ))
+                       for s, m, out, v, g in ranks])
+    for s, m, out, v, g in ranks:
+        assert g.data[0] == want
