@@ -292,3 +292,24 @@ def test_partitioned_airfoil_two_gloo_ranks_matches_oracle():
     assert np.abs(q - ref_q).max() <= TOL * np.abs(ref_q).max()
     for p in procs:
         assert p.exitcode == 0
+
+
+def test_halo_declaration_checks():
+    """op2.Halo takes the backend's communicator by default (one rank here)
+    and checks its lists as the reference does (pyop2/base.py:424-447)."""
+    from pyop2_b200 import _lib, backends, base
+    if backends.get_backend() == "pyop2_b200.void":
+        backends.set_backend("b200")
+    _lib.load()
+    h = base.Halo([[]], [[]])
+    assert h.comm.size == 1 and h.comm.rank == 0
+    with pytest.raises(AssertionError):
+        base.Halo([[], []], [[]])                    # two sends on one rank
+    with pytest.raises(AssertionError):
+        base.Halo([[0]], [[]])                       # a self-send
+    comms = halo.LocalGroup(2).comms()
+    h1 = base.Halo([[1, 2], []], [[5], []], comm=comms[1])
+    s = base.Set([2, 3, 4, 6], 1, "checked", halo=h1)
+    assert s.halo is h1 and s.sizes == (2, 3, 4, 6)
+    with pytest.raises(AssertionError):
+        base.Set([2, 3, 4, 6], 1, "bad", halo=base.Halo([[3], []], [[5], []], comm=comms[1]))
