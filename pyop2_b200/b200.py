@@ -1420,6 +1420,8 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
         R["ept"] = (ps + bs - 1) // bs
         if int(cfg.cfg['staged_pair']) == 2:
             R["pair"] = 2
+        if cfg.cfg['staged_bank_slots']:
+            R["padded"] = True       # padding slots (target -1) to skip
         indirect = False   # one launch over the locality partition's blocks
     elif indirect and (inc_mode or cfg.cfg['inc_mode']) == 'lma' and codegen.lma_capable(spec):
         spec.mode = "lma"

@@ -748,7 +748,8 @@ def _staged_copy_rows(R, used, bs, ind, dst, n, tl):
             continue
         L.append("%sfor (int r = threadIdx.x; r < %s; r += %d) {" % (ind, n % st, bs))
         L.append("%s  const op2b_i64 g = %s[r];" % (ind, tl % st))
-        L.append("%s  if (g < 0) continue;   // padding slot" % ind)
+        if R.get("padded"):
+            L.append("%s  if (g < 0) continue;   // padding slot" % ind)
         for q, slot, t, c in pairs:
             nb = c * _CSIZE[t]
             if nb % 4 == 0:
@@ -769,7 +770,8 @@ def _staged_copy_rows_regs(R, used, bs, ind, KR):
         if not pairs:
             continue
         for k in range(KR[st]):
-            L.append("%sif (threadIdx.x + %d < n_s%d && tg%d_%d >= 0) {" % (ind, k * bs, st, st, k))
+            pad = " && tg%d_%d >= 0" % (st, k) if R.get("padded") else ""
+            L.append("%sif (threadIdx.x + %d < n_s%d%s) {" % (ind, k * bs, st, pad))
             L.append("%s  const int r = threadIdx.x + %d;" % (ind, k * bs))
             L.append("%s  const op2b_i64 g = tg%d_%d;" % (ind, st, k))
             for q, slot, t, c in pairs:
@@ -790,7 +792,8 @@ def _staged_flush_regs(R, bs, ind, KR):
     L = []
     for q, (slot, st, ctype, cdim) in enumerate(R["inc_pairs"]):
         for k in range(KR[st]):
-            L.append("%sif (threadIdx.x + %d < n_s%d && tg%d_%d >= 0) {" % (ind, k * bs, st, st, k))
+            pad = " && tg%d_%d >= 0" % (st, k) if R.get("padded") else ""
+            L.append("%sif (threadIdx.x + %d < n_s%d%s) {" % (ind, k * bs, st, pad))
             L.append("%s  __align__(16) %s cur[%d]; op2b_srow_load(cur, acc%d, threadIdx.x + %d);"
                      % (ind, ctype, cdim, q, k * bs))
             L.append("%s  op2b_atomic_row(p.d%d + (op2b_i64)tg%d_%d * %d, cur);" % (ind, slot, st, k, cdim))
@@ -981,9 +984,9 @@ def _staged_flush(R, bs, ind):
         L.append("%sfor (int t = threadIdx.x; t < n_s%d * %d; t += %d) {" % (ind, st, cdim, bs))
         L.append("%s  const int r = t / %d, k = t - r * %d;" % (ind, cdim, cdim))
         L.append("%s  const op2b_i64 g = tl_s%d[r];" % (ind, st))
-        L.append("%s  if (g >= 0)   // not a padding slot" % ind)
-        L.append("%s    op2b_atomic_add(p.d%d + g * %d + k, acc%d[op2b_srow_index<%s, %d>(r, k)]);"
-                 % (ind, slot, cdim, q, ctype, cdim))
+        guard = "if (g >= 0) " if R.get("padded") else ""   # padding slots
+        L.append("%s  %sop2b_atomic_add(p.d%d + g * %d + k, acc%d[op2b_srow_index<%s, %d>(r, k)]);"
+                 % (ind, guard, slot, cdim, q, ctype, cdim))
         L.append("%s}" % ind)
     return L
 

@@ -445,14 +445,17 @@ def test_two_phase_kahan_precision_form(op2):
                                                                   replica_min_size=0),
                                   dict(staged_pair=2), dict(staged_pair=2, partition_size=512),
                                   dict(read_replicas=True, replica_min_size=0,
-                                       gathered_replicas=True)])
+                                       gathered_replicas=True),
+                                  dict(staged_bank_slots=True),
+                                  dict(staged_bank_slots=True, staged_tl_regs=True)])
 def test_airfoil_chain_launch_options_match_oracle(op2, opts):
     """The launch-level options on the staged airfoil chain: programmatic
     dependent launch (every stub waits for its predecessor), multiply-add
     contraction in INC-form loops, target ids in registers, READ replicas on
     small sets, two elements per thread in the staged passes (odd and even
-    pass counts), element-gathered READ copies; q and rms within 1e-12 of
-    the oracle after three iterations."""
+    pass counts), element-gathered READ copies, bank-aware slot numbering
+    (padding slots skipped by the copy and the flush); q and rms within
+    1e-12 of the oracle after three iterations."""
     from pyop2_b200 import b200
     from pyop2_b200 import configuration as cfg
     from pyop2_b200._lib import call
