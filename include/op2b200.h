@@ -99,6 +99,10 @@ int op2b_device_sync(void);
 int op2b_event_create(uint64_t *event);
 int op2b_event_destroy(uint64_t event);
 int op2b_event_record(uint64_t event, uint64_t stream);
+/* As op2b_event_record, but while the stream is being captured into a CUDA
+ * graph the record becomes a node of the graph, so every replay records the
+ * event (device timestamps inside a replayed graph). */
+int op2b_event_record_node(uint64_t event, uint64_t stream);
 int op2b_event_sync(uint64_t event);
 /* Non-blocking: *done = 1 if all work before the event's record has
  * completed, else 0 (cudaEventQuery). */

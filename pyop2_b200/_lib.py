@@ -45,6 +45,7 @@ _SIGS = {
     "op2b_event_create": [u64p],
     "op2b_event_destroy": [u64],
     "op2b_event_record": [u64, u64],
+    "op2b_event_record_node": [u64, u64],
     "op2b_event_sync": [u64],
     "op2b_event_query": [u64, i32p],
     "op2b_event_elapsed_ms": [u64, u64, C.POINTER(C.c_float)],

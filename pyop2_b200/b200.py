@@ -2256,8 +2256,10 @@ class Event(object):
         call("op2b_event_create", C.byref(h))
         self.handle = h.value
 
-    def record(self):
-        call("op2b_event_record", self.handle, 0)
+    def record(self, node=False):
+        """Record on the op2 stream; ``node``: inside b200.capture() the
+        record becomes a node of the graph, timing every replay."""
+        call("op2b_event_record_node" if node else "op2b_event_record", self.handle, 0)
         return self
 
     def synchronize(self):

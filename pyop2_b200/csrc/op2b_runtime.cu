@@ -383,6 +383,13 @@ int op2b_event_record(uint64_t event, uint64_t stream) {
   return OP2B_OK;
 }
 
+int op2b_event_record_node(uint64_t event, uint64_t stream) {
+  OP2B_REQUIRE_INIT();
+  OP2B_CUDA(cudaEventRecordWithFlags(reinterpret_cast<cudaEvent_t>(event), stream_of(stream),
+                                     cudaEventRecordExternal));
+  return OP2B_OK;
+}
+
 int op2b_event_sync(uint64_t event) {
   OP2B_REQUIRE_INIT();
   OP2B_CUDA(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(event)));
