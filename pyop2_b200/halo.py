@@ -195,11 +195,16 @@ class TorchComm(object):
         ops += [dist.P2POp(dist.irecv, b.tensor(), peer, self.group, tag) for peer, b in recvs]
         with self._ctx():
             works = dist.batch_isend_irecv(ops) if ops else []
+        # NCCL reads the send buffers on its own stream: they stay referenced
+        # until the issuing stream has waited for the transfers, so that a
+        # stream-ordered free cannot hand their memory to later work first
+        held = [b for _, b in sends] + [b for _, b in recvs]
 
         def finish():
             with self._ctx():
                 for w in works:
                     w.wait()
+            del held[:]
         return Request(finish)
 
     def allreduce(self, buf, op):
@@ -208,10 +213,12 @@ class TorchComm(object):
         t = buf.tensor()
         with self._ctx():
             w = dist.all_reduce(t, op=rop, group=self.group, async_op=True)
+        held = [buf]
 
         def finish():
             with self._ctx():
                 w.wait()
+            del held[:]
         return Request(finish)
 
 

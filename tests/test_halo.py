@@ -76,6 +76,63 @@ def test_self_comm():
         c.exchange([(1, halo.HostBuffer(v))], [])
 
 
+class _FakeWork(object):
+    def __init__(self, log):
+        self.log = log
+
+    def wait(self):
+        self.log.append("wait")
+
+
+class _FakeDist(object):
+    """The parts of torch.distributed TorchComm calls, recording the order."""
+
+    class ReduceOp(object):
+        SUM, MIN, MAX = "sum", "min", "max"
+
+    def __init__(self):
+        self.log = []
+
+    def isend(self, *a):
+        pass
+
+    irecv = isend
+
+    def P2POp(self, op, tensor, peer, group, tag):
+        return (op, tensor, peer)
+
+    def batch_isend_irecv(self, ops):
+        self.log.append("issue %d" % len(ops))
+        return [_FakeWork(self.log)]
+
+    def all_reduce(self, t, op, group, async_op):
+        self.log.append("allreduce")
+        return _FakeWork(self.log)
+
+
+def test_torch_comm_holds_buffers_until_waited():
+    # NCCL reads and writes the buffers on its own stream: the communicator
+    # must keep them referenced until its wait has run
+    import gc
+    import weakref
+
+    comm = halo.TorchComm.__new__(halo.TorchComm)
+    comm.dist, comm.group, comm.stream = _FakeDist(), None, None
+    comm.rank, comm.size, comm._nx = 0, 2, 0
+    send, recv, red = (halo.HostBuffer(np.zeros(4)) for _ in range(3))
+    refs = [weakref.ref(b) for b in (send, recv, red)]
+    req = comm.exchange([(1, send)], [(1, recv)])
+    rreq = comm.allreduce(red, "sum")
+    del send, recv, red
+    gc.collect()
+    assert all(r() is not None for r in refs)
+    req.wait()
+    rreq.wait()
+    gc.collect()
+    assert all(r() is None for r in refs)
+    assert comm.dist.log == ["issue 2", "allreduce", "wait", "wait"]
+
+
 def test_loop_phase_order():
     seen = []
 
