@@ -59,6 +59,7 @@ struct RegionPlan {
 };
 
 constexpr int kRgThreads = 256;
+constexpr int kRgStageThreads = 128;     // staging: more CTAs per SM than 256-thread ones
 constexpr int kRgMaxKeys = 16384;          // part_size * arity per staged Map
 constexpr uint64_t kUnset = ~0ull;
 constexpr int kRgLevelChunk = 8;           // BFS levels between two looks at progress
@@ -100,23 +101,39 @@ __global__ void rg_push_kernel(int n, const int32_t *__restrict__ map, int arity
   }
 }
 
-// Unlabelled elements take the smallest key among their targets, one level
-// further.  Every labelled target of an unlabelled element carries the
-// current level (an earlier one would have labelled the element earlier).
-__global__ void rg_pull_kernel(int n, const int32_t *__restrict__ map, int arity, int ntargets,
-                               uint64_t *__restrict__ ekey, const unsigned long long *__restrict__ tkey,
-                               int32_t *__restrict__ changed) {
+// One level of the search in one pass: unlabelled elements take the
+// smallest key of level <= `level` among their targets, one level further,
+// and hand the new key to their own targets at once.  Keys of level
+// `level` + 1 written during the pass are ignored by the pass's readers (a
+// level-`level` target would have labelled them earlier otherwise; the key's
+// level sits in its high word, so atomicMin never lets a level-`level`+1 key
+// replace an older one), so every pass reads what a separate push after the
+// whole previous pass would have left: the labels do not depend on
+// scheduling.  Every labelled target of an unlabelled element carries level
+// `level` (an earlier one would have labelled the element earlier).
+__global__ void rg_level_kernel(int n, const int32_t *__restrict__ map, int arity, int ntargets,
+                                uint32_t level, uint64_t *__restrict__ ekey,
+                                unsigned long long *__restrict__ tkey, int32_t *__restrict__ changed) {
   int any = 0;
+  const uint64_t limit = ((uint64_t)level + 1) << 32;   // keys below it: level <= `level`
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     if (ekey[e] != kUnset) continue;
     uint64_t best = kUnset;
     for (int r = 0; r < arity; ++r) {
       const int t = map[(int64_t)e * arity + r];
-      if (t >= 0 && t < ntargets) best = min(best, (uint64_t)tkey[t]);
+      if (t >= 0 && t < ntargets) {
+        const uint64_t k = (uint64_t)((volatile unsigned long long *)tkey)[t];
+        if (k < limit) best = min(best, k);
+      }
     }
     if (best != kUnset) {
-      ekey[e] = ((best >> 32) + 1) << 32 | (best & 0xffffffffull);
+      const uint64_t k = ((best >> 32) + 1) << 32 | (best & 0xffffffffull);
+      ekey[e] = k;
       any = 1;
+      for (int r = 0; r < arity; ++r) {
+        const int t = map[(int64_t)e * arity + r];
+        if (t >= 0 && t < ntargets) atomicMin(&tkey[t], (unsigned long long)k);
+      }
     }
   }
   if (__syncthreads_or(any) && threadIdx.x == 0) *changed = 1;
@@ -160,72 +177,141 @@ struct RgStage {
 // Neighbouring elements of a block (one ring of the breadth-first search)
 // touch neighbouring targets, so first-use numbers put the rows a warp reads
 // close together in shared memory.
+// The distinct targets are found with an open-addressing hash table in
+// shared memory (npow2 >= keys slots, so probing always ends); each slot
+// records the first key index that holds its target, and a scan over the key
+// indices of the flags "first use here" numbers the targets.  Which slot a
+// target lands in depends on the order of the inserts, the numbers do not.
+constexpr int kRgEmpty = INT_MIN;
+
 __global__ void rg_stage_kernel(const RgStage *__restrict__ stages, int nstage, int set_size,
                                 const int32_t *__restrict__ order, const int32_t *__restrict__ boff,
-                                int npow2, int32_t *__restrict__ tcnt, int16_t *__restrict__ loc) {
+                                int npow2, int keep_keys, int32_t *__restrict__ tcnt,
+                                int16_t *__restrict__ loc) {
   extern __shared__ int rg_smem[];
   const int blk = blockIdx.x, s = blockIdx.y;
   const RgStage st = stages[s];
   const int start = boff[blk], nelem = boff[blk + 1] - start;
   const int nkeys = nelem * st.arity;
-  int *a = rg_smem;             // keys, then (first use << 14 | sorted rank) pairs
-  int *u = rg_smem + npow2;     // sorted distinct targets
-  const int n = next_pow2_dev(nkeys);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int v = INT_MAX;
-    if (i < nkeys) {
+  const int H = npow2;
+  int *tab = rg_smem;           // [H] target of each slot
+  int *first = tab + H;         // [H] first key index of the slot's target, then -1 - its number
+  int *slot = first + H;        // [npow2] each key's slot
+  int *key = slot + npow2;      // [npow2] keys in position order (when keep_keys)
+  auto key_at = [&](int i) {
+    if (keep_keys) return key[i];
+    const int q = i / st.arity, r = i - q * st.arity;
+    return st.map[(int64_t)order[start + q] * st.arity + r];
+  };
+  for (int h = threadIdx.x; h < H; h += blockDim.x) {
+    tab[h] = kRgEmpty;
+    first[h] = INT_MAX;
+  }
+  if (keep_keys)
+    for (int i = threadIdx.x; i < nkeys; i += blockDim.x) {
       const int q = i / st.arity, r = i - q * st.arity;
-      v = st.map[(int64_t)order[start + q] * st.arity + r];
+      key[i] = st.map[(int64_t)order[start + q] * st.arity + r];
     }
-    a[i] = v;
-  }
-  __syncthreads();
-  block_bitonic_sort(a, n);
-  const int nu = block_unique(a, nkeys, n, u);
-  // first use of every distinct target (keys < 16384, so 14 bits each)
-  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = INT_MAX;
   __syncthreads();
   for (int i = threadIdx.x; i < nkeys; i += blockDim.x) {
-    const int q = i / st.arity, r = i - q * st.arity;
-    const int j = lower_bound(u, nu, st.map[(int64_t)order[start + q] * st.arity + r]);
-    atomicMin(&a[j], (i << 14) | j);
+    const int v = key_at(i);
+    int h = (int)(rg_hash((uint32_t)v) & (uint32_t)(H - 1));
+    for (int probe = 0; probe < H; ++probe) {
+      const int cur = atomicCAS(&tab[h], kRgEmpty, v);
+      if (cur == kRgEmpty || cur == v) break;
+      h = (h + 1) & (H - 1);
+    }
+    slot[i] = h;
+    atomicMin(&first[h], i);
   }
   __syncthreads();
-  block_bitonic_sort(a, next_pow2_dev(nu));
-  // a[k] & 0x3fff: sorted rank of the k-th target by first use; invert it
-  int *num = u + npow2;         // [nu] first-use number of each sorted rank
-  for (int k = threadIdx.x; k < nu; k += blockDim.x) {
-    const int j = a[k] & 0x3fff;
-    st.tmp[(int64_t)blk * st.cap + k] = u[j];
-    num[j] = k;
+  // number the distinct targets by first use: a scan, in key order, of the
+  // flags "this key is its target's first use"; a numbered slot's entry
+  // becomes negative, which no later key index equals
+  int carry = 0;
+  for (int base = 0; base < nkeys; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int h = i < nkeys ? slot[i] : 0;
+    const int flag = (i < nkeys && first[h] == i) ? 1 : 0;
+    int tot;
+    const int pos = block_excl_scan(flag, &tot);
+    if (flag) {
+      first[h] = -1 - (carry + pos);
+      st.tmp[(int64_t)blk * st.cap + carry + pos] = tab[h];
+    }
+    carry += tot;
+    __syncthreads();
   }
-  __syncthreads();
   for (int i = threadIdx.x; i < nkeys; i += blockDim.x) {
     const int q = i / st.arity, r = i - q * st.arity;
-    const int v = st.map[(int64_t)order[start + q] * st.arity + r];
-    loc[(int64_t)(st.loc_row + r) * set_size + start + q] = (int16_t)num[lower_bound(u, nu, v)];
+    loc[(int64_t)(st.loc_row + r) * set_size + start + q] = (int16_t)(-1 - first[slot[i]]);
   }
-  if (threadIdx.x == 0) tcnt[blk * nstage + s] = nu;
+  if (threadIdx.x == 0) tcnt[blk * nstage + s] = carry;
 }
 
-// One CTA per block: greedy thread colouring in position order over the
+// Lane 0's part of the thread colouring: one round (colours base ..
+// base + 31) of the greedy rule over the block's positions in order, R
+// targets per position (R = 0: `rows` read at run time).  With R known the
+// position's targets sit in registers and both mask loads issue together.
+template <int R>
+__device__ __forceinline__ int rg_greedy_round(const int *__restrict__ tgt, int rows, int nelem,
+                                               int base, uint32_t *__restrict__ masks,
+                                               int *__restrict__ col, int &ncol) {
+  int remaining = 0;
+  for (int i = 0; i < nelem; ++i) {
+    if (base > 0 && col[i] >= 0) continue;
+    uint32_t m = 0u;
+    if (R > 0) {
+      int t[R > 0 ? R : 1];
+#pragma unroll
+      for (int k = 0; k < R; ++k) t[k] = tgt[i * R + k];
+#pragma unroll
+      for (int k = 0; k < R; ++k) m |= masks[t[k]];
+      if (m == 0xffffffffu) {
+        ++remaining;
+        continue;
+      }
+      const int c = __ffs(~m) - 1;
+      col[i] = base + c;
+      ncol = max(ncol, base + c + 1);
+#pragma unroll
+      for (int k = 0; k < R; ++k) masks[t[k]] |= 1u << c;
+    } else {
+      for (int k = 0; k < rows; ++k) m |= masks[tgt[i * rows + k]];
+      if (m == 0xffffffffu) {
+        ++remaining;
+        continue;
+      }
+      const int c = __ffs(~m) - 1;
+      col[i] = base + c;
+      ncol = max(ncol, base + c + 1);
+      for (int k = 0; k < rows; ++k) masks[tgt[i * rows + k]] |= 1u << c;
+    }
+  }
+  return remaining;
+}
+
+// One warp per block: greedy thread colouring in position order over the
 // block-local targets of the INC staged Maps (masks of 32 colours per round,
-// as pyop2/plan.pyx:282-324).  The CTA first gathers every element's INC
-// targets (block-local numbers, offset per staged Map) into shared memory;
-// one thread then colours from there.
+// as pyop2/plan.pyx:282-324).  The warp gathers every element's INC targets
+// (block-local numbers, offset per staged Map) into shared memory, lane 0
+// colours from there (the rule is sequential), and the warp then sorts the
+// positions by colour, stably: per chunk of 32 positions, a lane's rank is
+// the count of its colour so far plus the earlier lanes of the chunk with
+// the same colour.  One-warp CTAs let many blocks colour at once per SM.
 __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_t *__restrict__ inc,
                                 int nstage, int set_size, int inc_rows, int part_size,
                                 const int32_t *__restrict__ boff, const int32_t *__restrict__ tcnt,
                                 const int16_t *__restrict__ loc, int32_t *__restrict__ thrcol,
                                 int32_t *__restrict__ nthrcol, int32_t *__restrict__ newpos) {
   extern __shared__ uint32_t rg_masks[];  // [mask words][part_size*inc_rows targets][part_size
-                                          //  colours][part_size+1 counts][part_size ranks]
-  const int blk = blockIdx.x;
+                                          //  colours][part_size+1 counts]
+  const int blk = blockIdx.x, lane = threadIdx.x;
   const int start = boff[blk], nelem = boff[blk + 1] - start;
   // local target numbering: the INC staged Maps' lists one after the other
   __shared__ int s_base[64];
   __shared__ int s_total;
-  if (threadIdx.x == 0) {
+  if (lane == 0) {
     int b = 0;
     for (int q = 0; q < nstage; ++q) {
       s_base[q] = b;
@@ -233,53 +319,59 @@ __global__ void rg_color_kernel(const RgStage *__restrict__ stages, const int32_
     }
     s_total = b;
   }
-  __syncthreads();
+  __syncwarp();
   const int total = s_total;
   int *tgt = reinterpret_cast<int *>(rg_masks + total);   // [nelem][inc_rows]
   int row = 0;
   for (int q = 0; q < nstage; ++q) {
     if (!inc[q]) continue;
     for (int r = 0; r < stages[q].arity; ++r, ++row)
-      for (int i = threadIdx.x; i < nelem; i += blockDim.x)
+      for (int i = lane; i < nelem; i += 32)
         tgt[i * inc_rows + row] = s_base[q] + loc[(int64_t)(stages[q].loc_row + r) * set_size + start + i];
   }
   int *col = tgt + part_size * inc_rows;                   // [nelem]
-  for (int i = threadIdx.x; i < nelem; i += blockDim.x) col[i] = -1;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int base = 0, remaining = nelem, ncol = 0;
-    while (remaining > 0) {
-      for (int i = 0; i < total; ++i) rg_masks[i] = 0u;
-      remaining = 0;
-      for (int i = 0; i < nelem; ++i) {
-        if (col[i] >= 0) continue;
-        uint32_t m = 0u;
-        for (int k = 0; k < inc_rows; ++k) m |= rg_masks[tgt[i * inc_rows + k]];
-        if (m == 0xffffffffu) {
-          ++remaining;
-          continue;
-        }
-        const int c = __ffs(~m) - 1;
-        col[i] = base + c;
-        ncol = max(ncol, base + c + 1);
-        for (int k = 0; k < inc_rows; ++k) rg_masks[tgt[i * inc_rows + k]] |= 1u << c;
+  int *cnt = col + part_size;                              // [ncol + 1]
+  for (int i = lane; i < nelem; i += 32) col[i] = -1;
+  int ncol = 0;
+  for (int base = 0, more = nelem > 0; more; base += 32) {
+    for (int i = lane; i < total; i += 32) rg_masks[i] = 0u;
+    __syncwarp();
+    int remaining = 0;
+    if (lane == 0) {
+      switch (inc_rows) {
+        case 1: remaining = rg_greedy_round<1>(tgt, 1, nelem, base, rg_masks, col, ncol); break;
+        case 2: remaining = rg_greedy_round<2>(tgt, 2, nelem, base, rg_masks, col, ncol); break;
+        case 3: remaining = rg_greedy_round<3>(tgt, 3, nelem, base, rg_masks, col, ncol); break;
+        case 4: remaining = rg_greedy_round<4>(tgt, 4, nelem, base, rg_masks, col, ncol); break;
+        default: remaining = rg_greedy_round<0>(tgt, inc_rows, nelem, base, rg_masks, col, ncol);
       }
-      base += 32;
     }
-    nthrcol[blk] = ncol;
-    // stable counting sort of the positions by colour
-    int *cnt = col + part_size;
-    int *rank = cnt + part_size + 1;
-    for (int c = 0; c <= ncol; ++c) cnt[c] = 0;
-    for (int i = 0; i < nelem; ++i) ++cnt[col[i] + 1];
-    for (int c = 0; c < ncol; ++c) cnt[c + 1] += cnt[c];
-    for (int i = 0; i < nelem; ++i) rank[i] = cnt[col[i]]++;
+    more = __shfl_sync(0xffffffffu, remaining, 0) > 0;
+    __syncwarp();
   }
-  __syncthreads();
-  const int *rank = col + 2 * part_size + 1;
-  for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
-    thrcol[start + rank[i]] = col[i];
-    newpos[start + i] = start + rank[i];
+  ncol = __shfl_sync(0xffffffffu, ncol, 0);
+  if (lane == 0) nthrcol[blk] = ncol;
+  // stable counting sort of the positions by colour
+  for (int c = lane; c <= ncol; c += 32) cnt[c] = 0;
+  __syncwarp();
+  for (int i = lane; i < nelem; i += 32) atomicAdd(&cnt[col[i] + 1], 1);
+  __syncwarp();
+  if (lane == 0)
+    for (int c = 0; c < ncol; ++c) cnt[c + 1] += cnt[c];   // cnt[c]: first rank of colour c
+  __syncwarp();
+  const unsigned below = (1u << lane) - 1u;
+  for (int i0 = 0; i0 < nelem; i0 += 32) {
+    const int i = i0 + lane;
+    const int c = i < nelem ? col[i] : -1 - lane;          // idle lanes match nobody
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    const int rank = i < nelem ? cnt[c] + __popc(peers & below) : 0;
+    __syncwarp();
+    if (i < nelem) {
+      if (lane == 31 - __clz(peers)) cnt[c] += __popc(peers);
+      thrcol[start + rank] = c;
+      newpos[start + i] = start + rank;
+    }
+    __syncwarp();
   }
 }
 
@@ -483,15 +575,15 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
     RG_CUDA(cudaMemcpyAsync(&nseeds, scal, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     rg_init_kernel<<<grid, kRgThreads, 0, s>>>(n, flag, rank, ekey);
     RG_CUDA(cudaMemsetAsync(tkey, 0xff, sizeof(uint64_t) * (size_t)grow_ntargets, s));
+    // the seeds hand their keys to their targets; each level's pass then
+    // hands on the keys of the elements it labels
+    rg_push_kernel<<<grid, kRgThreads, 0, s>>>(n, gmap, grow_arity, grow_ntargets, 0u, ekey, tkey);
     // levels in chunks; changed[j] records whether level base+j labelled anything
     for (int base = 0; base < kRgMaxLevels; base += kRgLevelChunk) {
       RG_CUDA(cudaMemsetAsync(scal, 0, sizeof(int32_t) * kRgLevelChunk, s));
-      for (int j = 0; j < kRgLevelChunk; ++j) {
-        rg_push_kernel<<<grid, kRgThreads, 0, s>>>(n, gmap, grow_arity, grow_ntargets,
-                                                   (uint32_t)(base + j), ekey, tkey);
-        rg_pull_kernel<<<grid, kRgThreads, 0, s>>>(n, gmap, grow_arity, grow_ntargets, ekey, tkey,
-                                                   scal + j);
-      }
+      for (int j = 0; j < kRgLevelChunk; ++j)
+        rg_level_kernel<<<grid, kRgThreads, 0, s>>>(n, gmap, grow_arity, grow_ntargets,
+                                                    (uint32_t)(base + j), ekey, tkey, scal + j);
       int32_t changed[kRgLevelChunk];
       RG_CUDA(cudaGetLastError());
       RG_CUDA(cudaMemcpyAsync(changed, scal, sizeof changed, cudaMemcpyDeviceToHost, s));
@@ -576,10 +668,13 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
     RG_CUDA(cudaMemcpyAsync(d_st, h_st.data(), sizeof(RgStage) * nstage, cudaMemcpyHostToDevice, s));
     int npow2 = 1;
     while (npow2 < part_size * max_arity) npow2 <<= 1;
-    const int smem = 3 * npow2 * (int)sizeof(int);
+    // the block's keys stay in shared memory when they fit beside the three
+    // working arrays, else they are read again from the Map
+    const int keep_keys = 4LL * npow2 * (int64_t)sizeof(int) <= smem_optin() ? 1 : 0;
+    const int smem = (3 + keep_keys) * npow2 * (int)sizeof(int);
     RG_CUDA(cudaFuncSetAttribute(rg_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    rg_stage_kernel<<<dim3(nblocks, nstage), kRgThreads, smem, s>>>(d_st, nstage, n, P->order,
-                                                                      P->boff, npow2, P->tcnt, P->loc);
+    rg_stage_kernel<<<dim3(nblocks, nstage), kRgStageThreads, smem, s>>>(
+        d_st, nstage, n, P->order, P->boff, npow2, keep_keys, P->tcnt, P->loc);
     RG_CUDA(cudaGetLastError());
     std::vector<int32_t> h_cnt((size_t)nblocks * nstage);
     RG_CUDA(cudaMemcpyAsync(h_cnt.data(), P->tcnt, sizeof(int32_t) * h_cnt.size(),
@@ -613,7 +708,7 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
         mask_words += P->max_count[q];
         inc_rows += stage_arity[q];
       }
-    const int64_t cwords = mask_words + (int64_t)part_size * inc_rows + 3LL * part_size + 1;
+    const int64_t cwords = mask_words + (int64_t)part_size * inc_rows + 2LL * part_size + 1;
     if (cwords * 4 > smem_optin())
       return fail(set_error(OP2B_ERR_ARG, "region plan: colouring needs %lld bytes of shared memory",
                             (long long)(cwords * 4)));
@@ -624,7 +719,7 @@ int op2b_region_plan_build(int32_t set_size, int32_t part_size, int32_t region_s
     RG_TRY(alloc((void **)&newpos, sizeof(int32_t) * n, true));
     RG_TRY(alloc((void **)&order2, sizeof(int32_t) * n, true));
     RG_TRY(alloc((void **)&loc2, sizeof(int16_t) * (size_t)loc_rows * n, true));
-    rg_color_kernel<<<nblocks, 128, csmem, s>>>(d_st, d_inc, nstage, n, inc_rows, part_size, P->boff,
+    rg_color_kernel<<<nblocks, 32, csmem, s>>>(d_st, d_inc, nstage, n, inc_rows, part_size, P->boff,
                                                 P->tcnt, P->loc, P->thrcol, P->nthrcol, newpos);
     RG_CUDA(cudaGetLastError());
     rg_permute_kernel<<<grid, kRgThreads, 0, s>>>(n, loc_rows, newpos, P->order, P->loc, order2, loc2);
