@@ -1778,6 +1778,19 @@ class _BoundLoop(object):
                 self._scratch += [part, cnt]
                 vals["gp%d" % j], vals["gc%d" % j] = part.ptr, cnt.ptr
         self._gptr = [None] * len(self._gbl)
+        # reduction Globals whose value before the loop can travel in the
+        # launch parameters: (flag field offset, struct format of one value)
+        self._ginit = []
+        for j, s in enumerate(self.gbl_specs):
+            g = self.spec.gbls[j]
+            if codegen.gbl_init_fields(g):
+                dt = loop.args[gargs[j]].data.dtype
+                fmt = ("<d" if dt == np.float64 else "<f4x" if dt == np.float32 else
+                       "<q" if dt.kind == "i" else "<Q")
+                self._ginit.append((self.layout.offset("gf%d" % j), fmt))
+            else:
+                self._ginit.append(None)
+        self._gflag = [0] * len(self._gbl)
         self._written = [d for d in self.dats if any(m != "READ" for m in self.dat_access[id(d)])]
         self._reducing = [k for k, (_, _, red) in enumerate(self._gbl) if red]
         n = self.nelem
@@ -1813,9 +1826,25 @@ class _BoundLoop(object):
             rep.ensure(d)
         buf = self._buf
         args = loop.args
+        # one launch that reduces over the whole set can take a Global's value
+        # from the host in its parameters (no upload before the loop)
+        one_launch = rng is None and not self.indirect and not _state.get('capturing')
         for k, (off, ai, red) in enumerate(self._gbl):
             g = args[ai].data
-            g._to_device()
+            init = self._ginit[k]
+            flag = 0
+            if init is not None and one_launch and g._state in (HOST, DEVICE_UNALLOCATED):
+                if g._device is None:
+                    g._device = DeviceBuffer(max(g._data.nbytes, 16))
+                goff, fmt = init
+                for c, v in enumerate(g._data.reshape(-1)):
+                    struct.pack_into(fmt, buf, goff + 8 + 8 * c, v)
+                flag = 1
+            else:
+                g._to_device()
+            if flag != self._gflag[k]:
+                struct.pack_into("<q", buf, self._ginit[k][0], flag)
+                self._gflag[k] = flag
             ptr = g._device.ptr
             if ptr != self._gptr[k]:
                 struct.pack_into("<Q", buf, off, ptr)

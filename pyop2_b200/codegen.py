@@ -180,6 +180,8 @@ class ParamLayout(object):
             f.append("g%d" % j)
             if g[2] != "READ":
                 f += ["gp%d" % j, "gc%d" % j]
+            if gbl_init_fields(g):
+                f += ["gf%d" % j] + ["gv%d_%d" % (j, k) for k in range(g[1])]
         f.append("err")
         self.fields = f
         self.index = {n: i for i, n in enumerate(f)}
@@ -221,6 +223,10 @@ def _struct_decl(spec, layout):
             t = "%s *" % spec.stages[int(n[2:])][2]
         elif n.startswith("mr") or n.startswith("mc") or n.startswith("m"):
             t = "const int *"
+        elif n.startswith("gf"):
+            t = "op2b_i64 "
+        elif n.startswith("gv"):
+            t = "op2b_u64 "
         elif n.startswith("gp"):
             t = "%s *" % spec.gbls[int(n[2:])][0]
         elif n.startswith("gc"):
@@ -301,6 +307,28 @@ def _ro(a):
     return "true" if a.ro else "false"
 
 
+# A reduction Global's value before the loop may travel in the launch
+# parameters (fields gf<slot>: flag, gv<slot>_<k>: component k's bits in an
+# 8-byte word) instead of its device copy, for these types and at most
+# GBL_INIT_MAX components: a Global the host has just created or set then
+# needs no upload.  Expressions turning the word back into the value:
+_GBL_INIT = {"double": "__longlong_as_double((long long)%s)",
+             "float": "__int_as_float((int)(unsigned)%s)",
+             "int": "(int)%s", "unsigned int": "(unsigned int)%s",
+             "long long": "(long long)%s", "unsigned long long": "(unsigned long long)%s"}
+GBL_INIT_MAX = 4
+
+
+def gbl_init_fields(g):
+    """Whether a Global slot (ctype, cdim, access) carries its value before
+    the loop in the launch parameters."""
+    return g[2] != "READ" and g[0] in _GBL_INIT and g[1] <= GBL_INIT_MAX
+
+
+def _gbl_init(a, k):
+    return _GBL_INIT[a.ctype] % ("p.gv%d_%d" % (a.slot, k))
+
+
 def _gbl_prologue(spec, lines):
     for n, a in enumerate(spec.args):
         if a.kind != "gbl":
@@ -313,6 +341,10 @@ def _gbl_prologue(spec, lines):
             lines.append("  %s r%d[%d];" % (t, n, c))
             if a.access == "INC":
                 lines.append("  op2b_zero(r%d);" % n)
+            elif gbl_init_fields(spec.gbls[a.slot]):
+                for k in range(c):
+                    lines.append("  r%d[%d] = p.gf%d ? %s : p.g%d[%d];"
+                                 % (n, k, a.slot, _gbl_init(a, k), a.slot, k))
             else:
                 lines.append("  for (int k = 0; k < %d; ++k) r%d[k] = p.g%d[k];" % (c, n, a.slot))
 
@@ -320,8 +352,15 @@ def _gbl_prologue(spec, lines):
 def _gbl_epilogue(spec, lines):
     for n, a in enumerate(spec.args):
         if a.kind == "gbl" and a.access != "READ":
-            lines.append("  op2b_reduce<%d, %s, %d>(r%d, p.g%d, p.gp%d, p.gc%d);" %
-                         (_RED_OP[a.access], a.ctype, a.cdim, n, a.slot, a.slot, a.slot))
+            if gbl_init_fields(spec.gbls[a.slot]):
+                lines.append("  { const %s i%d[%d] = {%s};" % (
+                    a.ctype, n, a.cdim, ", ".join(_gbl_init(a, k) for k in range(a.cdim))))
+                lines.append("    op2b_reduce<%d, %s, %d>(r%d, p.g%d, p.gp%d, p.gc%d, p.gf%d != 0, i%d); }"
+                             % (_RED_OP[a.access], a.ctype, a.cdim, n, a.slot, a.slot, a.slot,
+                                a.slot, n))
+            else:
+                lines.append("  op2b_reduce<%d, %s, %d>(r%d, p.g%d, p.gp%d, p.gc%d);" %
+                             (_RED_OP[a.access], a.ctype, a.cdim, n, a.slot, a.slot, a.slot))
 
 
 def _direct_row(a, n, e, lines_pre, lines_post, indent):

@@ -283,9 +283,12 @@ __device__ __forceinline__ T op2b_block_reduce(T v, T *scratch) {
 
 // OP: 0 = INC (sum), 1 = MIN, 2 = MAX.  gbl: the Global's device value;
 // partials: >= gridDim.x * N values; counter: zero before the launch, reset to
-// zero by the last CTA.
+// zero by the last CTA.  from_init: the last CTA combines with init[] (the
+// value before the loop, carried in the launch parameters, so a Global the
+// host has just set needs no upload) instead of reading gbl.
 template <int OP, typename T, int N>
-__device__ __forceinline__ void op2b_reduce(const T (&v)[N], T *gbl, T *partials, unsigned *counter) {
+__device__ __forceinline__ void op2b_reduce(const T (&v)[N], T *gbl, T *partials, unsigned *counter,
+                                            bool from_init = false, const T *init = nullptr) {
   __shared__ T red_scratch[32];
   __shared__ bool red_last;
 #pragma unroll
@@ -305,7 +308,7 @@ __device__ __forceinline__ void op2b_reduce(const T (&v)[N], T *gbl, T *partials
     for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
       acc = op2b_combine<OP>(acc, __ldcg(&partials[b * N + k]));
     acc = op2b_block_reduce<OP>(acc, red_scratch);
-    if (threadIdx.x == 0) gbl[k] = op2b_combine<OP>(gbl[k], acc);
+    if (threadIdx.x == 0) gbl[k] = op2b_combine<OP>(from_init ? init[k] : gbl[k], acc);
   }
   if (threadIdx.x == 0) *counter = 0u;
 }

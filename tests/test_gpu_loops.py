@@ -682,3 +682,49 @@ def test_read_replica_follows_writes(backend):
     run()
     x.zero()
     run()
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32, np.int32, np.uint64])
+def test_reduction_initial_value_in_launch_parameters(backend, dtype):
+    """A reduction Global the host has just created or set travels into the
+    loop in its launch parameters (no upload); its device value is used once
+    the device holds the newest copy, and always inside a recorded graph."""
+    from pyop2_b200 import b200, op2
+    n = 1000
+    s = op2.Set(n)
+    x = op2.Dat(s, np.arange(n) % 7, dtype, "x")
+    ct = {np.float64: "double", np.float32: "float", np.int32: "int",
+          np.uint64: "unsigned long long"}[dtype]
+    k = op2.Kernel("void k(%s *a, %s *g, %s *lo, %s *hi) { g[0] += a[0]; g[1] += 1;"
+                   " if (a[0] < lo[0]) lo[0] = a[0]; if (a[0] > hi[0]) hi[0] = a[0]; }"
+                   % (ct, ct, ct, ct), "k")
+    g = op2.Global(2, [3, 4], dtype, "g")
+    lo = op2.Global(1, 5, dtype, "lo")
+    hi = op2.Global(1, 2, dtype, "hi")
+
+    def run():
+        op2.par_loop(k, s, x(op2.IdentityMap, op2.READ), g(op2.INC), lo(op2.MIN), hi(op2.MAX))
+
+    tot = int((np.arange(n) % 7).sum())
+    run()                                        # fresh Globals: values from the parameters
+    np.testing.assert_array_equal(g.data_ro, np.array([3 + tot, 4 + n], dtype))
+    assert lo.data_ro[0] == 0 and hi.data_ro[0] == 6
+    run()                                        # device copies are the newest
+    np.testing.assert_array_equal(g.data_ro, np.array([3 + 2 * tot, 4 + 2 * n], dtype))
+    g.data = np.array([1, 1], dtype)             # host write
+    lo.data = np.array([9], dtype)
+    hi.data = np.array([-1 if dtype in (np.float64, np.float32, np.int32) else 0], dtype)
+    run()
+    np.testing.assert_array_equal(g.data_ro, np.array([1 + tot, 1 + n], dtype))
+    assert lo.data_ro[0] == 0 and hi.data_ro[0] == 6
+    g.data = np.array([0, 0], dtype)
+    run()
+    with b200.capture() as graph:                # graph: the device value each replay
+        run()
+    graph.launch()
+    graph.launch()
+    np.testing.assert_array_equal(g.data_ro, np.array([3 * tot, 3 * n], dtype))
+    graph.close()
+    g.data = np.array([2, 2], dtype)
+    run()
+    np.testing.assert_array_equal(g.data_ro, np.array([2 + tot, 2 + n], dtype))
