@@ -403,42 +403,51 @@ def run_gpu(args, ws, rank, local):
 
     # ---------------- roofline: res_calc's launches inside the step.  The
     # step is recorded once more with a CUDA event pair around each of its
-    # loops (event nodes of the graph, on the op2 stream) and replayed as in
-    # the timed region (L2 flush, then the step); each replay's per-loop
-    # durations are read back (res_calc's two give the roofline figure).
-    marks = []
+    # two res_calc launches (event nodes of the graph, on the op2 stream)
+    # and replayed as in the timed region (L2 flush, then the step); each
+    # replay's two res_calc durations are read back.  A second recording
+    # marks every loop the same way for the per-loop breakdown (each event
+    # node adds a little to the loop it follows, so short loops read high).
+    def marked_step(names):
+        marks = []
 
-    def marked(name, fn):
-        e0, e1 = b200.Event(), b200.Event()
-        e0.record(node=True)
-        fn()
-        e1.record(node=True)
-        marks.append((name, e0, e1))
+        def marked(name, fn):
+            if name not in names:
+                fn()
+                return
+            e0, e1 = b200.Event(), b200.Event()
+            e0.record(node=True)
+            fn()
+            e1.record(node=True)
+            marks.append((name, e0, e1))
 
-    def step_marked():
-        rms.zero()
-        marked("save_soln", lambda: airfoil.save_soln(op2, A))
-        for k in range(2):
-            marked("adt_calc", lambda: airfoil.adt_calc(op2, A))
-            marked("res_calc", lambda: airfoil.res_calc(op2, A))
-            marked("bres_calc", lambda: airfoil.bres_calc(op2, A))
-            marked("update", lambda: airfoil.update(op2, A, rms))
+        def run():
+            rms.zero()
+            marked("save_soln", lambda: airfoil.save_soln(op2, A))
+            for k in range(2):
+                marked("adt_calc", lambda: airfoil.adt_calc(op2, A))
+                marked("res_calc", lambda: airfoil.res_calc(op2, A))
+                marked("bres_calc", lambda: airfoil.bres_calc(op2, A))
+                marked("update", lambda: airfoil.update(op2, A, rms))
 
-    with b200.capture() as gm:
-        step_marked()
-    for _ in range(3):
-        b200.l2_flush()
-        gm.launch()
-    in_step = {}
-    for _ in range(max(10, min(args.steps, 50))):
-        b200.l2_flush()
-        gm.launch()
-        b200.synchronize()
-        for name, a, b in marks:
-            in_step.setdefault(name, []).append(a.elapsed_ms(b))
-    gm.close()
-    res_in_step = in_step["res_calc"]
+        with b200.capture() as gm:
+            run()
+        for _ in range(3):
+            b200.l2_flush()
+            gm.launch()
+        out = {}
+        for _ in range(max(10, min(args.steps, 50))):
+            b200.l2_flush()
+            gm.launch()
+            b200.synchronize()
+            for name, a, b in marks:
+                out.setdefault(name, []).append(a.elapsed_ms(b))
+        gm.close()
+        return out
+
+    res_in_step = marked_step(("res_calc",))["res_calc"]
     res_avg = statistics.mean(res_in_step)
+    in_step = marked_step(("save_soln", "adt_calc", "res_calc", "bres_calc", "update"))
 
     # ---------------- per-loop breakdown: each loop's mean time inside the
     # replayed step (above), and beside it ("alone_ms") the loop replayed
