@@ -15,9 +15,10 @@
 //  * order: elements sorted by (region, level, element id);
 //  * blocks: each region cut into nearly equal runs of at most part_size
 //    elements;
-//  * staging: per block and staged Map the sorted distinct targets over all
-//    Map rows (tlist / toff / tcnt) and, per position of the reordered set
-//    and Map row, the target's index in that list (loc, int16);
+//  * staging: per block and staged Map the distinct targets over all Map
+//    rows in order of first use (tlist / toff / tcnt) and, per position of
+//    the reordered set and Map row, the target's index in that list (loc,
+//    int16);
 //  * thread colouring: per block, the reference's greedy colouring
 //    (pyop2/plan.pyx:282-324: elements in order, 32-colour masks per round)
 //    over the targets of the staged Maps marked as INC targets, so elements
