@@ -1443,6 +1443,10 @@ def loop_spec(loop, block_size=None, fmad=None, owner_mode=None, mat_nnz_max=Non
                     and all(m.sparsity._max_row_nnz() <= 254 for m in mats)):
                 spec.mat_slots_rel = True
             split = cfg.cfg['itspace_split']
+            if split == "auto":
+                # large local blocks (P2 6x6 and up): 3 x 2 warps per 32
+                # elements measured fastest; small ones keep one thread
+                split = "3x2" if len(extents) == 2 and extents[0] * extents[1] >= 36 else ""
             if (split and spec.mat_per_entry and len(extents) == 2
                     and all(s.kind == "mat" or s.access == "READ" for s in specs)):
                 nr, nc = (int(v) for v in str(split).lower().split("x"))

@@ -97,8 +97,9 @@ keys of the B200 backend:
   space of an atomic-form Mat assembly (scalar Mats added entry by entry,
   every other argument READ) into R x C blocks of local positions evaluated
   by different warps for the same 32 elements: fewer values live per
-  thread, more warps resident; ``''`` (default) keeps one thread per
-  element;
+  thread, more warps resident; ``''`` keeps one thread per element;
+  ``'auto'`` (default) splits 3 x 2 when the local block has at least 36
+  entries (P2 and up) and keeps one thread per element below;
 * ``mat_slots_rel``: with per-entry adds, read each local row's columns
   from a compact slot table (one 64-bit word of in-row positions per element
   and local row, added to the row start read through the Map) instead of one
@@ -145,7 +146,7 @@ _defaults = {
     'gathered_max_gb': 2.0,
     'fmad_inc': False,
     'programmatic_launch': False,
-    'itspace_split': '',
+    'itspace_split': 'auto',
     'staged_tl_regs': False,
     'direct_unroll': 1,
     'mat_slots_rel': False,
