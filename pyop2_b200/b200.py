@@ -1815,7 +1815,8 @@ class _BoundLoop(object):
         self._run(loop, rng)
         args = loop.args
         gbl = tuple((id(args[ai].data), "W" if red else "R") for _, ai, red in self._gbl)
-        trace.append((pre, _capture_tail(), self.accesses + gbl))
+        n = self.nelem if rng is None else rng[1] - rng[0]
+        trace.append((pre, _capture_tail(), self.accesses + gbl, n))
 
     def _run(self, loop, rng=None):
         if getattr(self, "_buf", None) is None:
@@ -2347,20 +2348,23 @@ def _capture_tail():
     return node.value
 
 
-def _relaxed_exec(graph, trace):
+def _relaxed_exec(graph, trace, small_only=False):
     """Instantiate the captured chain ``graph`` with the edges between
     independent par_loops dropped (:mod:`pyop2_b200.overlap`); ``trace``
-    holds per loop the chain's tail before and after its nodes and its
-    accesses.  A loop of more than one node, and any node between loops,
-    is a barrier."""
-    marks = [m for pre, post, _ in trace for m in (pre, post)]
+    holds per loop the chain's tail before and after its nodes, its
+    accesses and its element count.  A loop of more than one node, and any
+    node between loops, is a barrier.  ``small_only``: only loops over fewer
+    elements than one 256-thread CTA per SM covers are relaxed; the others
+    keep program order among themselves."""
+    marks = [m for pre, post, _, _ in trace for m in (pre, post)]
     nm = len(marks)
     pos = (C.c_int64 * max(nm, 1))()
     nnodes = C.c_int64()
     call("op2b_graph_chain_positions", graph, (C.c_uint64 * max(nm, 1))(*marks), nm, pos,
          C.byref(nnodes))
-    segs, cursor = [], 0
-    for k, (_, _, acc) in enumerate(trace):
+    segs, cursor, small = [], 0, []
+    limit = _state['sm_count'] * 256
+    for k, (_, _, acc, n) in enumerate(trace):
         first, last = pos[2 * k] + 1, pos[2 * k + 1]
         if last < first:
             continue                      # the loop added no node
@@ -2368,11 +2372,14 @@ def _relaxed_exec(graph, trace):
             raise DeviceError("overlapped capture: loop %d's nodes are out of order" % k)
         if first > cursor:
             segs.append((cursor, first - 1, None))
+            small.append(False)
         segs.append((first, last, acc if last == first else None))
+        small.append(last == first and n < limit)
         cursor = last + 1
     if cursor < nnodes.value:
         segs.append((cursor, nnodes.value - 1, None))
-    deps = overlap.dependencies([acc for _, _, acc in segs])
+        small.append(False)
+    deps = overlap.dependencies([acc for _, _, acc in segs], small if small_only else None)
     ptr, idx = [0], []
     for d in deps:
         idx.extend(d)
@@ -2398,11 +2405,18 @@ class capture(object):
 
     ``overlap`` (default: the ``graph_overlap`` configuration key) lets
     loops that touch no common data in a conflicting way run side by side
-    in the graph (:mod:`pyop2_b200.overlap`); other device work recorded in
-    the block stays in program order with everything around it."""
+    in the graph (:mod:`pyop2_b200.overlap`): ``True`` relaxes every loop,
+    ``'small'`` only loops too small to fill the GPU (the others keep
+    program order among themselves), ``False`` none; other device work
+    recorded in the block stays in program order with everything around
+    it."""
 
     def __init__(self, overlap=None):
-        self.overlap = bool(cfg.cfg['graph_overlap']) if overlap is None else bool(overlap)
+        mode = cfg.cfg['graph_overlap'] if overlap is None else overlap
+        if mode not in (True, False, "small"):
+            raise ValueError("overlap %r (True, False or 'small')" % (mode,))
+        self.overlap = bool(mode)
+        self.small_only = mode == "small"
 
     def __enter__(self):
         self.graph = Graph()
@@ -2430,7 +2444,8 @@ class capture(object):
         _lib.check(rc, "op2b_graph_end_capture")
         try:
             # segments (par_loop or barrier) and the earlier segments each follows
-            self.graph.handle, self.graph.segments = _relaxed_exec(g.value, trace)
+            self.graph.handle, self.graph.segments = _relaxed_exec(g.value, trace,
+                                                                    self.small_only)
         finally:
             call("op2b_graph_free", g.value)
         return False

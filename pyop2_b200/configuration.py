@@ -106,7 +106,10 @@ keys of the B200 backend:
   32-bit position per local entry;
 * ``graph_overlap``: a CUDA graph recorded with ``b200.capture`` lets
   par_loops that touch no common data in a conflicting way run side by side
-  (reads of one object, atomic increments of one object); other device work
+  (reads of one object, atomic increments of one object): ``True`` every
+  such loop, ``'small'`` only loops over fewer elements than one 256-thread
+  CTA per SM covers (they run beside their big neighbours, which keep
+  program order among themselves), ``False`` none; other device work
   recorded in the graph stays in program order with everything around it;
 * ``hbm_budget_gb``: device memory (GB) the serving engine's MeshStore
   admits meshes and requests against by default;

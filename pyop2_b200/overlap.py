@@ -41,9 +41,32 @@ def loop_accesses(pairs):
     return tuple(out.items())
 
 
-def dependencies(segments):
+def dependencies(segments, floating=None):
     """For each segment (accesses or None, in program order) the sorted list
-    of earlier segments it must follow."""
+    of earlier segments it must follow.
+
+    ``floating`` (optional, one flag per segment): only the flagged loops
+    are relaxed; every other loop also follows the previous unflagged loop
+    (or barrier), so those keep program order among themselves.  The
+    flagged ones are loops too small to fill the GPU, which then run beside
+    their big neighbours instead of taking a turn of their own."""
+    deps = _relaxed(segments)
+    if floating is None:
+        return deps
+    out, prev = [], None
+    for i, acc in enumerate(segments):
+        d = set(deps[i])
+        if acc is None:
+            prev = i
+        elif not floating[i]:
+            if prev is not None:
+                d.add(prev)
+            prev = i
+        out.append(sorted(d))
+    return out
+
+
+def _relaxed(segments):
     deps = []
     state = {}            # key -> {"w": writers, "r": readers, "inc": bool, "base": list}
     barrier = None

@@ -102,3 +102,52 @@ def test_overlapped_capture_keeps_other_device_work_in_order(op2):
     np.testing.assert_array_equal(b.data_ro.ravel(), np.zeros(n))
     assert [is_loop for is_loop, _ in g.segments] == [True, False, True]
     assert g.segments[2][1] == [1]
+
+
+def test_small_loops_float_beside_big_ones(op2):
+    """overlap='small': on a mesh whose cells and edges fill the GPU only
+    bres_calc (900 boundary edges) is relaxed -- it runs beside res_calc --
+    while the big loops keep program order; results as in program order."""
+    from pyop2_b200 import b200, base
+    from pyop2_b200.workloads import airfoil
+    for c in list(base.Const._defs):
+        c.remove_from_namespace()
+    A = airfoil.build(op2, 300, 150, 0)
+    q0 = A.p_q.data_ro.copy()
+    rms = op2.Global(1, 0.0, np.float64, "rms")
+    dats = (A.p_q, A.p_qold, A.p_adt, A.p_res)
+
+    def reset():
+        A.p_q.data[:] = q0
+        A.p_qold.data[:] = q0
+        A.p_adt.data[:] = 0.0
+        A.p_res.data[:] = 0.0
+        _upload(*dats)
+
+    def step():
+        rms.zero()
+        airfoil.iteration(op2, A, rms)
+
+    reset()
+    step()
+    reset()
+    for _ in range(3):
+        step()
+    ref_q, ref_rms = A.p_q.data_ro.copy(), float(rms.data[0])
+    reset()
+    with b200.capture(overlap="small") as g:
+        step()
+    for _ in range(3):
+        g.launch()
+    q, r = A.p_q.data_ro.copy(), float(rms.data[0])
+    assert np.abs(q - ref_q).max() <= 1e-12 * np.abs(ref_q).max()
+    assert abs(r - ref_rms) <= 1e-12 * abs(ref_rms)
+    segs = g.segments
+    assert len(segs) == 10
+    assert 1 in segs[2][1]                    # adt_calc after save_soln (both big)
+    assert 2 in segs[3][1]                    # res_calc after adt_calc
+    assert 3 not in segs[4][1]                # bres_calc beside res_calc
+    assert {3, 4} <= set(segs[5][1])          # update after both
+    with pytest.raises(ValueError):
+        b200.capture(overlap="sometimes")
+    g.close()

@@ -88,3 +88,31 @@ def test_mixed_kinds_of_one_key_write():
     assert dict(overlap.loop_accesses([("a", "I"), ("a", "I")]))["a"] == "I"
     with pytest.raises(ValueError):
         overlap.dependencies([(("a", "X"),)])
+
+
+def test_airfoil_step_small_loops_float():
+    """Only bres_calc (3,600 edges) floats: it runs beside res_calc, while
+    the big loops keep program order among themselves."""
+    fl = [False, False, False, True, False, False, False, True, False]
+    d = overlap.dependencies(_airfoil_step(), fl)
+    assert d[1] == [0]                     # adt_calc after save_soln (both big)
+    assert d[2] == [1]
+    assert d[3] == [1]                     # bres_calc beside res_calc
+    assert d[4] == [0, 1, 2, 3]            # update waits for both
+    assert d[5] == [1, 2, 3, 4]
+    assert d[7] == [4, 5]                  # the second bres_calc beside the second res_calc
+    assert d[8] == [0, 4, 5, 6, 7]
+    # nothing floats: program order
+    chain = overlap.dependencies(_airfoil_step(), [False] * 9)
+    assert all(i - 1 in chain[i] for i in range(1, 9))
+
+
+def test_floating_loops_keep_every_conflict_ordered():
+    """A floating loop still follows every conflicting earlier loop, and a
+    barrier orders everything around it."""
+    segs = [(("a", "W"),), (("b", "W"),), None, (("a", "R"),), (("c", "W"),)]
+    d = overlap.dependencies(segs, [False, True, False, True, False])
+    assert d[1] == []                      # floats: no conflict with segment 0
+    assert d[2] == [0, 1]                  # barrier after both
+    assert d[3] == [2]                     # after the barrier only
+    assert d[4] == [2]                     # big loop: after the barrier (previous big)
