@@ -497,3 +497,33 @@ def test_batched_coloured_form_compiles(host_op2):
     assert spec.mode == "atomic" and spec.mat_alias == (0, 0) and spec.mat_per_entry
     src, _, _ = nvrtc_compile(spec)
     assert "p.ms1" not in src.split("extern \"C\"")[-1]
+
+
+def test_reduction_initial_value_fields(host_op2):
+    """A reduction Global of a supported type and at most four components
+    gets a flag and one 8-byte word per component in the parameter block;
+    the stub takes the value before the loop from them when the flag is set
+    (MIN/MAX start from it, the last CTA combines the sum with it); larger
+    or READ Globals keep the device value only.  Every form compiles."""
+    op2 = host_op2
+    s = op2.Set(10, 1)
+    x = op2.Dat(s, np.zeros(10), np.float64)
+    for dt, ct in ((np.float64, "double"), (np.float32, "float"), (np.int32, "int"),
+                   (np.uint32, "unsigned int"), (np.int64, "long long"),
+                   (np.uint64, "unsigned long long")):
+        g = op2.Global(3, [0, 0, 0], dt)
+        big = op2.Global(5, [0] * 5, dt)
+        rd = op2.Global(1, [1], dt)
+        k = op2.Kernel("void k(double *a, %s *g, %s *b, %s *r) { }" % (ct, ct, ct), "k")
+        for acc in (op2.INC, op2.MIN, op2.MAX):
+            src, layout, _ = nvrtc_compile(spec_of(op2, k, s, x(op2.IdentityMap, op2.READ),
+                                                   g(acc), big(op2.INC), rd(op2.READ)))
+            f = layout.fields
+            assert ["gf0", "gv0_0", "gv0_1", "gv0_2"] == [n for n in f if n.startswith(("gf0", "gv0"))]
+            assert not any(n.startswith(("gf1", "gv1", "gf2", "gv2")) for n in f)
+            assert "p.gf0 != 0, i1" in src
+            if acc is not op2.INC:
+                assert "r1[2] = p.gf0 ?" in src
+    assert not codegen.gbl_init_fields(("unsigned char", 1, "INC"))
+    assert not codegen.gbl_init_fields(("double", 1, "READ"))
+    assert codegen.gbl_init_fields(("double", codegen.GBL_INIT_MAX, "MAX"))
