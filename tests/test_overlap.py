@@ -116,3 +116,15 @@ def test_floating_loops_keep_every_conflict_ordered():
     assert d[2] == [0, 1]                  # barrier after both
     assert d[3] == [2]                     # after the barrier only
     assert d[4] == [2]                     # big loop: after the barrier (previous big)
+
+
+def test_capture_modes():
+    """b200.capture(overlap=...) accepts True, False and 'small' (the
+    configuration key's values) and nothing else; no device is touched
+    before the block is entered."""
+    from pyop2_b200 import b200
+    assert (b200.capture(overlap=True).overlap, b200.capture(overlap=True).small_only) == (True, False)
+    assert (b200.capture(overlap="small").overlap, b200.capture(overlap="small").small_only) == (True, True)
+    assert b200.capture(overlap=False).overlap is False
+    with pytest.raises(ValueError):
+        b200.capture(overlap="sometimes")
